@@ -1,0 +1,260 @@
+/*
+ * mpm_b200.h -- C ABI of the B200-native MPM snow step.
+ *
+ * This is the drop-in boundary for the particle step of H-YWu/mpm
+ * (chains::MPMSolver3D / chains::APICMPMSolver3D).  Every entry point takes
+ * plain pointers and sizes; no CUDA, Eigen or torch type crosses it.  Each
+ * declaration names the reference interface it replaces (file:line inside the
+ * reference project).
+ *
+ * Conventions
+ *  - Every call returns an mpm_status.  Nothing in the library calls exit();
+ *    mpm_last_error_string() returns a message for the calling thread.
+ *  - Host arrays of 3-vectors are interleaved (x0,y0,z0,x1,...), matching the
+ *    Eigen::Vector3f layout of the reference's particles.
+ *  - Particle downloads are returned in the caller's original particle order,
+ *    although the device keeps particles sorted by grid cell.
+ *  - A solver handle is single-threaded; each handle owns one CUDA stream.
+ */
+#ifndef MPM_B200_H_
+#define MPM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPM_API __attribute__((visibility("default")))
+#else
+#define MPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_B200_ABI_VERSION 1
+
+/* Status codes.  The reference prints and calls exit() on CUDA errors
+ * (include/cuda_utils.h:6-20) and throws std::runtime_error on bad enums
+ * (src/mpm3d_parser.cpp:10,17); here both become return codes. */
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID_ARG = 1,
+    MPM_ERR_IO = 2,
+    MPM_ERR_PARSE = 3,
+    MPM_ERR_OOM = 4,
+    MPM_ERR_CUDA = 5,
+    MPM_ERR_NUMERIC = 6,   /* NaN/Inf particle state detected on the device */
+    MPM_ERR_BUDGET = 7,    /* device-memory budget of a batch exceeded       */
+    MPM_ERR_TIMEOUT = 8,
+    MPM_ERR_UNSUPPORTED = 9
+} mpm_status;
+
+/* chains::InterpolationType (include/enums.h:6-10) */
+enum {
+    MPM_INTERP_LINEAR = 0,
+    MPM_INTERP_QUADRATIC_BSPLINE = 1,
+    MPM_INTERP_CUBIC_BSPLINE = 2
+};
+
+/* chains::ConstitutiveModel (include/enums.h:12-15) */
+enum {
+    MPM_MODEL_FIXED_COROTATED = 0,
+    MPM_MODEL_NEO_HOOKEAN = 1
+};
+
+/* Transfer scheme: MPMSolver3D (PIC-FLIP, include/mpm_solver3d.h:21) or
+ * APICMPMSolver3D (include/apic_mpm_solver3d.h:20). */
+enum {
+    MPM_TRANSFER_PIC_FLIP = 0,
+    MPM_TRANSFER_APIC = 1
+};
+
+/* Grid boundary condition.
+ *  REFERENCE: applyBoundaryCollision on the grid box at the node's
+ *             "distorted" position x_i + dt v*_i (src/mpm_solver3d.cu:405-426,
+ *             src/collision_object3d.cu:7-54).
+ *  STICKY:    v* = 0 on nodes within `sticky_cells` of any grid face. */
+enum {
+    MPM_BOUNDARY_REFERENCE = 0,
+    MPM_BOUNDARY_STICKY = 1
+};
+
+/* Initial particle volume.
+ *  GRID_ESTIMATE: V0 = m / (sum_i m_i w_ip / h^3), as the reference's
+ *                 initialize() does (src/mpm_solver3d.cu:131-223).
+ *  PRESCRIBED:    V0 taken from mpm_particles_in.volume. */
+enum {
+    MPM_VOLUME_GRID_ESTIMATE = 0,
+    MPM_VOLUME_PRESCRIBED = 1
+};
+
+/* Per-group material.  Lame parameters are derived exactly as the
+ * reference's particle constructor does (src/material_point3d.cu:25-26). */
+typedef struct mpm_material {
+    float youngs_modulus;
+    float poisson_ratio;
+    float hardening;             /* xi      */
+    float critical_compression;  /* theta_c */
+    float critical_stretch;      /* theta_s */
+    int32_t model;               /* MPM_MODEL_* */
+} mpm_material;
+
+/* Scene description: the arguments of the reference's solver constructors
+ * (include/mpm_solver3d.h:25-34, include/apic_mpm_solver3d.h:24-32) plus the
+ * options the benchmark scenes need. */
+typedef struct mpm_scene_desc {
+    float origin[3];
+    int32_t resolution[3];
+    float stride;                /* grid spacing h                              */
+    float friction;              /* boundary friction coefficient               */
+    float blend;                 /* FLIP weight alpha (PIC-FLIP only)           */
+    float dt;                    /* fixed time step                             */
+    float gravity;               /* |g| along -y; the reference hard-codes 9.80665 */
+    int32_t transfer;            /* MPM_TRANSFER_*                              */
+    int32_t interpolation;       /* MPM_INTERP_*                                */
+    int32_t boundary;            /* MPM_BOUNDARY_*                              */
+    int32_t sticky_cells;        /* wall thickness in cells for STICKY          */
+    int32_t volume_mode;         /* MPM_VOLUME_*                                */
+    int32_t particles_collision; /* initial _enable_particles_collision (0/1)   */
+} mpm_scene_desc;
+
+/* Host-side particle input.  Replaces thrust::host_vector<MaterialPoint3D>
+ * (include/material_point3d.h:14-22); the per-particle material constants
+ * of the reference become an index into `materials`. */
+typedef struct mpm_particles_in {
+    size_t n;
+    const float* position;       /* 3n, interleaved                  */
+    const float* velocity;       /* 3n, interleaved                  */
+    const float* mass;           /* n                                */
+    const uint16_t* material;    /* n, may be NULL if nmaterials == 1 */
+    const float* volume;         /* n, only read for VOLUME_PRESCRIBED */
+    const mpm_material* materials;
+    int32_t nmaterials;
+} mpm_particles_in;
+
+/* Particle fields for mpm_solver_download (floats per particle). */
+enum {
+    MPM_FIELD_POSITION = 0,          /* 3 */
+    MPM_FIELD_VELOCITY = 1,          /* 3 */
+    MPM_FIELD_FE = 2,                /* 9, row-major */
+    MPM_FIELD_FP = 3,                /* 9, row-major */
+    MPM_FIELD_B = 4,                 /* 9, row-major, APIC only */
+    MPM_FIELD_VOLUME0 = 5,           /* 1 */
+    MPM_FIELD_MASS = 6,              /* 1 */
+    MPM_FIELD_POSITION4 = 7,         /* 4: (x, y, z, 1), the headless VBO export */
+    MPM_FIELD_DET_FE = 8,            /* 1 */
+    MPM_FIELD_DET_FP = 9             /* 1 */
+};
+
+/* Dense grid fields for mpm_solver_download_grid (floats per node, node
+ * index x + X*(y + Y*z) as in src/mpm_solver3d.cu:257). */
+enum {
+    MPM_GRID_MASS = 0,               /* 1 */
+    MPM_GRID_VELOCITY = 1,           /* 3: momentum after P2G, v after update */
+    MPM_GRID_FORCE = 2,              /* 3 */
+    MPM_GRID_VELOCITY_STAR = 3       /* 3 */
+};
+
+typedef struct mpm_solver mpm_solver;
+
+/* Library version / capability query. */
+MPM_API int32_t mpm_abi_version(void);
+/* Message for the last failing call on this thread ("" if none). */
+MPM_API const char* mpm_last_error_string(void);
+/* Number of CUDA devices visible (0 on a host without a GPU). */
+MPM_API mpm_status mpm_device_count(int32_t* count);
+/* Select the CUDA device that later solver/batch creations on this thread
+ * use (the library's CUDA runtime keeps its own current device). */
+MPM_API mpm_status mpm_set_device(int32_t device);
+
+/* Counters of the last step (read back from the device; synchronizes). */
+typedef struct mpm_step_stats {
+    uint32_t active_blocks;    /* 4^3-cell blocks holding particles          */
+    uint32_t outside_blocks;   /* scenes with particles whose stencil misses the grid */
+    uint32_t active_nodes;     /* grid nodes with non-zero mass              */
+    uint32_t reserved;
+} mpm_step_stats;
+
+/* Construct a solver on the current CUDA device, upload the particles and
+ * run initialize().  Replaces MPMSolver3D::MPMSolver3D
+ * (src/mpm_solver3d.cu:36-91) and APICMPMSolver3D::APICMPMSolver3D
+ * (src/apic_mpm_solver3d.cu:36-90). */
+MPM_API mpm_status mpm_solver_create(const mpm_scene_desc* desc,
+                             const mpm_particles_in* particles,
+                             mpm_solver** out);
+/* Replaces ~MPMSolver3D (src/mpm_solver3d.cu:93-98). */
+MPM_API mpm_status mpm_solver_destroy(mpm_solver* s);
+
+/* simulateOneStep() repeated nsteps times (src/mpm_solver3d.cu:100-125,
+ * src/apic_mpm_solver3d.cu:99-124).  Asynchronous on the solver's stream;
+ * returns errors of earlier steps. */
+MPM_API mpm_status mpm_solver_step(mpm_solver* s, int32_t nsteps);
+/* Wait for the solver's stream; reports MPM_ERR_NUMERIC if a non-finite
+ * particle state was seen since the last call. */
+MPM_API mpm_status mpm_solver_synchronize(mpm_solver* s);
+
+/* Sub-steps of simulateOneStep, run in split (unfused) form for testing and
+ * for callers that drive the step themselves
+ * (include/mpm_solver3d.h:40-63, include/apic_mpm_solver3d.h:38-61). */
+MPM_API mpm_status mpm_solver_initialize(mpm_solver* s);                  /* :131-223 */
+MPM_API mpm_status mpm_solver_reset_grid(mpm_solver* s);                  /* :225-235 */
+MPM_API mpm_status mpm_solver_particles_to_grid(mpm_solver* s);           /* :237-294 */
+MPM_API mpm_status mpm_solver_compute_external_forces(mpm_solver* s);     /* :296-298 */
+MPM_API mpm_status mpm_solver_compute_gravity_forces(mpm_solver* s);      /* :394-403 */
+MPM_API mpm_status mpm_solver_update_grid_velocities(mpm_solver* s, float dt);   /* :300-310 */
+MPM_API mpm_status mpm_solver_grid_collision(mpm_solver* s, float dt);    /* :405-426 */
+MPM_API mpm_status mpm_solver_solve_linear_system(mpm_solver* s, float dt);      /* :312-314, no-op */
+MPM_API mpm_status mpm_solver_grid_to_particles(mpm_solver* s, float dt, float blend); /* :316-379 */
+MPM_API mpm_status mpm_solver_particles_collision(mpm_solver* s, float dt);      /* :428-445 */
+MPM_API mpm_status mpm_solver_advect_particles(mpm_solver* s, float dt);  /* :381-391 */
+
+/* _enable_particles_collision and switchIfEnableParticlesCollision()
+ * (include/mpm_solver3d.h:23,40, src/mpm_solver3d.cu:127-129). */
+MPM_API mpm_status mpm_solver_set_particles_collision(mpm_solver* s, int32_t enable);
+MPM_API mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32_t* enable);
+
+MPM_API mpm_status mpm_solver_num_particles(const mpm_solver* s, size_t* n);
+MPM_API mpm_status mpm_solver_get_desc(const mpm_solver* s, mpm_scene_desc* desc);
+
+/* Download a particle field in the original particle order.  `host_out`
+ * holds n * floats-per-particle floats.  MPM_FIELD_POSITION4 replaces the
+ * GL buffer export (src/mpm_solver3d.cu:447-508). */
+MPM_API mpm_status mpm_solver_download(mpm_solver* s, int32_t field, float* host_out);
+/* Download a dense grid field (res^3 * components floats).  Valid after
+ * particles_to_grid() and the grid sub-steps of the split API, or after
+ * mpm_solver_step when the solver keeps the dense debug grid. */
+MPM_API mpm_status mpm_solver_download_grid(mpm_solver* s, int32_t field, float* host_out);
+
+/* Overwrite the particle state (original order) with host data of the same
+ * layout as mpm_solver_download; marks cached stress as stale. */
+MPM_API mpm_status mpm_solver_upload(mpm_solver* s, int32_t field, const float* host_in);
+
+/* Stable device radix sort of n 32-bit keys by their low `bits` bits, the
+ * sort every step runs on particle cell keys (no counterpart in the
+ * reference, which scatters unsorted with atomics).  Outputs the sorted keys
+ * and, for each sorted position, the input index.  Host buffers; used to
+ * check the sort bit-exactly against a CPU stable sort. */
+MPM_API mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, uint32_t* sorted_keys,
+                                 uint32_t* perm);
+
+/* Run nsteps steps bracketed by CUDA events recorded on the solver's own
+ * stream and return the device time in *ms (synchronizes).  Used by the
+ * benchmark; same work as mpm_solver_step. */
+MPM_API mpm_status mpm_solver_timed_step(mpm_solver* s, int32_t nsteps, float* ms);
+
+MPM_API mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out);
+
+/* Total kernel launches issued by this library in this process. */
+MPM_API mpm_status mpm_kernel_launches(uint64_t* count);
+
+/* Timing of the solver's kernels: fills ms[k] with the average device time
+ * of kernel family k over the last timed steps (see mpm_solver_profile). */
+MPM_API mpm_status mpm_solver_profile(mpm_solver* s, int32_t enable);
+MPM_API mpm_status mpm_solver_profile_read(mpm_solver* s, float* ms, int32_t* counts, int32_t nfamilies);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPM_B200_H_ */

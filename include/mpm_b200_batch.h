@@ -1,0 +1,46 @@
+/*
+ * mpm_b200_batch.h -- batched scenes on one GPU.
+ *
+ * The reference advances exactly one scene per solver object
+ * (chains::MPMSolver3D, include/mpm_solver3d.h:21-96) and has no batching;
+ * these entry points have no counterpart in the reference.  A batch advances
+ * many independent scenes of different particle counts, grids, transfers and
+ * materials with one launch sequence per step (sort, P2G, grid, G2P over the
+ * active grid blocks of every scene).  Scenes may be added and removed
+ * between steps, which the serving loop uses for continuous batching.
+ */
+#ifndef MPM_B200_BATCH_H_
+#define MPM_B200_BATCH_H_
+
+#include "mpm_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mpm_batch mpm_batch;
+
+MPM_API mpm_status mpm_batch_create(mpm_batch** out);
+MPM_API mpm_status mpm_batch_destroy(mpm_batch* b);
+/* Upload a scene (initialized on the next step); returns its id. */
+MPM_API mpm_status mpm_batch_add_scene(mpm_batch* b, const mpm_scene_desc* desc,
+                               const mpm_particles_in* particles, int32_t* scene_id);
+/* Release a scene's device state.  Waits for the batch's stream. */
+MPM_API mpm_status mpm_batch_remove_scene(mpm_batch* b, int32_t scene_id);
+/* Advance every scene nsteps steps (asynchronous). */
+MPM_API mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps);
+MPM_API mpm_status mpm_batch_synchronize(mpm_batch* b);
+/* Download a particle field of one scene in its original particle order. */
+MPM_API mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
+MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
+MPM_API mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out);
+/* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */
+MPM_API mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms);
+MPM_API mpm_status mpm_batch_profile(mpm_batch* b, int32_t enable);
+MPM_API mpm_status mpm_batch_profile_read(mpm_batch* b, float* ms, int32_t* counts, int32_t nfamilies);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPM_B200_BATCH_H_ */

@@ -1,0 +1,1195 @@
+// engine.cu -- host engine: scene batches, device memory, step orchestration,
+// and the C ABI declared in include/mpm_b200.h.
+//
+// A solver handle (mpm_solver) is an Engine holding one scene; a batch
+// (mpm_batch, include/mpm_b200_batch.h) holds many.  Every step of a batch is
+// one sequence of launches on the engine's stream:
+//   [keys] -> radix sort -> block compaction -> [stress] -> P2G -> grid -> G2P
+// where the bracketed kernels only run after uploads or split-API calls
+// (in steady state G2P produces next step's keys and stress).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+#include "../../include/mpm_b200_batch.h"
+#include "engine_host.hpp"
+
+namespace mpm {
+
+static thread_local std::string g_last_error;
+
+static mpm_status fail(mpm_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+#define CUDA_TRY(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? MPM_ERR_OOM : MPM_ERR_CUDA,                  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+        }                                                                                              \
+    } while (0)
+
+#define MPM_TRY(call)                  \
+    do {                               \
+        mpm_status s_ = (call);        \
+        if (s_ != MPM_OK) return s_;   \
+    } while (0)
+
+enum KernelFamily { KF_KEYS = 0, KF_SORT, KF_COMPACT, KF_STRESS, KF_P2G, KF_GRID, KF_G2P, KF_COUNT };
+
+static int stencilSize(int interp) {
+    return interp == MPM_INTERP_LINEAR ? 2 : (interp == MPM_INTERP_QUADRATIC_BSPLINE ? 3 : 4);
+}
+static float stencilRange(int interp) {
+    return interp == MPM_INTERP_LINEAR ? 1.0f : (interp == MPM_INTERP_QUADRATIC_BSPLINE ? 1.5f : 2.0f);
+}
+
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevMem() {
+        if (p) cudaFree(p);
+    }
+    mpm_status alloc(size_t b, const char* what) {
+        if (p && bytes >= b) return MPM_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return fail(MPM_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" + std::to_string(b) + " bytes)");
+        }
+        bytes = b;
+        return MPM_OK;
+    }
+    template <class T>
+    T* as() const {
+        return (T*)p;
+    }
+};
+
+struct SceneHost {
+    int id = -1;
+    mpm_scene_desc desc{};
+    size_t n = 0;
+    int S = 4;
+    int nb[3] = {0, 0, 0};
+    uint32_t nblocks = 0;
+    DevMem buf_f[2], buf_pid[2], buf_mat[2];
+    DevMem vstar, vold, dbg, mats;
+    int nmat = 1;
+    bool need_init = true;
+    size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
+};
+
+class Engine {
+public:
+    Engine() {}
+    ~Engine() {
+        if (stream_) cudaStreamSynchronize(stream_);
+        for (int k = 0; k < KF_COUNT; ++k) {
+            if (ev_[k][0]) cudaEventDestroy(ev_[k][0]);
+            if (ev_[k][1]) cudaEventDestroy(ev_[k][1]);
+            if (open_[k]) cudaEventDestroy(open_[k]);
+        }
+        for (auto& r : records_) {
+            cudaEventDestroy(r.e0);
+            cudaEventDestroy(r.e1);
+        }
+        for (auto e : event_pool_) cudaEventDestroy(e);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    mpm_status init() {
+        CUDA_TRY(cudaGetDevice(&device_));
+        CUDA_TRY(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_));
+        CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        MPM_TRY(err_.alloc(sizeof(uint32_t), "error flags"));
+        CUDA_TRY(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), stream_));
+        for (int k = 0; k < KF_COUNT; ++k) {
+            CUDA_TRY(cudaEventCreate(&ev_[k][0]));
+            CUDA_TRY(cudaEventCreate(&ev_[k][1]));
+        }
+        return MPM_OK;
+    }
+
+    static mpm_status validate(const mpm_scene_desc& d, const mpm_particles_in& p) {
+        for (int a = 0; a < 3; ++a)
+            if (d.resolution[a] <= 0 || d.resolution[a] > (1 << 16))
+                return fail(MPM_ERR_INVALID_ARG, "grid resolution must be in [1, 65536]");
+        if (!(d.stride > 0.f) || !std::isfinite(d.stride)) return fail(MPM_ERR_INVALID_ARG, "stride must be > 0");
+        if (!(d.dt > 0.f) || !std::isfinite(d.dt)) return fail(MPM_ERR_INVALID_ARG, "dt must be > 0");
+        if (d.interpolation < MPM_INTERP_LINEAR || d.interpolation > MPM_INTERP_CUBIC_BSPLINE)
+            return fail(MPM_ERR_INVALID_ARG, "unsupported interpolation type");
+        if (d.transfer != MPM_TRANSFER_PIC_FLIP && d.transfer != MPM_TRANSFER_APIC)
+            return fail(MPM_ERR_INVALID_ARG, "unsupported transfer");
+        if (d.transfer == MPM_TRANSFER_APIC && d.interpolation == MPM_INTERP_LINEAR)
+            return fail(MPM_ERR_INVALID_ARG,
+                        "APIC with linear interpolation has a singular inertia tensor D (reference leaves it TODO)");
+        if (d.boundary != MPM_BOUNDARY_REFERENCE && d.boundary != MPM_BOUNDARY_STICKY)
+            return fail(MPM_ERR_INVALID_ARG, "unsupported boundary mode");
+        if (d.boundary == MPM_BOUNDARY_STICKY && d.sticky_cells < 0)
+            return fail(MPM_ERR_INVALID_ARG, "sticky_cells must be >= 0");
+        if (d.volume_mode != MPM_VOLUME_GRID_ESTIMATE && d.volume_mode != MPM_VOLUME_PRESCRIBED)
+            return fail(MPM_ERR_INVALID_ARG, "unsupported volume mode");
+        if (p.n > 0 && (!p.position || !p.velocity || !p.mass))
+            return fail(MPM_ERR_INVALID_ARG, "particle position, velocity and mass arrays are required");
+        if (p.n > (size_t)0x7fffffff) return fail(MPM_ERR_INVALID_ARG, "too many particles");
+        if (d.volume_mode == MPM_VOLUME_PRESCRIBED && p.n > 0 && !p.volume)
+            return fail(MPM_ERR_INVALID_ARG, "prescribed volume mode needs a volume array");
+        if (p.nmaterials < 1 || !p.materials) return fail(MPM_ERR_INVALID_ARG, "at least one material is required");
+        if (p.nmaterials > 1 && p.n > 0 && !p.material)
+            return fail(MPM_ERR_INVALID_ARG, "per-particle material ids are required with several materials");
+        if (p.nmaterials > 65535) return fail(MPM_ERR_INVALID_ARG, "too many materials");
+        for (int i = 0; i < p.nmaterials; ++i) {
+            const mpm_material& m = p.materials[i];
+            if (m.model != MPM_MODEL_FIXED_COROTATED && m.model != MPM_MODEL_NEO_HOOKEAN)
+                return fail(MPM_ERR_INVALID_ARG, "unsupported constitutive model");
+            if (!(m.poisson_ratio < 0.5f) || !(m.poisson_ratio > -1.0f))
+                return fail(MPM_ERR_INVALID_ARG, "Poisson ratio must be in (-1, 0.5)");
+        }
+        if (p.material)
+            for (size_t i = 0; i < p.n; ++i)
+                if (p.material[i] >= p.nmaterials) return fail(MPM_ERR_INVALID_ARG, "material id out of range");
+        return MPM_OK;
+    }
+
+    mpm_status addScene(const mpm_scene_desc& d, const mpm_particles_in& p, int* out_id) {
+        MPM_TRY(validate(d, p));
+        auto sc = std::make_unique<SceneHost>();
+        sc->desc = d;
+        sc->n = p.n;
+        sc->S = stencilSize(d.interpolation);
+        for (int a = 0; a < 3; ++a) sc->nb[a] = ((d.resolution[a] + 3) >> 2) + 1;
+        sc->nblocks = (uint32_t)sc->nb[0] * sc->nb[1] * sc->nb[2];
+        const size_t cap = std::max<size_t>(p.n, 1);
+        for (int b = 0; b < 2; ++b) {
+            MPM_TRY(sc->buf_f[b].alloc(sizeof(float) * NFIELDS * cap, "particle state"));
+            MPM_TRY(sc->buf_pid[b].alloc(sizeof(uint32_t) * cap, "particle ids"));
+            MPM_TRY(sc->buf_mat[b].alloc(sizeof(uint16_t) * cap, "particle materials"));
+        }
+        const size_t nodes = sc->nodes();
+        MPM_TRY(sc->vstar.alloc(sizeof(float4) * nodes, "grid v*"));
+        CUDA_TRY(cudaMemsetAsync(sc->vstar.p, 0, sizeof(float4) * nodes, stream_));
+        if (d.transfer == MPM_TRANSFER_PIC_FLIP) {
+            MPM_TRY(sc->vold.alloc(sizeof(float4) * nodes, "grid v"));
+            CUDA_TRY(cudaMemsetAsync(sc->vold.p, 0, sizeof(float4) * nodes, stream_));
+        }
+        // Materials: Lame parameters as in src/material_point3d.cu:25-26.
+        std::vector<MaterialDev> mats(p.nmaterials);
+        for (int i = 0; i < p.nmaterials; ++i) {
+            const mpm_material& m = p.materials[i];
+            double E = m.youngs_modulus, nu = m.poisson_ratio;
+            mats[i].mu0 = (float)(E / (2.0 * (1.0 + nu)));
+            mats[i].lambda0 = (float)((double)(m.youngs_modulus * m.poisson_ratio) / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+            mats[i].xi = m.hardening;
+            mats[i].theta_c = m.critical_compression;
+            mats[i].theta_s = m.critical_stretch;
+            mats[i].model = m.model;
+        }
+        sc->nmat = p.nmaterials;
+        MPM_TRY(sc->mats.alloc(sizeof(MaterialDev) * mats.size(), "materials"));
+        CUDA_TRY(cudaMemcpyAsync(sc->mats.p, mats.data(), sizeof(MaterialDev) * mats.size(), cudaMemcpyHostToDevice,
+                                 stream_));
+        // Particle state in the caller's order (Fe = Fp = I, B = 0).
+        if (p.n > 0) {
+            std::vector<float> host((size_t)NFIELDS * p.n, 0.f);
+            for (size_t i = 0; i < p.n; ++i) {
+                for (int a = 0; a < 3; ++a) {
+                    host[(F_X + a) * p.n + i] = p.position[3 * i + a];
+                    host[(F_V + a) * p.n + i] = p.velocity[3 * i + a];
+                }
+                for (int k = 0; k < 9; k += 4) {
+                    host[(F_FE + k) * p.n + i] = 1.f;
+                    host[(F_FP + k) * p.n + i] = 1.f;
+                }
+                host[F_MASS * p.n + i] = p.mass[i];
+                host[F_VOL * p.n + i] = (d.volume_mode == MPM_VOLUME_PRESCRIBED) ? p.volume[i] : 0.f;
+            }
+            std::vector<uint32_t> pid(p.n);
+            for (size_t i = 0; i < p.n; ++i) pid[i] = (uint32_t)i;
+            const int b = parity_;
+            CUDA_TRY(cudaMemcpy(sc->buf_f[b].p, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice));
+            CUDA_TRY(cudaMemcpy(sc->buf_pid[b].p, pid.data(), sizeof(uint32_t) * p.n, cudaMemcpyHostToDevice));
+            if (p.material)
+                CUDA_TRY(cudaMemcpy(sc->buf_mat[b].p, p.material, sizeof(uint16_t) * p.n, cudaMemcpyHostToDevice));
+            else
+                CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * p.n, stream_));
+        }
+        sc->need_init = true;
+        sc->id = next_id_++;
+        *out_id = sc->id;
+        scenes_.push_back(std::move(sc));
+        dirty_ = true;
+        keys_valid_ = false;
+        stress_valid_ = false;
+        sorted_valid_ = false;
+        return MPM_OK;
+    }
+
+    mpm_status removeScene(int id) {
+        for (size_t i = 0; i < scenes_.size(); ++i)
+            if (scenes_[i]->id == id) {
+                CUDA_TRY(cudaStreamSynchronize(stream_));
+                scenes_.erase(scenes_.begin() + i);
+                dirty_ = true;
+                keys_valid_ = false;
+                sorted_valid_ = false;
+                return MPM_OK;
+            }
+        return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+    }
+
+    SceneHost* scene(int id) {
+        for (auto& s : scenes_)
+            if (s->id == id) return s.get();
+        return nullptr;
+    }
+    int sceneIndex(int id) const {
+        for (size_t i = 0; i < scenes_.size(); ++i)
+            if (scenes_[i]->id == id) return (int)i;
+        return -1;
+    }
+
+    // Rebuild the device scene table and the batch-wide scratch after the
+    // set of scenes changed.
+    mpm_status rebuild() {
+        if (!dirty_) return MPM_OK;
+        const int ns = (int)scenes_.size();
+        host_scenes_.assign(ns, SceneDev{});
+        std::vector<uint32_t> sbb(ns + 1, 0);
+        size_t ntot = 0;
+        uint64_t tb = 0;
+        max_nodes_ = 0;
+        max_n_ = 0;
+        for (int i = 0; i < ns; ++i) {
+            SceneHost& s = *scenes_[i];
+            SceneDev& d = host_scenes_[i];
+            for (int a = 0; a < 3; ++a) {
+                d.origin[a] = s.desc.origin[a];
+                d.res[a] = s.desc.resolution[a];
+                d.nb[a] = s.nb[a];
+                d.target[a] = s.desc.origin[a] + s.desc.stride * (float)s.desc.resolution[a];
+            }
+            d.h = s.desc.stride;
+            d.inv_h = 1.0f / s.desc.stride;
+            d.range = stencilRange(s.desc.interpolation);
+            d.block_base = (uint32_t)tb;
+            d.nblocks = s.nblocks;
+            sbb[i] = (uint32_t)tb;
+            tb += (uint64_t)s.nblocks + 1;  // + the scene's outside block
+            d.key_offset = (uint32_t)ntot;
+            d.n = (uint32_t)s.n;
+            d.cap = (uint32_t)std::max<size_t>(s.n, 1);
+            ntot += s.n;
+            d.dt = s.desc.dt;
+            d.gravity = s.desc.gravity;
+            d.friction = s.desc.friction;
+            d.blend = s.desc.blend;
+            d.dinv = 0.f;
+            if (s.desc.transfer == MPM_TRANSFER_APIC) {
+                // D = k h^2 I, k = 1/3 cubic, 1/4 quadratic (src/apic_mpm_solver3d.cu:151-157)
+                float k = s.desc.interpolation == MPM_INTERP_CUBIC_BSPLINE ? (float)(1 / 3.0) : (float)(1 / 4.0);
+                d.dinv = 1.0f / (k * s.desc.stride * s.desc.stride);
+            }
+            d.transfer = s.desc.transfer;
+            d.interp = s.desc.interpolation;
+            d.S = s.S;
+            d.boundary = s.desc.boundary;
+            d.sticky = s.desc.sticky_cells;
+            d.pcoll = s.desc.particles_collision;
+            d.nmat = s.nmat;
+            for (int b = 0; b < 2; ++b) {
+                d.buf[b].f = s.buf_f[b].as<float>();
+                d.buf[b].pid = s.buf_pid[b].as<uint32_t>();
+                d.buf[b].mat = s.buf_mat[b].as<uint16_t>();
+            }
+            d.vstar = s.vstar.as<float4>();
+            d.vold = s.vold.as<float4>();
+            d.mats = s.mats.as<MaterialDev>();
+            d.dbg = s.dbg.as<float>();
+            max_nodes_ = std::max(max_nodes_, s.nodes());
+            max_n_ = std::max(max_n_, s.n);
+        }
+        sbb[ns] = (uint32_t)tb;
+        if (tb * 64 > 0xffffffffull) return fail(MPM_ERR_UNSUPPORTED, "batch grid too large for 32-bit cell keys");
+        if (ntot > 0x7fffffffull) return fail(MPM_ERR_UNSUPPORTED, "batch has too many particles");
+        ntot_ = ntot;
+        total_blocks_ = (uint32_t)tb;
+        key_bits_ = 1;
+        while (((uint64_t)1 << key_bits_) < tb * 64) ++key_bits_;
+        // batch scratch
+        const size_t nk = std::max<size_t>(ntot, 1);
+        for (int k = 0; k < 2; ++k) {
+            MPM_TRY(keys_[k].alloc(sizeof(uint32_t) * nk, "keys"));
+            MPM_TRY(vals_[k].alloc(sizeof(uint32_t) * nk, "values"));
+        }
+        const size_t tiles = radixTiles(nk);
+        MPM_TRY(hist_.alloc(sizeof(uint32_t) * 256 * tiles, "radix histogram"));
+        MPM_TRY(scan32_.alloc(sizeof(uint32_t) * (scanScratchElems(256 * tiles) + 1), "scan scratch"));
+        MPM_TRY(block_count_.alloc(sizeof(uint32_t) * tb, "block counts"));
+        CUDA_TRY(cudaMemsetAsync(block_count_.p, 0, sizeof(uint32_t) * tb, stream_));
+        MPM_TRY(packed_.alloc(sizeof(unsigned long long) * tb, "block scan"));
+        MPM_TRY(scanned_.alloc(sizeof(unsigned long long) * tb, "block scan"));
+        MPM_TRY(scan64_.alloc(sizeof(unsigned long long) * (scanScratchElems(tb) + 1), "block scan scratch"));
+        MPM_TRY(total64_.alloc(sizeof(unsigned long long), "block scan total"));
+        MPM_TRY(sbb_.alloc(sizeof(uint32_t) * (ns + 1), "scene block bases"));
+        CUDA_TRY(cudaMemcpyAsync(sbb_.p, sbb.data(), sizeof(uint32_t) * (ns + 1), cudaMemcpyHostToDevice, stream_));
+        max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk));
+        MPM_TRY(active_.alloc(sizeof(BlockItem) * max_active_, "active blocks"));
+        MPM_TRY(outside_.alloc(sizeof(BlockItem) * std::max(ns, 1), "outside blocks"));
+        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 4, "counters"));
+        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 4, stream_));
+        MPM_TRY(block_slot_.alloc(sizeof(int32_t) * tb, "block slots"));
+        int maxS = 2;
+        for (auto& s : scenes_) maxS = std::max(maxS, s->S);
+        tile_stride_ = (size_t)7 * tileNodes(maxS);
+        MPM_TRY(tiles_.alloc(sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
+        MPM_TRY(scenes_dev_.alloc(sizeof(SceneDev) * std::max(ns, 1), "scene table"));
+        CUDA_TRY(cudaMemcpyAsync(scenes_dev_.p, host_scenes_.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice,
+                                 stream_));
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        kcur_ = 0;
+        dirty_ = false;
+        keys_valid_ = false;
+        sorted_valid_ = false;
+        return MPM_OK;
+    }
+
+    mpm_status uploadSceneTable() {
+        CUDA_TRY(cudaMemcpyAsync(scenes_dev_.p, host_scenes_.data(), sizeof(SceneDev) * host_scenes_.size(),
+                                 cudaMemcpyHostToDevice, stream_));
+        return MPM_OK;
+    }
+
+    LaunchCtx ctx() const {
+        LaunchCtx c;
+        c.scenes = scenes_dev_.as<SceneDev>();
+        c.nscenes = (int)scenes_.size();
+        c.stream = stream_;
+        c.num_sms = num_sms_;
+        c.particle_blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((max_n_ + kThreads - 1) / kThreads,
+                                                                           (size_t)num_sms_ * 16));
+        c.node_blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((max_nodes_ + kThreads - 1) / kThreads,
+                                                                       (size_t)num_sms_ * 16));
+        c.persistent_blocks = (unsigned)std::max<size_t>(1, std::min<size_t>(max_active_ + 64, (size_t)num_sms_ * 4));
+        return c;
+    }
+
+    StepArgs args(const uint32_t* sorted_keys, const uint32_t* perm, uint32_t* next_keys) const {
+        StepArgs a;
+        a.scenes = scenes_dev_.as<SceneDev>();
+        a.nscenes = (int)scenes_.size();
+        a.parity = parity_;
+        a.sorted_keys = sorted_keys;
+        a.perm = perm;
+        a.active = active_.as<BlockItem>();
+        a.counters = counters_.as<uint32_t>();
+        a.outside = outside_.as<BlockItem>();
+        a.block_slot = block_slot_.as<int32_t>();
+        a.tiles = tiles_.as<float>();
+        a.tile_stride = (uint32_t)tile_stride_;
+        a.next_keys = next_keys;
+        a.block_count = block_count_.as<uint32_t>();
+        a.err = err_.as<uint32_t>();
+        a.stats = counters_.as<uint32_t>();
+        return a;
+    }
+
+    BlockBuffers blockBuffers() const {
+        BlockBuffers bb;
+        bb.block_count = block_count_.as<uint32_t>();
+        bb.packed = packed_.as<unsigned long long>();
+        bb.scanned = scanned_.as<unsigned long long>();
+        bb.scan_partials64 = scan64_.as<unsigned long long>();
+        bb.total64 = total64_.as<unsigned long long>();
+        bb.scene_block_base = sbb_.as<uint32_t>();
+        bb.active = active_.as<BlockItem>();
+        bb.outside = outside_.as<BlockItem>();
+        bb.counters = counters_.as<uint32_t>();
+        bb.block_slot = block_slot_.as<int32_t>();
+        return bb;
+    }
+
+    // Profiling: an event pair per kernel family launch, recorded on the
+    // engine's stream without synchronizing; resolved in accumulateProfile().
+    cudaEvent_t takeEvent() {
+        cudaEvent_t e = nullptr;
+        if (!event_pool_.empty()) {
+            e = event_pool_.back();
+            event_pool_.pop_back();
+        } else if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            e = nullptr;
+        }
+        return e;
+    }
+    void mark(int fam, int which) {
+        if (!profiling_) return;
+        if (which == 0) {
+            open_[fam] = takeEvent();
+            if (open_[fam]) cudaEventRecord(open_[fam], stream_);
+        } else if (open_[fam]) {
+            cudaEvent_t e1 = takeEvent();
+            if (e1) {
+                cudaEventRecord(e1, stream_);
+                records_.push_back({fam, open_[fam], e1});
+            } else {
+                event_pool_.push_back(open_[fam]);
+            }
+            open_[fam] = nullptr;
+        }
+    }
+    void collect(int) {}
+
+    // Keys of the live order (if stale) + sort + compaction.
+    mpm_status sortLive() {
+        if (!keys_valid_) {
+            mark(KF_KEYS, 0);
+            CUDA_TRY(cudaMemsetAsync(block_count_.p, 0, sizeof(uint32_t) * total_blocks_, stream_));
+            launchKeys(ctx(), parity_, keys_[kcur_].as<uint32_t>(), block_count_.as<uint32_t>(), err_.as<uint32_t>());
+            mark(KF_KEYS, 1);
+            collect(KF_KEYS);
+            keys_valid_ = true;
+        }
+        bool inB = false;
+        mark(KF_SORT, 0);
+        CUDA_TRY(radixSortPairs(keys_[kcur_].as<uint32_t>(), vals_[kcur_].as<uint32_t>(),
+                                keys_[1 - kcur_].as<uint32_t>(), vals_[1 - kcur_].as<uint32_t>(), ntot_, key_bits_,
+                                hist_.as<uint32_t>(), scan32_.as<uint32_t>(), &inB, stream_));
+        mark(KF_SORT, 1);
+        collect(KF_SORT);
+        sorted_ = inB ? 1 - kcur_ : kcur_;
+        mark(KF_COMPACT, 0);
+        launchCompact(ctx(), blockBuffers(), total_blocks_);
+        mark(KF_COMPACT, 1);
+        collect(KF_COMPACT);
+        CUDA_TRY(cudaGetLastError());
+        sorted_valid_ = true;
+        return MPM_OK;
+    }
+
+    struct Combo {
+        int S;
+        int transfer;
+    };
+    std::vector<Combo> combos() const {
+        std::vector<Combo> c;
+        for (auto& s : scenes_) {
+            bool found = false;
+            for (auto& e : c)
+                if (e.S == s->S && e.transfer == s->desc.transfer) found = true;
+            if (!found) c.push_back({s->S, s->desc.transfer});
+        }
+        return c;
+    }
+    std::vector<int> stencilSizes() const {
+        std::vector<int> v;
+        for (auto& s : scenes_)
+            if (std::find(v.begin(), v.end(), s->S) == v.end()) v.push_back(s->S);
+        return v;
+    }
+
+    mpm_status ensureReady() {
+        if (scenes_.empty()) return fail(MPM_ERR_INVALID_ARG, "no scenes");
+        MPM_TRY(rebuild());
+        bool need = false;
+        for (auto& s : scenes_) need |= s->need_init;
+        if (need) MPM_TRY(initialize(false));
+        return MPM_OK;
+    }
+
+    // initialize(): V0 from the grid mass (src/mpm_solver3d.cu:131-223).
+    mpm_status initialize(bool all) {
+        MPM_TRY(rebuild());
+        bool any_estimate = false;
+        for (auto& s : scenes_)
+            if ((all || s->need_init) && s->desc.volume_mode == MPM_VOLUME_GRID_ESTIMATE) any_estimate = true;
+        if (any_estimate) {
+            MPM_TRY(sortLive());
+            StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
+            LaunchCtx c = ctx();
+            for (int S : stencilSizes()) {
+                launchP2G(c, a, S, MODE_MASS, -1);
+                launchGrid(c, a, S, MODE_MASS, -1);
+            }
+            // The volume kernel runs per scene so that only scenes being
+            // initialized get a new V0.
+            for (size_t i = 0; i < scenes_.size(); ++i) {
+                SceneHost& s = *scenes_[i];
+                if (!(all || s.need_init) || s.desc.volume_mode != MPM_VOLUME_GRID_ESTIMATE) continue;
+                LaunchCtx one = c;
+                one.scenes = scenes_dev_.as<SceneDev>() + i;
+                one.nscenes = 1;
+                launchVolume(one, parity_, s.S);
+            }
+            CUDA_TRY(cudaGetLastError());
+            keys_valid_ = false;  // block counts were consumed by the compaction
+        }
+        for (auto& s : scenes_) s->need_init = false;
+        stress_valid_ = false;
+        return MPM_OK;
+    }
+
+    // One fused simulateOneStep over every scene of the batch.
+    mpm_status stepOnce() {
+        MPM_TRY(sortLive());
+        if (!stress_valid_) {
+            mark(KF_STRESS, 0);
+            launchStress(ctx(), parity_);
+            mark(KF_STRESS, 1);
+            collect(KF_STRESS);
+            stress_valid_ = true;
+        }
+        const int next = 1 - sorted_;
+        StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
+        LaunchCtx c = ctx();
+        auto cs = combos();
+        mark(KF_P2G, 0);
+        for (auto& k : cs)
+            launchP2G(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+        mark(KF_P2G, 1);
+        collect(KF_P2G);
+        mark(KF_GRID, 0);
+        for (auto& k : cs)
+            launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+        mark(KF_GRID, 1);
+        collect(KF_GRID);
+        mark(KF_G2P, 0);
+        for (auto& k : cs) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, true);
+        mark(KF_G2P, 1);
+        collect(KF_G2P);
+        CUDA_TRY(cudaGetLastError());
+        parity_ ^= 1;
+        kcur_ = next;
+        keys_valid_ = true;   // G2P wrote next step's keys and block counts
+        stress_valid_ = true; // and next step's stress
+        sorted_valid_ = false;
+        return MPM_OK;
+    }
+
+    mpm_status step(int n) {
+        if (n < 0) return fail(MPM_ERR_INVALID_ARG, "nsteps must be >= 0");
+        MPM_TRY(ensureReady());
+        for (int i = 0; i < n; ++i) MPM_TRY(stepOnce());
+        return MPM_OK;
+    }
+
+    mpm_status timedStep(int n, float* ms) {
+        if (!ms) return fail(MPM_ERR_INVALID_ARG, "null output");
+        MPM_TRY(ensureReady());
+        CUDA_TRY(cudaEventRecord(ev_[0][0], stream_));
+        for (int i = 0; i < n; ++i) MPM_TRY(stepOnce());
+        CUDA_TRY(cudaEventRecord(ev_[0][1], stream_));
+        CUDA_TRY(cudaEventSynchronize(ev_[0][1]));
+        CUDA_TRY(cudaEventElapsedTime(ms, ev_[0][0], ev_[0][1]));
+        return MPM_OK;
+    }
+
+    mpm_status accumulateProfile() {
+        if (records_.empty()) return MPM_OK;
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        for (auto& r : records_) {
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, r.e0, r.e1));
+            prof_ms_[r.fam] += ms;
+            prof_cnt_[r.fam] += 1;
+            event_pool_.push_back(r.e0);
+            event_pool_.push_back(r.e1);
+        }
+        records_.clear();
+        return MPM_OK;
+    }
+
+    mpm_status stats(mpm_step_stats* out) {
+        if (!out) return fail(MPM_ERR_INVALID_ARG, "null output");
+        *out = mpm_step_stats{};
+        if (dirty_ || !counters_.p) return MPM_OK;
+        uint32_t c[4] = {0, 0, 0, 0};
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        CUDA_TRY(cudaMemcpy(c, counters_.p, sizeof(c), cudaMemcpyDeviceToHost));
+        out->active_blocks = c[0];
+        out->outside_blocks = c[1];
+        out->active_nodes = c[2];
+        return MPM_OK;
+    }
+
+    mpm_status synchronize() {
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        uint32_t e = 0;
+        CUDA_TRY(cudaMemcpy(&e, err_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (e) {
+            CUDA_TRY(cudaMemset(err_.p, 0, sizeof(uint32_t)));
+            if (e & ERR_NONFINITE) return fail(MPM_ERR_NUMERIC, "non-finite particle position detected on the device");
+            return fail(MPM_ERR_CUDA, "device error flag " + std::to_string(e));
+        }
+        return MPM_OK;
+    }
+
+    // ---- split API --------------------------------------------------------
+    mpm_status ensureDbg() {
+        bool changed = false;
+        for (auto& s : scenes_)
+            if (!s->dbg.p) {
+                MPM_TRY(s->dbg.alloc(sizeof(float) * 10 * s->nodes(), "dense debug grid"));
+                CUDA_TRY(cudaMemsetAsync(s->dbg.p, 0, sizeof(float) * 10 * s->nodes(), stream_));
+                changed = true;
+            }
+        if (changed) {
+            for (size_t i = 0; i < scenes_.size(); ++i) host_scenes_[i].dbg = scenes_[i]->dbg.as<float>();
+            MPM_TRY(uploadSceneTable());
+        }
+        return MPM_OK;
+    }
+    mpm_status resetGrid() {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        for (auto& s : scenes_) CUDA_TRY(cudaMemsetAsync(s->dbg.p, 0, sizeof(float) * 10 * s->nodes(), stream_));
+        return MPM_OK;
+    }
+    mpm_status particlesToGrid() {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        MPM_TRY(sortLive());
+        if (!stress_valid_) {
+            launchStress(ctx(), parity_);
+            stress_valid_ = true;
+        }
+        StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
+        LaunchCtx c = ctx();
+        for (int S : stencilSizes()) {
+            launchP2G(c, a, S, MODE_SPLIT, -1);
+            launchGrid(c, a, S, MODE_SPLIT, -1);
+        }
+        CUDA_TRY(cudaGetLastError());
+        keys_valid_ = false;
+        return MPM_OK;
+    }
+    mpm_status gravity() {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        launchDenseGravity(ctx());
+        CUDA_TRY(cudaGetLastError());
+        return MPM_OK;
+    }
+    mpm_status updateGridVelocities(float dt) {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        launchDenseUpdate(ctx(), dt);
+        CUDA_TRY(cudaGetLastError());
+        return MPM_OK;
+    }
+    mpm_status gridCollision(float dt) {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        launchDenseCollision(ctx(), dt);
+        CUDA_TRY(cudaGetLastError());
+        return MPM_OK;
+    }
+    mpm_status gridToParticles(float dt, float blend, bool override_blend) {
+        MPM_TRY(ensureReady());
+        MPM_TRY(ensureDbg());
+        if (!sorted_valid_) MPM_TRY(sortLive());
+        if (!stress_valid_) {
+            launchStress(ctx(), parity_);
+            stress_valid_ = true;
+        }
+        launchDensePack(ctx());
+        std::vector<SceneDev> saved = host_scenes_;
+        for (auto& d : host_scenes_) {
+            d.dt = dt;
+            if (override_blend) d.blend = blend;
+        }
+        MPM_TRY(uploadSceneTable());
+        StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
+        LaunchCtx c = ctx();
+        for (auto& k : combos()) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, false);
+        CUDA_TRY(cudaGetLastError());
+        host_scenes_ = saved;
+        MPM_TRY(uploadSceneTable());
+        parity_ ^= 1;
+        keys_valid_ = false;
+        sorted_valid_ = false;
+        stress_valid_ = true;
+        return MPM_OK;
+    }
+    mpm_status particlesCollision(float dt) {
+        MPM_TRY(ensureReady());
+        launchParticlesCollision(ctx(), parity_, dt);
+        CUDA_TRY(cudaGetLastError());
+        return MPM_OK;
+    }
+    mpm_status advect(float dt) {
+        MPM_TRY(ensureReady());
+        launchAdvect(ctx(), parity_, dt);
+        CUDA_TRY(cudaGetLastError());
+        keys_valid_ = false;
+        sorted_valid_ = false;
+        return MPM_OK;
+    }
+
+    // ---- data movement ----------------------------------------------------
+    static int fieldInfo(int field, int* base, int* comps, int* mode) {
+        *mode = 0;
+        switch (field) {
+            case MPM_FIELD_POSITION: *base = F_X; *comps = 3; return 3;
+            case MPM_FIELD_VELOCITY: *base = F_V; *comps = 3; return 3;
+            case MPM_FIELD_FE: *base = F_FE; *comps = 9; return 9;
+            case MPM_FIELD_FP: *base = F_FP; *comps = 9; return 9;
+            case MPM_FIELD_B: *base = F_B; *comps = 9; return 9;
+            case MPM_FIELD_VOLUME0: *base = F_VOL; *comps = 1; return 1;
+            case MPM_FIELD_MASS: *base = F_MASS; *comps = 1; return 1;
+            case MPM_FIELD_POSITION4: *base = F_X; *comps = 4; *mode = 1; return 4;
+            case MPM_FIELD_DET_FE: *base = F_FE; *comps = 1; *mode = 2; return 1;
+            case MPM_FIELD_DET_FP: *base = F_FP; *comps = 1; *mode = 2; return 1;
+            default: return 0;
+        }
+    }
+
+    mpm_status download(int id, int field, float* host, bool sync = true) {
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!host) return fail(MPM_ERR_INVALID_ARG, "null output pointer");
+        int base, comps, mode;
+        int per = fieldInfo(field, &base, &comps, &mode);
+        if (!per) return fail(MPM_ERR_INVALID_ARG, "unknown particle field");
+        SceneHost& s = *scenes_[idx];
+        if (field == MPM_FIELD_B && s.desc.transfer != MPM_TRANSFER_APIC)
+            return fail(MPM_ERR_INVALID_ARG, "B is only defined for APIC scenes");
+        if (s.n == 0) return MPM_OK;
+        const size_t bytes = sizeof(float) * per * s.n;
+        MPM_TRY(tmp_.alloc(bytes, "download buffer"));
+        LaunchCtx c = ctx();
+        launchGatherField(c, idx, parity_, base, comps, mode, tmp_.as<float>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(host, tmp_.p, bytes, cudaMemcpyDeviceToHost, stream_));
+        if (sync) return synchronize();
+        return MPM_OK;
+    }
+
+    mpm_status upload(int id, int field, const float* host) {
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!host) return fail(MPM_ERR_INVALID_ARG, "null input pointer");
+        int base, comps, mode;
+        int per = fieldInfo(field, &base, &comps, &mode);
+        if (!per || mode != 0 || field == MPM_FIELD_MASS)
+            return fail(MPM_ERR_INVALID_ARG, "field cannot be uploaded");
+        SceneHost& s = *scenes_[idx];
+        if (s.n == 0) return MPM_OK;
+        const size_t bytes = sizeof(float) * per * s.n;
+        MPM_TRY(tmp_.alloc(bytes, "upload buffer"));
+        CUDA_TRY(cudaMemcpyAsync(tmp_.p, host, bytes, cudaMemcpyHostToDevice, stream_));
+        launchScatterField(ctx(), idx, parity_, base, comps, tmp_.as<float>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        stress_valid_ = false;
+        if (field == MPM_FIELD_POSITION) {
+            keys_valid_ = false;
+            sorted_valid_ = false;
+        }
+        return MPM_OK;
+    }
+
+    mpm_status downloadGrid(int id, int field, float* host) {
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        SceneHost& s = *scenes_[idx];
+        if (!s.dbg.p) return fail(MPM_ERR_INVALID_ARG, "the dense grid exists only after split-API grid calls");
+        const size_t nodes = s.nodes();
+        std::vector<float> planes;
+        int first, comps;
+        switch (field) {
+            case MPM_GRID_MASS: first = 0; comps = 1; break;
+            case MPM_GRID_VELOCITY: first = 1; comps = 3; break;
+            case MPM_GRID_FORCE: first = 4; comps = 3; break;
+            case MPM_GRID_VELOCITY_STAR: first = 7; comps = 3; break;
+            default: return fail(MPM_ERR_INVALID_ARG, "unknown grid field");
+        }
+        planes.resize(nodes * comps);
+        CUDA_TRY(cudaMemcpyAsync(planes.data(), s.dbg.as<float>() + first * nodes, sizeof(float) * nodes * comps,
+                                 cudaMemcpyDeviceToHost, stream_));
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        for (size_t i = 0; i < nodes; ++i)
+            for (int c = 0; c < comps; ++c) host[comps * i + c] = planes[c * nodes + i];
+        return MPM_OK;
+    }
+
+    mpm_status setParticlesCollision(int id, int enable) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        scenes_[idx]->desc.particles_collision = enable ? 1 : 0;
+        if (!dirty_) {
+            host_scenes_[idx].pcoll = enable ? 1 : 0;
+            MPM_TRY(uploadSceneTable());
+        }
+        return MPM_OK;
+    }
+
+    mpm_status profile(int enable) {
+        MPM_TRY(accumulateProfile());
+        if (enable) {
+            for (int k = 0; k < KF_COUNT; ++k) {
+                prof_ms_[k] = 0;
+                prof_cnt_[k] = 0;
+            }
+        }
+        profiling_ = enable != 0;
+        return MPM_OK;
+    }
+    mpm_status profileRead(float* ms, int32_t* counts, int nf) {
+        MPM_TRY(accumulateProfile());
+        for (int k = 0; k < nf && k < KF_COUNT; ++k) {
+            if (ms) ms[k] = prof_cnt_[k] ? (float)(prof_ms_[k] / prof_cnt_[k]) : 0.f;
+            if (counts) counts[k] = prof_cnt_[k];
+        }
+        return MPM_OK;
+    }
+
+    size_t numScenes() const { return scenes_.size(); }
+    size_t totalParticles() const {
+        size_t n = 0;
+        for (auto& s : scenes_) n += s->n;
+        return n;
+    }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    int device_ = 0, num_sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    std::vector<std::unique_ptr<SceneHost>> scenes_;
+    std::vector<SceneDev> host_scenes_;
+    int next_id_ = 0;
+    bool dirty_ = true, keys_valid_ = false, stress_valid_ = false, sorted_valid_ = false;
+    int parity_ = 0, kcur_ = 0, sorted_ = 0;
+    size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
+    uint32_t total_blocks_ = 0;
+    int key_bits_ = 1;
+    DevMem keys_[2], vals_[2], hist_, scan32_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
+        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
+    bool profiling_ = false;
+    cudaEvent_t ev_[KF_COUNT][2] = {};
+    struct Record {
+        int fam;
+        cudaEvent_t e0, e1;
+    };
+    std::vector<Record> records_;
+    std::vector<cudaEvent_t> event_pool_;
+    cudaEvent_t open_[KF_COUNT] = {};
+    double prof_ms_[KF_COUNT] = {};
+    int prof_cnt_[KF_COUNT] = {};
+};
+
+}  // namespace mpm
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using mpm::Engine;
+
+struct mpm_solver {
+    Engine eng;
+    int scene = -1;
+};
+
+struct mpm_batch {
+    Engine eng;
+};
+
+#define GUARD(expr)                                                     \
+    try {                                                               \
+        return (expr);                                                  \
+    } catch (const std::bad_alloc&) {                                   \
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");        \
+    } catch (const std::exception& e) {                                 \
+        return mpm::fail(MPM_ERR_CUDA, e.what());                       \
+    }
+
+extern "C" {
+
+int32_t mpm_abi_version(void) { return MPM_B200_ABI_VERSION; }
+
+const char* mpm_last_error_string(void) { return mpm::g_last_error.c_str(); }
+
+mpm_status mpm_device_count(int32_t* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    if (count) *count = n;
+    return MPM_OK;
+}
+
+static mpm_status check(const mpm_solver* s) {
+    if (!s) return mpm::fail(MPM_ERR_INVALID_ARG, "null solver handle");
+    return MPM_OK;
+}
+
+mpm_status mpm_solver_create(const mpm_scene_desc* desc, const mpm_particles_in* particles, mpm_solver** out) {
+    if (!desc || !particles || !out) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    try {
+        mpm_status st = Engine::validate(*desc, *particles);
+        if (st != MPM_OK) return st;
+        std::unique_ptr<mpm_solver> s(new mpm_solver);
+        st = s->eng.init();
+        if (st != MPM_OK) return st;
+        st = s->eng.addScene(*desc, *particles, &s->scene);
+        if (st != MPM_OK) return st;
+        st = s->eng.ensureReady();
+        if (st != MPM_OK) return st;
+        st = s->eng.synchronize();
+        if (st != MPM_OK) return st;
+        *out = s.release();
+        return MPM_OK;
+    } catch (const std::bad_alloc&) {
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+}
+
+mpm_status mpm_solver_destroy(mpm_solver* s) {
+    if (!s) return MPM_OK;
+    cudaStreamSynchronize(s->eng.stream());
+    delete s;
+    return MPM_OK;
+}
+
+mpm_status mpm_solver_step(mpm_solver* s, int32_t nsteps) {
+    MPM_TRY(check(s));
+    GUARD(s->eng.step(nsteps));
+}
+mpm_status mpm_solver_synchronize(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.synchronize();
+}
+mpm_status mpm_solver_initialize(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.initialize(true);
+}
+mpm_status mpm_solver_reset_grid(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.resetGrid();
+}
+mpm_status mpm_solver_particles_to_grid(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.particlesToGrid();
+}
+mpm_status mpm_solver_compute_external_forces(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.gravity();
+}
+mpm_status mpm_solver_compute_gravity_forces(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.gravity();
+}
+mpm_status mpm_solver_update_grid_velocities(mpm_solver* s, float dt) {
+    MPM_TRY(check(s));
+    return s->eng.updateGridVelocities(dt);
+}
+mpm_status mpm_solver_grid_collision(mpm_solver* s, float dt) {
+    MPM_TRY(check(s));
+    return s->eng.gridCollision(dt);
+}
+mpm_status mpm_solver_solve_linear_system(mpm_solver* s, float dt) {
+    (void)dt;
+    MPM_TRY(check(s));
+    return MPM_OK;  // the reference's explicit solver leaves this a TODO (src/mpm_solver3d.cu:312-314)
+}
+mpm_status mpm_solver_grid_to_particles(mpm_solver* s, float dt, float blend) {
+    MPM_TRY(check(s));
+    return s->eng.gridToParticles(dt, blend, true);
+}
+mpm_status mpm_solver_particles_collision(mpm_solver* s, float dt) {
+    MPM_TRY(check(s));
+    return s->eng.particlesCollision(dt);
+}
+mpm_status mpm_solver_advect_particles(mpm_solver* s, float dt) {
+    MPM_TRY(check(s));
+    return s->eng.advect(dt);
+}
+mpm_status mpm_solver_set_particles_collision(mpm_solver* s, int32_t enable) {
+    MPM_TRY(check(s));
+    return s->eng.setParticlesCollision(s->scene, enable);
+}
+mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32_t* enable) {
+    MPM_TRY(check(s));
+    if (!enable) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
+    *enable = const_cast<mpm_solver*>(s)->eng.scene(s->scene)->desc.particles_collision;
+    return MPM_OK;
+}
+mpm_status mpm_solver_num_particles(const mpm_solver* s, size_t* n) {
+    MPM_TRY(check(s));
+    if (!n) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
+    *n = const_cast<mpm_solver*>(s)->eng.scene(s->scene)->n;
+    return MPM_OK;
+}
+mpm_status mpm_solver_get_desc(const mpm_solver* s, mpm_scene_desc* desc) {
+    MPM_TRY(check(s));
+    if (!desc) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
+    *desc = const_cast<mpm_solver*>(s)->eng.scene(s->scene)->desc;
+    return MPM_OK;
+}
+mpm_status mpm_solver_download(mpm_solver* s, int32_t field, float* host_out) {
+    MPM_TRY(check(s));
+    return s->eng.download(s->scene, field, host_out);
+}
+mpm_status mpm_solver_download_grid(mpm_solver* s, int32_t field, float* host_out) {
+    MPM_TRY(check(s));
+    if (!host_out) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
+    return s->eng.downloadGrid(s->scene, field, host_out);
+}
+mpm_status mpm_solver_upload(mpm_solver* s, int32_t field, const float* host_in) {
+    MPM_TRY(check(s));
+    return s->eng.upload(s->scene, field, host_in);
+}
+mpm_status mpm_solver_timed_step(mpm_solver* s, int32_t nsteps, float* ms) {
+    MPM_TRY(check(s));
+    GUARD(s->eng.timedStep(nsteps, ms));
+}
+mpm_status mpm_set_device(int32_t device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return mpm::fail(MPM_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    return MPM_OK;
+}
+mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out) {
+    MPM_TRY(check(s));
+    return s->eng.stats(out);
+}
+mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.stats(out);
+}
+mpm_status mpm_kernel_launches(uint64_t* count) {
+    if (!count) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
+    *count = mpm::kernelLaunches();
+    return MPM_OK;
+}
+mpm_status mpm_solver_profile(mpm_solver* s, int32_t enable) {
+    MPM_TRY(check(s));
+    return s->eng.profile(enable);
+}
+mpm_status mpm_solver_profile_read(mpm_solver* s, float* ms, int32_t* counts, int32_t nfamilies) {
+    MPM_TRY(check(s));
+    return s->eng.profileRead(ms, counts, nfamilies);
+}
+
+mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, uint32_t* sorted_keys, uint32_t* perm) {
+    if ((!keys || !sorted_keys || !perm) && n > 0) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    if (bits < 1 || bits > 32) return mpm::fail(MPM_ERR_INVALID_ARG, "bits must be in [1, 32]");
+    if (n == 0) return MPM_OK;
+    if (n > 0x7fffffffull) return mpm::fail(MPM_ERR_INVALID_ARG, "too many keys");
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return mpm::fail(MPM_ERR_CUDA, "mpm_sort_keys: no CUDA device");
+    }
+    mpm::DevMem k[2], v[2], hist, part;
+    mpm_status s = MPM_OK;
+    for (int i = 0; i < 2 && s == MPM_OK; ++i) {
+        s = k[i].alloc(sizeof(uint32_t) * n, "keys");
+        if (s == MPM_OK) s = v[i].alloc(sizeof(uint32_t) * n, "values");
+    }
+    const size_t tiles = mpm::radixTiles(n);
+    if (s == MPM_OK) s = hist.alloc(sizeof(uint32_t) * 256 * tiles, "histogram");
+    if (s == MPM_OK) s = part.alloc(sizeof(uint32_t) * (mpm::scanScratchElems(256 * tiles) + 1), "scan scratch");
+    bool inB = false;
+    cudaError_t e = cudaSuccess;
+    if (s == MPM_OK) {
+        e = cudaMemcpyAsync(k[0].p, keys, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = mpm::radixSortPairs(k[0].as<uint32_t>(), v[0].as<uint32_t>(), k[1].as<uint32_t>(), v[1].as<uint32_t>(),
+                                    n, bits, hist.as<uint32_t>(), part.as<uint32_t>(), &inB, st);
+        const int r = inB ? 1 : 0;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sorted_keys, k[r].p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(perm, v[r].p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s != MPM_OK) return s;
+    if (e != cudaSuccess) return mpm::fail(MPM_ERR_CUDA, std::string("mpm_sort_keys: ") + cudaGetErrorString(e));
+    return MPM_OK;
+}
+
+// ---- batch API (include/mpm_b200_batch.h) ----------------------------------
+mpm_status mpm_batch_create(mpm_batch** out) {
+    if (!out) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    std::unique_ptr<mpm_batch> b(new mpm_batch);
+    mpm_status st = b->eng.init();
+    if (st != MPM_OK) return st;
+    *out = b.release();
+    return MPM_OK;
+}
+mpm_status mpm_batch_destroy(mpm_batch* b) {
+    if (!b) return MPM_OK;
+    cudaStreamSynchronize(b->eng.stream());
+    delete b;
+    return MPM_OK;
+}
+mpm_status mpm_batch_add_scene(mpm_batch* b, const mpm_scene_desc* desc, const mpm_particles_in* particles,
+                               int32_t* scene_id) {
+    if (!b || !desc || !particles || !scene_id) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    int id = -1;
+    mpm_status st = b->eng.addScene(*desc, *particles, &id);
+    *scene_id = id;
+    return st;
+}
+mpm_status mpm_batch_remove_scene(mpm_batch* b, int32_t scene_id) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.removeScene(scene_id);
+}
+mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    GUARD(b->eng.step(nsteps));
+}
+mpm_status mpm_batch_synchronize(mpm_batch* b) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.synchronize();
+}
+mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.download(scene_id, field, host_out);
+}
+mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
+    if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    *n = (int32_t)b->eng.numScenes();
+    return MPM_OK;
+}
+mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    GUARD(b->eng.timedStep(nsteps, ms));
+}
+mpm_status mpm_batch_profile(mpm_batch* b, int32_t enable) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.profile(enable);
+}
+mpm_status mpm_batch_profile_read(mpm_batch* b, float* ms, int32_t* counts, int32_t nfamilies) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.profileRead(ms, counts, nfamilies);
+}
+
+}  // extern "C"

@@ -1,0 +1,114 @@
+// engine.cuh -- device-side data layout of the B200 MPM step.
+//
+// HBM layout (one scene):
+//   particles : two ping-pong SoA buffers.  Buffer k holds NFIELDS float
+//               planes of `cap` floats (x[3] v[3] Fe[9] Fp[9] B[9] tau[6]
+//               mass vol0), plus pid (original index, u32) and mat (u16).
+//               After every step the live buffer is sorted by cell key.
+//   grid      : dense float4 v* (xyz, w = node mass) and, for PIC-FLIP,
+//               float4 v; node index x + X*(y + Y*z).
+//   keys      : per-particle u32 key = (global block << 6) | cell-in-block,
+//               blocks are 4^3 cells of stencil bases, shifted by one block
+//               so that bases down to -3 stay non-negative.
+// Batch-wide scratch: radix-sort ping-pong keys/values, the active-block
+// list, the dense block->slot map and the per-block P2G tiles.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mpm {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+enum Field : int {
+    F_X = 0,
+    F_V = 3,
+    F_FE = 6,
+    F_FP = 15,
+    F_B = 24,
+    F_TAU = 33,  // symmetric V0 * stress: xx yy zz xy xz yz
+    F_MASS = 39,
+    F_VOL = 40,
+    NFIELDS = 41
+};
+
+// Device error flags (bit mask).
+enum : uint32_t {
+    ERR_NONFINITE = 1u,      // a particle position/velocity became NaN/Inf
+    ERR_TILE_OVERFLOW = 2u,  // more active blocks than tile slots (never expected)
+    ERR_INDEX = 4u,          // a permutation or stencil index failed its range check (never expected)
+};
+
+struct ParticleBuf {
+    float* f;        // NFIELDS * cap
+    uint32_t* pid;   // cap
+    uint16_t* mat;   // cap
+};
+
+struct MaterialDev {
+    float mu0, lambda0, xi, theta_c, theta_s;
+    int model;
+};
+
+struct SceneDev {
+    float origin[3];
+    float h, inv_h, range;
+    float target[3];
+    int res[3];
+    int nb[3];             // blocks per axis
+    uint32_t block_base;   // global id of this scene's first block
+    uint32_t nblocks;      // nb.x*nb.y*nb.z; block_base + nblocks is the scene's "outside" block
+    uint32_t key_offset;   // first global particle slot of this scene
+    uint32_t n;            // particles
+    uint32_t cap;          // plane stride of the particle buffers
+    float dt, gravity, friction, blend, dinv;
+    int transfer, interp, S, boundary, sticky, pcoll, nmat;
+    ParticleBuf buf[2];
+    float4* vstar;         // dense res^3
+    float4* vold;          // dense res^3 (PIC-FLIP)
+    const MaterialDev* mats;
+    float* dbg;            // split-mode dense grid: mass, vel[3], force[3], vstar[3] planes
+};
+
+struct BlockItem {
+    uint32_t block;   // global block id
+    uint32_t start;   // first sorted particle (global)
+    uint32_t count;
+    uint32_t scene;
+};
+
+// Per-step kernel arguments.
+struct StepArgs {
+    const SceneDev* scenes;
+    int nscenes;
+    int parity;                  // live particle buffer index
+    const uint32_t* sorted_keys; // N
+    const uint32_t* perm;        // N: sorted position -> global old slot
+    const BlockItem* active;
+    const uint32_t* counters;    // [0] active blocks, [1] outside blocks
+    const BlockItem* outside;
+    const int32_t* block_slot;   // dense: block -> slot or -1
+    float* tiles;                // [slot][F][TN]
+    uint32_t tile_stride;        // floats per slot
+    uint32_t* next_keys;         // N
+    uint32_t* block_count;       // dense per block
+    uint32_t* err;               // error flags
+    uint32_t* stats;             // [2]: nodes with mass written by the grid pass
+};
+
+// P2G/grid-pass variants.
+enum P2GMode : int {
+    MODE_APIC_FUSED = 0,  // fields: m, p + dt f        (F = 4)
+    MODE_FLIP = 1,        // fields: m, p, f            (F = 7)
+    MODE_SPLIT = 2,       // fields: m, p, f (any transfer, split API, F = 7)
+    MODE_MASS = 3         // fields: m                  (F = 1)
+};
+
+__host__ __device__ constexpr int modeFields(int mode) {
+    return mode == MODE_APIC_FUSED ? 4 : (mode == MODE_MASS ? 1 : 7);
+}
+__host__ __device__ constexpr int tileNodes(int S) { return (S + 3) * (S + 3) * (S + 3); }
+
+}  // namespace mpm

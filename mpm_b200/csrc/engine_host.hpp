@@ -1,0 +1,68 @@
+// engine_host.hpp -- host-side launch interface between the engine and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/mpm_b200.h"
+#include "engine.cuh"
+
+namespace mpm {
+
+struct LaunchCtx {
+    const SceneDev* scenes;   // device scene table
+    int nscenes;
+    cudaStream_t stream;
+    unsigned particle_blocks;   // grid.x of per-particle kernels (grid.y = scene)
+    unsigned node_blocks;       // grid.x of dense per-node kernels
+    unsigned persistent_blocks; // grid of the persistent block kernels
+    int num_sms;
+};
+
+struct BlockBuffers {
+    uint32_t* block_count;            // total_blocks
+    unsigned long long* packed;       // total_blocks
+    unsigned long long* scanned;      // total_blocks
+    unsigned long long* scan_partials64;
+    unsigned long long* total64;      // 1
+    uint32_t* scene_block_base;       // nscenes + 1
+    BlockItem* active;                // max_active
+    BlockItem* outside;               // nscenes
+    uint32_t* counters;               // [0] active, [1] outside
+    int32_t* block_slot;              // total_blocks
+};
+
+// Host-side count of kernel launches issued by the library (kernels.cu).
+void noteLaunches(uint64_t n);
+uint64_t kernelLaunches();
+
+// sort.cu
+size_t scanScratchElems(size_t n);
+template <class T>
+cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, cudaStream_t st);
+size_t radixTiles(size_t n);
+cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n, int bits,
+                           uint32_t* hist, uint32_t* scan_partials, bool* result_in_b, cudaStream_t st);
+
+// kernels.cu
+void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err);
+void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks);
+void launchStress(const LaunchCtx& c, int parity);
+void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
+void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
+void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused);
+void launchDenseGravity(const LaunchCtx& c);
+void launchDenseUpdate(const LaunchCtx& c, float dt);
+void launchDenseCollision(const LaunchCtx& c, float dt);
+void launchDensePack(const LaunchCtx& c);
+void launchParticlesCollision(const LaunchCtx& c, int parity, float dt);
+void launchAdvect(const LaunchCtx& c, int parity, float dt);
+void launchVolume(const LaunchCtx& c, int parity, int S);
+void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out);
+void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in);
+size_t p2gSmemBytes(int S, int mode);
+
+}  // namespace mpm

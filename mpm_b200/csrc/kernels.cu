@@ -1,0 +1,1136 @@
+// kernels.cu -- the MPM step kernels for sm_100a.
+//
+//   keyKernel       cell keys of the live particle order (first step / after uploads)
+//   packBlocks / compactBlocks   active-block list from per-block particle counts
+//   stressKernel    V0 * stress (tau) from Fe, Fp (first step / after uploads)
+//   p2gKernel       deterministic block scatter (src/mpm_solver3d.cu:237-294,
+//                   src/apic_mpm_solver3d.cu:245-304)
+//   gridKernel      tile merge + gravity + velocity update + collision in one
+//                   pass (src/mpm_solver3d.cu:394-426, src/grid3d.cu:36-41)
+//   g2pKernel       gather + transfer blend + Fe/Fp plasticity + SVD + next
+//                   step's stress + particle collision + advection + next key
+//                   (src/mpm_solver3d.cu:316-391,428-445; apic :326-388)
+//   split-mode kernels for the reference's sub-step API.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "engine_host.hpp"
+#include "mpm_math.cuh"
+
+#include <atomic>
+
+namespace mpm {
+
+static std::atomic<uint64_t> g_launches{0};
+void noteLaunches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+__device__ __forceinline__ float ldg(const float* p) { return __ldg(p); }
+
+// Stencil base ceil(x/h - r) per axis (src/mpm_solver3d.cu:252-255).  Returns
+// false when the stencil misses the grid in some axis (or x is not finite).
+__device__ __forceinline__ bool stencilBase(const SceneDev& sc, const float* x, int* base) {
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float fb = ceilf(__fsub_rn(__fdiv_rn(x[a], sc.h), sc.range));
+        bool ok = (fb >= (float)(1 - sc.S)) && (fb <= (float)(sc.res[a] - 1));
+        inside = inside && ok;
+        base[a] = ok ? (int)fb : 0;
+    }
+    return inside;
+}
+
+__device__ __forceinline__ uint32_t makeKey(const SceneDev& sc, const int* base) {
+    int b[3], c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int t = base[a] + 4;
+        b[a] = t >> 2;
+        c[a] = t & 3;
+    }
+    uint32_t blk = sc.block_base + (uint32_t)((b[2] * sc.nb[1] + b[1]) * sc.nb[0] + b[0]);
+    return (blk << 6) | (uint32_t)(c[2] << 4) | (uint32_t)(c[1] << 2) | (uint32_t)c[0];
+}
+
+__device__ __forceinline__ uint32_t outsideKey(const SceneDev& sc) { return (sc.block_base + sc.nblocks) << 6; }
+
+__device__ __forceinline__ uint32_t particleKey(const SceneDev& sc, const float* x, uint32_t* err) {
+    int base[3];
+    bool fin = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]);
+    if (!fin) atomicOr(err, ERR_NONFINITE);
+    if (fin && stencilBase(sc, x, base)) return makeKey(sc, base);
+    return outsideKey(sc);
+}
+
+// Lame parameters after hardening (src/material_point3d.cu:158-162).
+__device__ __forceinline__ void plasticLame(const MaterialDev& m, const float* Fp, float& mu, float& la) {
+    float Jp = det3(Fp);
+    float f = expf(m.xi * (1.0f - Jp));
+    mu = m.mu0 * f;
+    la = m.lambda0 * f;
+}
+
+// tau = V0 * (dPsi/dFe) Fe^T, symmetric (xx yy zz xy xz yz), from the SVD of Fe.
+//  fixed corotated (src/material_point3d.cu:110-128):
+//     2 mu (Fe - R) Fe^T + la (J-1) J I  =  2 mu U diag(s(s-1)) U^T + la (J-1) J I
+//  Neo-Hookean (:131-155), with s clamped to >= FLT_EPSILON (Fe projected):
+//     mu (Fe Fe^T - I) + la ln(J) I      =  mu U diag(s^2) U^T - mu I + la ln J I
+__device__ __forceinline__ void tauFromSvd(int model, const float* U, const float* s, float mu, float la, float V0,
+                                           float* tau) {
+    float d[3], diag;
+    float J = s[0] * s[1] * s[2];
+    if (model == MPM_MODEL_NEO_HOOKEAN) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) d[k] = mu * s[k] * s[k];
+        diag = la * logf(J) - mu;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) d[k] = 2.0f * mu * s[k] * (s[k] - 1.0f);
+        diag = la * (J - 1.0f) * J;
+    }
+    const int I[6] = {0, 1, 2, 0, 0, 1}, Jx[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        int i = I[e], j = Jx[e];
+        float v = U[3 * i] * d[0] * U[3 * j] + U[3 * i + 1] * d[1] * U[3 * j + 1] + U[3 * i + 2] * d[2] * U[3 * j + 2];
+        if (e < 3) v += diag;
+        tau[e] = V0 * v;
+    }
+}
+
+// Stress of a particle from its current Fe (Neo-Hookean projects Fe in place).
+__device__ __forceinline__ void stressFromFe(const MaterialDev& m, float* Fe, const float* Fp, float V0, float* tau) {
+    float U[9], V[9], s[3];
+    svd3(Fe, U, s, V);
+    float mu, la;
+    plasticLame(m, Fp, mu, la);
+    if (m.model == MPM_MODEL_NEO_HOOKEAN) {
+        bool proj = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            proj |= s[k] < kFltEps;
+            s[k] = fmaxf(s[k], kFltEps);
+        }
+        if (proj) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    Fe[3 * i + j] = U[3 * i] * s[0] * V[3 * j] + U[3 * i + 1] * s[1] * V[3 * j + 1] +
+                                    U[3 * i + 2] * s[2] * V[3 * j + 2];
+        }
+    }
+    tauFromSvd(m.model, U, s, mu, la, V0, tau);
+}
+
+__device__ __forceinline__ int sceneOfBlock(const uint32_t* scene_block_base, int nscenes, uint32_t b) {
+    int lo = 0, hi = nscenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (scene_block_base[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Keys of the live particle order (used when keys were not produced by G2P).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) keyKernel(const SceneDev* __restrict__ scenes, int parity,
+                                                       uint32_t* __restrict__ keys, uint32_t* __restrict__ block_count,
+                                                       uint32_t* __restrict__ err) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    const float* f = sc.buf[parity].f;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        float x[3] = {f[(F_X + 0) * cap + i], f[(F_X + 1) * cap + i], f[(F_X + 2) * cap + i]};
+        uint32_t key = particleKey(sc, x, err);
+        keys[sc.key_offset + i] = key;
+        atomicAdd(&block_count[key >> 6], 1u);
+    }
+}
+
+// Packs (active flag << 32 | count) per global block.  Scene outside blocks
+// never become active.
+__global__ void __launch_bounds__(kThreads) packBlocksKernel(const uint32_t* __restrict__ block_count,
+                                                              unsigned long long* __restrict__ packed,
+                                                              uint32_t total_blocks,
+                                                              const uint32_t* __restrict__ scene_block_base,
+                                                              int nscenes, uint32_t* __restrict__ counters) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters[1] = 0;
+        counters[2] = 0;
+    }
+    for (uint32_t b = blockIdx.x * kThreads + threadIdx.x; b < total_blocks; b += gridDim.x * kThreads) {
+        uint32_t c = block_count[b];
+        int s = sceneOfBlock(scene_block_base, nscenes, b);
+        bool outside = (b == scene_block_base[s + 1] - 1);
+        unsigned long long flag = (c > 0 && !outside) ? 1ull : 0ull;
+        packed[b] = (flag << 32) | (unsigned long long)c;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) compactBlocksKernel(
+    const unsigned long long* __restrict__ packed, const unsigned long long* __restrict__ scanned,
+    const unsigned long long* __restrict__ total, uint32_t total_blocks, const uint32_t* __restrict__ scene_block_base,
+    int nscenes, BlockItem* __restrict__ active, BlockItem* __restrict__ outside, uint32_t* __restrict__ counters,
+    int32_t* __restrict__ block_slot, uint32_t* __restrict__ block_count) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = (uint32_t)(*total >> 32);
+    for (uint32_t b = blockIdx.x * kThreads + threadIdx.x; b < total_blocks; b += gridDim.x * kThreads) {
+        unsigned long long v = packed[b], s = scanned[b];
+        uint32_t count = (uint32_t)(v & 0xffffffffull);
+        uint32_t start = (uint32_t)(s & 0xffffffffull);
+        int scene = sceneOfBlock(scene_block_base, nscenes, b);
+        if (v >> 32) {
+            uint32_t slot = (uint32_t)(s >> 32);
+            active[slot] = BlockItem{b, start, count, (uint32_t)scene};
+            block_slot[b] = (int32_t)slot;
+        } else {
+            block_slot[b] = -1;
+            if (count > 0) {
+                uint32_t o = atomicAdd(&counters[1], 1u);
+                outside[o] = BlockItem{b, start, count, (uint32_t)scene};
+            }
+        }
+        block_count[b] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tau from Fe/Fp for the live order (first step, after uploads).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) stressKernel(const SceneDev* __restrict__ scenes, int parity) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    float* f = sc.buf[parity].f;
+    const uint16_t* mat = sc.buf[parity].mat;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        float Fe[9], Fp[9], tau[6];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            Fe[k] = f[(F_FE + k) * cap + i];
+            Fp[k] = f[(F_FP + k) * cap + i];
+        }
+        MaterialDev m = sc.mats[sc.nmat > 1 ? mat[i] : 0];
+        stressFromFe(m, Fe, Fp, f[F_VOL * cap + i], tau);
+        if (m.model == MPM_MODEL_NEO_HOOKEAN)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) f[(F_FE + k) * cap + i] = Fe[k];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) f[(F_TAU + k) * cap + i] = tau[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2G: one CTA per active 4^3-cell block (persistent loop).  Each warp takes
+// whole cells; its lanes own the S^3 stencil nodes of the cell and accumulate
+// the cell's particles in sorted order in registers.  Cell partial sums are
+// merged into the (S+3)^3 block tile by a fixed-order gather, and the tile is
+// written to scratch.  No floating-point atomics: bitwise deterministic.
+// ---------------------------------------------------------------------------
+template <int S, int MODE>
+struct P2GLayout {
+    static constexpr int F = modeFields(MODE);
+    static constexpr int NS = S * S * S;              // stencil nodes
+    static constexpr int NJ = (NS + 31) / 32;         // nodes per lane
+    static constexpr int TN = tileNodes(S);
+    static constexpr int TJ = (TN + kThreads - 1) / kThreads;
+    // staged payload per particle: w[3][S], dw[3][S], then mode extras
+    static constexpr int OW = 0, ODW = 3 * S;
+    static constexpr int OM = (MODE == MODE_MASS) ? 3 * S : 6 * S;
+    static constexpr int OQ = OM + 1;   // q or m v (3)
+    static constexpr int OHC = OQ + 3;  // h m C (9)
+    static constexpr int OT = (MODE == MODE_FLIP) ? OQ + 3 : OHC + 9;  // stress term (6)
+    static constexpr int RAW = (MODE == MODE_MASS) ? OM + 1 : OT + 6;
+    static constexpr int P = RAW | 1;   // odd stride: conflict-free staging writes
+    static constexpr int kCells = 32;   // cells per half-block
+    static constexpr size_t smemFloats = (size_t)kWarps * 32 * P + (size_t)kCells * F * 64;
+    static constexpr size_t smemBytes = smemFloats * 4 + 3 * 64 * 4;
+};
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_transfer) {
+    using L = P2GLayout<S, MODE>;
+    constexpr int F = L::F;
+    extern __shared__ float smem[];
+    float* stage = smem;                                     // [warp][32][P]
+    float* partial = smem + (size_t)kWarps * 32 * L::P;      // [cell][F][64]
+    int* cellBeg = (int*)(partial + (size_t)L::kCells * F * 64);
+    int* cellEnd = cellBeg + 64;
+    int* cellNonEmpty = cellEnd + 64;
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nact = args.counters[0];
+    for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
+        const BlockItem it = args.active[w];
+        const SceneDev& sc = args.scenes[it.scene];
+        if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
+        const float* pf = sc.buf[args.parity].f;
+        const size_t cap = sc.cap;
+        const uint32_t lb = it.block - sc.block_base;
+        const int bx = (int)(lb % (uint32_t)sc.nb[0]);
+        const int by = (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]);
+        const int bz = (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]));
+        const int t0[3] = {4 * bx - 4, 4 * by - 4, 4 * bz - 4};
+
+        // Cell ranges inside the block (keys are sorted by cell).
+        for (int c = threadIdx.x; c < 64; c += kThreads) cellBeg[c] = cellEnd[c] = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
+            uint32_t g = it.start + i;
+            uint32_t c = args.sorted_keys[g] & 63u;
+            if (i == 0 || (args.sorted_keys[g - 1] & 63u) != c) cellBeg[c] = (int)i;
+            if (i == it.count - 1 || (args.sorted_keys[g + 1] & 63u) != c) cellEnd[c] = (int)i + 1;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < 64; c += kThreads) cellNonEmpty[c] = cellEnd[c] > cellBeg[c];
+
+        float tacc[L::TJ][F];
+#pragma unroll
+        for (int j = 0; j < L::TJ; ++j)
+#pragma unroll
+            for (int f = 0; f < F; ++f) tacc[j][f] = 0.f;
+
+        const float dt = sc.dt, h = sc.h;
+        for (int half = 0; half < 2; ++half) {
+            // ---- particle phase: warp per cell ----
+            for (int cl = warp; cl < L::kCells; cl += kWarps) {
+                const int cell = half * 32 + cl;
+                const int beg = cellBeg[cell], end = cellEnd[cell];
+                float acc[L::NJ][F];
+#pragma unroll
+                for (int j = 0; j < L::NJ; ++j)
+#pragma unroll
+                    for (int f = 0; f < F; ++f) acc[j][f] = 0.f;
+                float* st = stage + (size_t)warp * 32 * L::P;
+                for (int g0 = beg; g0 < end; g0 += 32) {
+                    const int np = min(32, end - g0);
+                    if (lane < np) {
+                        float* my = st + lane * L::P;
+                        const uint32_t gs = it.start + (uint32_t)(g0 + lane);
+                        uint32_t old = args.perm[gs] - sc.key_offset;
+                        const bool bad = old >= sc.n;  // range check: flag and contribute nothing
+                        if (bad) {
+                            atomicOr(args.err, ERR_INDEX);
+                            old = 0;
+                        }
+                        float x[3] = {ldg(pf + (F_X + 0) * cap + old), ldg(pf + (F_X + 1) * cap + old),
+                                      ldg(pf + (F_X + 2) * cap + old)};
+                        int base[3];
+                        stencilBase(sc, x, base);
+                        float delta[3];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
+                            delta[a] = x[a] - gp0;
+#pragma unroll
+                            for (int k = 0; k < S; ++k) {
+                                float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                                float d = __fdiv_rn(__fsub_rn(x[a], gp), h);
+                                my[L::OW + a * S + k] = splineN<S>(d);
+                                if (MODE != MODE_MASS) my[L::ODW + a * S + k] = __fdiv_rn(splineNDot<S>(d), h);
+                            }
+                        }
+                        const float m = bad ? 0.f : ldg(pf + F_MASS * cap + old);
+                        my[L::OM] = m;
+                        if (MODE != MODE_MASS) {
+                            float v[3] = {ldg(pf + (F_V + 0) * cap + old), ldg(pf + (F_V + 1) * cap + old),
+                                          ldg(pf + (F_V + 2) * cap + old)};
+                            float tau[6];
+#pragma unroll
+                            for (int k = 0; k < 6; ++k) tau[k] = ldg(pf + (F_TAU + k) * cap + old);
+                            const float ts = bad ? 0.f : ((MODE == MODE_APIC_FUSED) ? -dt : -1.0f);
+#pragma unroll
+                            for (int k = 0; k < 6; ++k) my[L::OT + k] = ts * tau[k];
+                            if (MODE == MODE_FLIP) {
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) my[L::OQ + a] = m * v[a];
+                            } else {
+                                float mC[9];
+                                if (sc.transfer == MPM_TRANSFER_APIC) {
+                                    const float md = m * sc.dinv;
+#pragma unroll
+                                    for (int k = 0; k < 9; ++k) mC[k] = md * ldg(pf + (F_B + k) * cap + old);
+                                } else {
+#pragma unroll
+                                    for (int k = 0; k < 9; ++k) mC[k] = 0.f;
+                                }
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) {
+                                    my[L::OQ + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
+                                                                mC[3 * a + 2] * delta[2]);
+#pragma unroll
+                                    for (int b = 0; b < 3; ++b) my[L::OHC + 3 * a + b] = h * mC[3 * a + b];
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    for (int q = 0; q < np; ++q) {
+                        const float* pq = st + q * L::P;
+                        const float m = pq[L::OM];
+#pragma unroll
+                        for (int j = 0; j < L::NJ; ++j) {
+                            const int k = lane + 32 * j;
+                            if (k < L::NS) {
+                                const int a = k % S, b = (k / S) % S, c = k / (S * S);
+                                const float wa = pq[L::OW + a], wb = pq[L::OW + S + b], wc = pq[L::OW + 2 * S + c];
+                                const float wab = wa * wb;
+                                const float wgt = wab * wc;
+                                acc[j][0] = fmaf(m, wgt, acc[j][0]);
+                                if (MODE != MODE_MASS) {
+                                    const float da = pq[L::ODW + a], db = pq[L::ODW + S + b], dc = pq[L::ODW + 2 * S + c];
+                                    const float gx = da * wb * wc, gy = wa * db * wc, gz = wab * dc;
+                                    const float* T = pq + L::OT;  // xx yy zz xy xz yz
+                                    const float tg0 = fmaf(T[0], gx, fmaf(T[3], gy, T[4] * gz));
+                                    const float tg1 = fmaf(T[3], gx, fmaf(T[1], gy, T[5] * gz));
+                                    const float tg2 = fmaf(T[4], gx, fmaf(T[5], gy, T[2] * gz));
+                                    if (MODE == MODE_FLIP) {
+                                        acc[j][1] = fmaf(wgt, pq[L::OQ + 0], acc[j][1]);
+                                        acc[j][2] = fmaf(wgt, pq[L::OQ + 1], acc[j][2]);
+                                        acc[j][3] = fmaf(wgt, pq[L::OQ + 2], acc[j][3]);
+                                        acc[j][4] += tg0;
+                                        acc[j][5] += tg1;
+                                        acc[j][6] += tg2;
+                                    } else {
+                                        const float fa = (float)a, fb = (float)b, fc = (float)c;
+                                        const float* hC = pq + L::OHC;
+                                        float u0 = fmaf(hC[0], fa, fmaf(hC[1], fb, fmaf(hC[2], fc, pq[L::OQ + 0])));
+                                        float u1 = fmaf(hC[3], fa, fmaf(hC[4], fb, fmaf(hC[5], fc, pq[L::OQ + 1])));
+                                        float u2 = fmaf(hC[6], fa, fmaf(hC[7], fb, fmaf(hC[8], fc, pq[L::OQ + 2])));
+                                        if (MODE == MODE_APIC_FUSED) {
+                                            acc[j][1] += fmaf(wgt, u0, tg0);
+                                            acc[j][2] += fmaf(wgt, u1, tg1);
+                                            acc[j][3] += fmaf(wgt, u2, tg2);
+                                        } else {  // MODE_SPLIT
+                                            acc[j][1] = fmaf(wgt, u0, acc[j][1]);
+                                            acc[j][2] = fmaf(wgt, u1, acc[j][2]);
+                                            acc[j][3] = fmaf(wgt, u2, acc[j][3]);
+                                            acc[j][4] += tg0;
+                                            acc[j][5] += tg1;
+                                            acc[j][6] += tg2;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+                float* pc = partial + (size_t)cl * F * 64;
+#pragma unroll
+                for (int j = 0; j < L::NJ; ++j) {
+                    const int k = lane + 32 * j;
+                    if (k < L::NS)
+#pragma unroll
+                        for (int f = 0; f < F; ++f) pc[f * 64 + k] = acc[j][f];
+                }
+            }
+            __syncthreads();
+            // ---- gather phase: fixed-order merge of this half's cells ----
+#pragma unroll
+            for (int j = 0; j < L::TJ; ++j) {
+                const int tn = threadIdx.x + j * kThreads;
+                if (tn < L::TN) {
+                    const int tx = tn % (S + 3), ty = (tn / (S + 3)) % (S + 3), tz = tn / ((S + 3) * (S + 3));
+#pragma unroll
+                    for (int czl = 0; czl < 2; ++czl) {
+                        const int cz = half * 2 + czl, dz = tz - cz;
+                        if (dz < 0 || dz >= S) continue;
+                        for (int cy = 0; cy < 4; ++cy) {
+                            const int dy = ty - cy;
+                            if (dy < 0 || dy >= S) continue;
+                            for (int cx = 0; cx < 4; ++cx) {
+                                const int dx = tx - cx;
+                                if (dx < 0 || dx >= S) continue;
+                                const int cell = (cz * 4 + cy) * 4 + cx;
+                                if (!cellNonEmpty[cell]) continue;
+                                const int cl = cell - half * 32;
+                                const int k = dx + S * (dy + S * dz);
+                                const float* pc = partial + (size_t)cl * F * 64 + k;
+#pragma unroll
+                                for (int f = 0; f < F; ++f) tacc[j][f] += pc[f * 64];
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        float* tile = args.tiles + (size_t)w * args.tile_stride;
+#pragma unroll
+        for (int j = 0; j < L::TJ; ++j) {
+            const int tn = threadIdx.x + j * kThreads;
+            if (tn < L::TN)
+#pragma unroll
+                for (int f = 0; f < F; ++f) tile[f * L::TN + tn] = tacc[j][f];
+        }
+        (void)t0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grid pass: merge the <= 8 overlapping tiles of every node in fixed order,
+// then gravity, v = p/m, v* = v + dt f/m (m > FLT_EPSILON), boundary.
+// Node-block N (4^3 nodes starting at 4N-4) is processed by the active block
+// B = N - d with the smallest d in {0,1}^3 (x + 2y + 4z order).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int blockSlotAt(const StepArgs& args, const SceneDev& sc, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= sc.nb[0] || y >= sc.nb[1] || z >= sc.nb[2]) return -1;
+    return args.block_slot[sc.block_base + (uint32_t)((z * sc.nb[1] + y) * sc.nb[0] + x)];
+}
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_transfer) {
+    constexpr int F = modeFields(MODE);
+    constexpr int T = S + 3;
+    constexpr int TN = tileNodes(S);
+    const uint32_t nact = args.counters[0];
+    for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
+        const BlockItem it = args.active[w];
+        const SceneDev& sc = args.scenes[it.scene];
+        if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
+        const uint32_t lb = it.block - sc.block_base;
+        const int B[3] = {(int)(lb % (uint32_t)sc.nb[0]), (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]),
+                          (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]))};
+        for (int round = 0; round < 2; ++round) {
+            const int d = round * 4 + (threadIdx.x >> 6);
+            const int dd[3] = {d & 1, (d >> 1) & 1, (d >> 2) & 1};
+            const int N[3] = {B[0] + dd[0], B[1] + dd[1], B[2] + dd[2]};
+            if (N[0] >= sc.nb[0] || N[1] >= sc.nb[1] || N[2] >= sc.nb[2]) continue;
+            bool owner = true;
+            for (int e = 0; e < d && owner; ++e)
+                if (blockSlotAt(args, sc, N[0] - (e & 1), N[1] - ((e >> 1) & 1), N[2] - ((e >> 2) & 1)) >= 0)
+                    owner = false;
+            if (!owner) continue;
+            const int l = threadIdx.x & 63;
+            const int L[3] = {l & 3, (l >> 2) & 3, l >> 4};
+            const int n[3] = {4 * N[0] - 4 + L[0], 4 * N[1] - 4 + L[1], 4 * N[2] - 4 + L[2]};
+            if (n[0] < 0 || n[1] < 0 || n[2] < 0 || n[0] >= sc.res[0] || n[1] >= sc.res[1] || n[2] >= sc.res[2])
+                continue;
+            float acc[F];
+#pragma unroll
+            for (int f = 0; f < F; ++f) acc[f] = 0.f;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int de[3] = {e & 1, (e >> 1) & 1, (e >> 2) & 1};
+                const int ix = L[0] + 4 * de[0], iy = L[1] + 4 * de[1], iz = L[2] + 4 * de[2];
+                if (ix >= T || iy >= T || iz >= T) continue;
+                const int slot = blockSlotAt(args, sc, N[0] - de[0], N[1] - de[1], N[2] - de[2]);
+                if (slot < 0) continue;
+                const float* tile = args.tiles + (size_t)slot * args.tile_stride + ix + T * (iy + T * iz);
+#pragma unroll
+                for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+            }
+            const size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);
+            const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];
+            if (MODE == MODE_SPLIT) {
+                float* dbg = sc.dbg;
+                dbg[node] += acc[0];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    dbg[(1 + a) * nodes + node] += acc[1 + a];
+                    dbg[(4 + a) * nodes + node] += acc[4 + a];
+                }
+                continue;
+            }
+            if (MODE == MODE_MASS) {
+                sc.vstar[node] = make_float4(0.f, 0.f, 0.f, acc[0]);
+                continue;
+            }
+            const float m = acc[0], dt = sc.dt;
+            if (m > 0.f) atomicAdd(&args.stats[2], 1u);
+            float vs[3] = {0.f, 0.f, 0.f}, vo[3] = {0.f, 0.f, 0.f};
+            if (MODE == MODE_APIC_FUSED) {
+                if (m > kFltEps) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) vs[a] = __fdiv_rn(acc[1 + a], m);
+                    vs[1] -= dt * sc.gravity;
+                }
+            } else {  // MODE_FLIP
+                if (m > kFltEps) {
+                    float fy = acc[5] - sc.gravity * m;
+                    const float fo[3] = {acc[4], fy, acc[6]};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        vo[a] = __fdiv_rn(acc[1 + a], m);
+                        vs[a] = vo[a] + __fdiv_rn(dt * fo[a], m);
+                    }
+                } else {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) vo[a] = acc[1 + a];
+                }
+            }
+            if (sc.boundary == MPM_BOUNDARY_STICKY) {
+                bool wall = false;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) wall |= (n[a] < sc.sticky) || (n[a] >= sc.res[a] - sc.sticky);
+                if (wall) vs[0] = vs[1] = vs[2] = 0.f;
+            } else {
+                float pos[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
+                boundaryCollision(pos, vs, sc.origin, sc.target, sc.friction);
+            }
+            sc.vstar[node] = make_float4(vs[0], vs[1], vs[2], m);
+            if (MODE == MODE_FLIP) sc.vold[node] = make_float4(vo[0], vo[1], vo[2], 0.f);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// G2P, fused with the particle update.  One CTA per active block: the block's
+// (S+3)^3 node tile of v* (and v) is staged in shared memory, then one thread
+// per particle.  Writes the particle to its sorted slot of the other buffer.
+// ---------------------------------------------------------------------------
+template <int S, bool APIC>
+__device__ __forceinline__ void particleUpdate(const StepArgs& args, const SceneDev& sc, uint32_t gs,
+                                               const float4* tvs, const float4* tvo, const int* t0, bool fused) {
+    constexpr int T = S + 3;
+    const float* pf = sc.buf[args.parity].f;
+    float* nf = sc.buf[args.parity ^ 1].f;
+    const size_t cap = sc.cap;
+    const uint32_t old = args.perm[gs] - sc.key_offset;
+    const uint32_t dst = gs - sc.key_offset;
+    if (old >= sc.n || dst >= sc.n) {  // range check: never expected, skip instead of faulting
+        atomicOr(args.err, ERR_INDEX);
+        return;
+    }
+    const float h = sc.h, dt = sc.dt;
+    float x[3], v[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        x[a] = ldg(pf + (F_X + a) * cap + old);
+        v[a] = ldg(pf + (F_V + a) * cap + old);
+    }
+    float vpic[3] = {0.f, 0.f, 0.f}, dflip[3] = {0.f, 0.f, 0.f};
+    float gv[9], K[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gv[k] = K[k] = 0.f;
+    float delta[3] = {0.f, 0.f, 0.f};
+    int base[3];
+    bool in_tile = false;
+    if (tvs) {
+        in_tile = stencilBase(sc, x, base);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) in_tile = in_tile && base[a] - t0[a] >= 0 && base[a] - t0[a] <= 3;
+        if (!in_tile) atomicOr(args.err, ERR_INDEX);  // key and position disagree: never expected
+    }
+    if (in_tile) {
+        float w[3][S], dw[3][S];
+        int lo[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = base[a] - t0[a];
+            float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
+            delta[a] = x[a] - gp0;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                float d = __fdiv_rn(__fsub_rn(x[a], gp), h);
+                w[a][k] = splineN<S>(d);
+                dw[a][k] = __fdiv_rn(splineNDot<S>(d), h);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+#pragma unroll
+            for (int b = 0; b < S; ++b) {
+                float r0[3] = {0.f, 0.f, 0.f}, r1[3] = {0.f, 0.f, 0.f}, rd[3] = {0.f, 0.f, 0.f},
+                      rv[3] = {0.f, 0.f, 0.f};
+                const int rowbase = lo[0] + T * ((lo[1] + b) + T * (lo[2] + c));
+#pragma unroll
+                for (int a = 0; a < S; ++a) {
+                    const float4 g = tvs[rowbase + a];
+                    const float gs3[3] = {g.x, g.y, g.z};
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        r0[i] = fmaf(w[0][a], gs3[i], r0[i]);
+                        rd[i] = fmaf(dw[0][a], gs3[i], rd[i]);
+                        if (APIC) r1[i] = fmaf(w[0][a] * (float)a, gs3[i], r1[i]);
+                    }
+                    if (!APIC) {
+                        const float4 o = tvo[rowbase + a];
+                        rv[0] = fmaf(w[0][a], g.x - o.x, rv[0]);
+                        rv[1] = fmaf(w[0][a], g.y - o.y, rv[1]);
+                        rv[2] = fmaf(w[0][a], g.z - o.z, rv[2]);
+                    }
+                }
+                const float wyz = w[1][b] * w[2][c];
+                const float dy = dw[1][b] * w[2][c];
+                const float dz = w[1][b] * dw[2][c];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    vpic[i] = fmaf(wyz, r0[i], vpic[i]);
+                    gv[3 * i + 0] = fmaf(wyz, rd[i], gv[3 * i + 0]);
+                    gv[3 * i + 1] = fmaf(dy, r0[i], gv[3 * i + 1]);
+                    gv[3 * i + 2] = fmaf(dz, r0[i], gv[3 * i + 2]);
+                    if (APIC) {
+                        K[3 * i + 0] = fmaf(wyz, r1[i], K[3 * i + 0]);
+                        K[3 * i + 1] = fmaf(wyz * (float)b, r0[i], K[3 * i + 1]);
+                        K[3 * i + 2] = fmaf(wyz * (float)c, r0[i], K[3 * i + 2]);
+                    } else {
+                        dflip[i] = fmaf(wyz, rv[i], dflip[i]);
+                    }
+                }
+            }
+        }
+    }
+    // New velocity (src/mpm_solver3d.cu:362-363; apic :366-374).
+    float vn[3];
+    if (APIC) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) vn[i] = vpic[i];
+    } else {
+        const float al = sc.blend, om = 1.0f - sc.blend;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) vn[i] = al * (v[i] + dflip[i]) + om * vpic[i];
+    }
+    // Fe <- (I + dt grad v) Fe ; F = Fe Fp ; SVD clamp (src/material_point3d.cu:53-70).
+    float Fe[9], Fp[9], A[9], Fn[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        Fe[k] = ldg(pf + (F_FE + k) * cap + old);
+        Fp[k] = ldg(pf + (F_FP + k) * cap + old);
+        A[k] = dt * gv[k] + ((k % 4 == 0) ? 1.0f : 0.0f);
+    }
+    matmul3(A, Fe, Fn);
+    float U[9], V[9], s[3];
+    svd3(Fn, U, s, V);
+    const uint16_t mid = sc.nmat > 1 ? sc.buf[args.parity].mat[old] : (uint16_t)0;
+    const MaterialDev m = sc.mats[mid];
+    const float hi = 1.0f + m.theta_s, lo = 1.0f - m.theta_c;
+    bool clamped = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float c = fmaxf(fminf(s[k], hi), lo);
+        clamped |= c != s[k];
+        s[k] = c;
+    }
+    if (clamped) {
+        // Fe = U S V^T ; Fp = V S^-1 U^T (Fe Fp)
+        float Ff[9];
+        matmul3(Fn, Fp, Ff);
+        float US[9], VSi[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                US[3 * i + k] = U[3 * i + k] * s[k];
+                VSi[3 * i + k] = V[3 * i + k] / s[k];
+            }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                Fe[3 * i + j] = US[3 * i] * V[3 * j] + US[3 * i + 1] * V[3 * j + 1] + US[3 * i + 2] * V[3 * j + 2];
+                A[3 * i + j] = VSi[3 * i] * U[3 * j] + VSi[3 * i + 1] * U[3 * j + 1] + VSi[3 * i + 2] * U[3 * j + 2];
+            }
+        matmul3(A, Ff, Fp);
+    } else {
+        // No singular value clamped: U S V^T = Fn and V S^-1 U^T Fn Fp = Fp in
+        // exact arithmetic; keeping Fn and Fp avoids the FP32 SVD round-off.
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Fe[k] = Fn[k];
+    }
+    // Next step's stress from the clamped SVD (Fe = U S V^T exactly).
+    const float V0 = ldg(pf + F_VOL * cap + old);
+    float mu, la, tau[6];
+    plasticLame(m, Fp, mu, la);
+    if (m.model == MPM_MODEL_NEO_HOOKEAN) {
+        bool proj = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            proj |= s[k] < kFltEps;
+            s[k] = fmaxf(s[k], kFltEps);
+        }
+        if (proj)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    Fe[3 * i + j] = U[3 * i] * s[0] * V[3 * j] + U[3 * i + 1] * s[1] * V[3 * j + 1] +
+                                    U[3 * i + 2] * s[2] * V[3 * j + 2];
+    }
+    tauFromSvd(m.model, U, s, mu, la, V0, tau);
+    if (fused) {
+        if (sc.pcoll) {  // particlesCollision (src/mpm_solver3d.cu:428-445)
+            float pos[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) pos[a] = x[a] + dt * vn[a];
+            boundaryCollision(pos, vn, sc.origin, sc.target, sc.friction);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x[a] += dt * vn[a];  // advectParticles (:381-391)
+        const uint32_t key = particleKey(sc, x, args.err);
+        args.next_keys[gs] = key;
+        atomicAdd(&args.block_count[key >> 6], 1u);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        nf[(F_X + a) * cap + dst] = x[a];
+        nf[(F_V + a) * cap + dst] = vn[a];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        nf[(F_FE + k) * cap + dst] = Fe[k];
+        nf[(F_FP + k) * cap + dst] = Fp[k];
+    }
+    if (APIC) {
+        // B = sum w v* (x_i - x_p)^T = h K - vpic delta^T
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) nf[(F_B + 3 * i + j) * cap + dst] = h * K[3 * i + j] - vpic[i] * delta[j];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) nf[(F_TAU + k) * cap + dst] = tau[k];
+    nf[F_MASS * cap + dst] = ldg(pf + F_MASS * cap + old);
+    nf[F_VOL * cap + dst] = V0;
+    sc.buf[args.parity ^ 1].pid[dst] = sc.buf[args.parity].pid[old];
+    if (sc.nmat > 1) sc.buf[args.parity ^ 1].mat[dst] = mid;
+}
+
+template <int S, bool APIC>
+__global__ void __launch_bounds__(kThreads) g2pKernel(StepArgs args, int fused) {
+    constexpr int T = S + 3;
+    constexpr int TN = tileNodes(S);
+    __shared__ float4 tvs[TN];
+    __shared__ float4 tvo[APIC ? 1 : TN];
+    const int want = APIC ? MPM_TRANSFER_APIC : MPM_TRANSFER_PIC_FLIP;
+    const uint32_t nact = args.counters[0];
+    const uint32_t nout = args.counters[1];
+    for (uint32_t w = blockIdx.x; w < nact + nout; w += gridDim.x) {
+        const bool inside = w < nact;
+        const BlockItem it = inside ? args.active[w] : args.outside[w - nact];
+        const SceneDev& sc = args.scenes[it.scene];
+        if (sc.S != S || sc.transfer != want) continue;
+        int t0[3] = {0, 0, 0};
+        if (inside) {
+            const uint32_t lb = it.block - sc.block_base;
+            t0[0] = 4 * (int)(lb % (uint32_t)sc.nb[0]) - 4;
+            t0[1] = 4 * (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]) - 4;
+            t0[2] = 4 * (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1])) - 4;
+            for (int tn = threadIdx.x; tn < TN; tn += kThreads) {
+                const int n[3] = {t0[0] + tn % T, t0[1] + (tn / T) % T, t0[2] + tn / (T * T)};
+                const bool in = n[0] >= 0 && n[1] >= 0 && n[2] >= 0 && n[0] < sc.res[0] && n[1] < sc.res[1] &&
+                                n[2] < sc.res[2];
+                const size_t node = in ? (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]) : 0;
+                tvs[tn] = in ? sc.vstar[node] : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (!APIC) tvo[tn] = in ? sc.vold[node] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            __syncthreads();
+        }
+        for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
+            particleUpdate<S, APIC>(args, sc, it.start + i, inside ? tvs : nullptr, APIC ? nullptr : tvo, t0,
+                                    fused != 0);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Split-mode dense grid kernels on sc.dbg planes: mass, vel[3], force[3], vstar[3].
+// ---------------------------------------------------------------------------
+__global__ void denseGravityKernel(const SceneDev* __restrict__ scenes) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads) {
+        float m = sc.dbg[i];
+        if (m > kFltEps) sc.dbg[5 * nodes + i] -= sc.gravity * m;  // force.y
+    }
+}
+
+__global__ void denseUpdateVelocityKernel(const SceneDev* __restrict__ scenes, float dt) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads) {
+        float m = sc.dbg[i];
+        if (m > kFltEps) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float v = __fdiv_rn(sc.dbg[(1 + a) * nodes + i], m);
+                sc.dbg[(1 + a) * nodes + i] = v;
+                sc.dbg[(7 + a) * nodes + i] = v + __fdiv_rn(dt * sc.dbg[(4 + a) * nodes + i], m);
+            }
+        }
+    }
+}
+
+__global__ void denseCollisionKernel(const SceneDev* __restrict__ scenes, float dt) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads) {
+        const int n[3] = {(int)(i % sc.res[0]), (int)((i / sc.res[0]) % sc.res[1]),
+                          (int)(i / ((size_t)sc.res[0] * sc.res[1]))};
+        float vs[3] = {sc.dbg[7 * nodes + i], sc.dbg[8 * nodes + i], sc.dbg[9 * nodes + i]};
+        if (sc.boundary == MPM_BOUNDARY_STICKY) {
+            bool wall = false;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) wall |= (n[a] < sc.sticky) || (n[a] >= sc.res[a] - sc.sticky);
+            if (wall) vs[0] = vs[1] = vs[2] = 0.f;
+        } else {
+            float pos[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
+            boundaryCollision(pos, vs, sc.origin, sc.target, sc.friction);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sc.dbg[(7 + a) * nodes + i] = vs[a];
+    }
+}
+
+// dbg planes -> float4 v*, v for the G2P kernel.
+__global__ void densePackKernel(const SceneDev* __restrict__ scenes) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads) {
+        sc.vstar[i] = make_float4(sc.dbg[7 * nodes + i], sc.dbg[8 * nodes + i], sc.dbg[9 * nodes + i], sc.dbg[i]);
+        if (sc.vold)
+            sc.vold[i] = make_float4(sc.dbg[nodes + i], sc.dbg[2 * nodes + i], sc.dbg[3 * nodes + i], 0.f);
+    }
+}
+
+__global__ void particlesCollisionKernel(const SceneDev* __restrict__ scenes, int parity, float dt) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    float* f = sc.buf[parity].f;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        float x[3], v[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            v[a] = f[(F_V + a) * cap + i];
+            x[a] = f[(F_X + a) * cap + i] + dt * v[a];
+        }
+        boundaryCollision(x, v, sc.origin, sc.target, sc.friction);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[(F_V + a) * cap + i] = v[a];
+    }
+}
+
+__global__ void advectKernel(const SceneDev* __restrict__ scenes, int parity, float dt) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    float* f = sc.buf[parity].f;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[(F_X + a) * cap + i] += dt * f[(F_V + a) * cap + i];
+}
+
+// initialize(): V0 = m / (sum_i m_i w_ip / h^3) with node masses in vstar.w
+// (src/mpm_solver3d.cu:173-214).  Live order, dense node reads.
+template <int S>
+__global__ void volumeKernel(const SceneDev* __restrict__ scenes, int parity) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    float* f = sc.buf[parity].f;
+    const size_t cap = sc.cap;
+    const float h = sc.h;
+    const float inv_cell_vol = (float)(1.0 / (double)(h * h * h));
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        float x[3] = {f[F_X * cap + i], f[(F_X + 1) * cap + i], f[(F_X + 2) * cap + i]};
+        int base[3];
+        float dens = 0.f;
+        if (stencilBase(sc, x, base)) {
+            float w[3][S];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                    w[a][k] = splineN<S>(__fdiv_rn(__fsub_rn(x[a], gp), h));
+                }
+            for (int c = 0; c < S; ++c)
+                for (int b = 0; b < S; ++b)
+                    for (int a = 0; a < S; ++a) {
+                        int n[3] = {base[0] + a, base[1] + b, base[2] + c};
+                        if (n[0] < 0 || n[1] < 0 || n[2] < 0 || n[0] >= sc.res[0] || n[1] >= sc.res[1] ||
+                            n[2] >= sc.res[2])
+                            continue;
+                        size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);
+                        float wgt = w[0][a] * w[1][b] * w[2][c];
+                        dens += (sc.vstar[node].w * wgt) * inv_cell_vol;
+                    }
+        }
+        f[F_VOL * cap + i] = f[F_MASS * cap + i] / dens;
+    }
+}
+
+// Scatter a live-order particle field back to the original order.
+__global__ void gatherFieldKernel(const SceneDev* __restrict__ scenes, int scene, int parity, int field, int comps,
+                                  int mode, float* __restrict__ out) {
+    const SceneDev& sc = scenes[scene];
+    const float* f = sc.buf[parity].f;
+    const uint32_t* pid = sc.buf[parity].pid;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        const uint32_t o = pid[i];
+        if (mode == 1) {  // position4
+#pragma unroll
+            for (int a = 0; a < 3; ++a) out[4 * (size_t)o + a] = f[(F_X + a) * cap + i];
+            out[4 * (size_t)o + 3] = 1.0f;
+        } else if (mode == 2) {  // det of a 3x3 field
+            float M[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) M[k] = f[(field + k) * cap + i];
+            out[o] = det3(M);
+        } else {
+            for (int c = 0; c < comps; ++c) out[(size_t)comps * o + c] = f[(field + c) * cap + i];
+        }
+    }
+}
+
+// Overwrite a live-order particle field from original-order data.
+__global__ void scatterFieldKernel(const SceneDev* __restrict__ scenes, int scene, int parity, int field, int comps,
+                                   const float* __restrict__ in) {
+    const SceneDev& sc = scenes[scene];
+    float* f = sc.buf[parity].f;
+    const uint32_t* pid = sc.buf[parity].pid;
+    const size_t cap = sc.cap;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        const uint32_t o = pid[i];
+        for (int c = 0; c < comps; ++c) f[(field + c) * cap + i] = in[(size_t)comps * o + c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launch wrappers (host).
+// ---------------------------------------------------------------------------
+void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err) {
+    noteLaunches(1);
+    keyKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, keys, block_count, err);
+}
+
+void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks) {
+    noteLaunches(2);
+    unsigned grid = (unsigned)std::min<size_t>((total_blocks + kThreads - 1) / kThreads, (size_t)c.num_sms * 8);
+    if (grid == 0) grid = 1;
+    packBlocksKernel<<<grid, kThreads, 0, c.stream>>>(bb.block_count, bb.packed, total_blocks, bb.scene_block_base,
+                                                      c.nscenes, bb.counters);
+    exclusiveScan<unsigned long long>(bb.packed, bb.scanned, total_blocks, bb.scan_partials64, bb.total64, c.stream);
+    compactBlocksKernel<<<grid, kThreads, 0, c.stream>>>(bb.packed, bb.scanned, bb.total64, total_blocks,
+                                                         bb.scene_block_base, c.nscenes, bb.active, bb.outside,
+                                                         bb.counters, bb.block_slot, bb.block_count);
+}
+
+void launchStress(const LaunchCtx& c, int parity) {
+    noteLaunches(1);
+    stressKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity);
+}
+
+template <int S, int MODE>
+static void setP2GAttr() {
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(p2gKernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)P2GLayout<S, MODE>::smemBytes);
+        done = true;
+    }
+}
+
+template <int S, int MODE>
+static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
+    setP2GAttr<S, MODE>();
+    p2gKernel<S, MODE><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE>::smemBytes, c.stream>>>(a, want);
+}
+
+void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer) {
+    noteLaunches(1);
+#define P2G_CASE(SS)                                                                   \
+    if (S == SS) {                                                                     \
+        switch (mode) {                                                                \
+            case MODE_APIC_FUSED: p2gOne<SS, MODE_APIC_FUSED>(c, a, want_transfer); break; \
+            case MODE_FLIP: p2gOne<SS, MODE_FLIP>(c, a, want_transfer); break;         \
+            case MODE_SPLIT: p2gOne<SS, MODE_SPLIT>(c, a, want_transfer); break;       \
+            default: p2gOne<SS, MODE_MASS>(c, a, want_transfer); break;                \
+        }                                                                              \
+    }
+    P2G_CASE(2) P2G_CASE(3) P2G_CASE(4)
+#undef P2G_CASE
+}
+
+void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer) {
+    noteLaunches(1);
+#define GRID_CASE(SS)                                                                                         \
+    if (S == SS) {                                                                                            \
+        switch (mode) {                                                                                       \
+            case MODE_APIC_FUSED: gridKernel<SS, MODE_APIC_FUSED><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, want_transfer); break; \
+            case MODE_FLIP: gridKernel<SS, MODE_FLIP><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, want_transfer); break; \
+            case MODE_SPLIT: gridKernel<SS, MODE_SPLIT><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, want_transfer); break; \
+            default: gridKernel<SS, MODE_MASS><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, want_transfer); break; \
+        }                                                                                                     \
+    }
+    GRID_CASE(2) GRID_CASE(3) GRID_CASE(4)
+#undef GRID_CASE
+}
+
+void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused) {
+    noteLaunches(1);
+#define G2P_CASE(SS)                                                                                   \
+    if (S == SS) {                                                                                     \
+        if (apic) g2pKernel<SS, true><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, fused ? 1 : 0); \
+        else g2pKernel<SS, false><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, fused ? 1 : 0);     \
+    }
+    G2P_CASE(2) G2P_CASE(3) G2P_CASE(4)
+#undef G2P_CASE
+}
+
+void launchDenseGravity(const LaunchCtx& c) {
+    noteLaunches(1);
+    denseGravityKernel<<<dim3(c.node_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes);
+}
+void launchDenseUpdate(const LaunchCtx& c, float dt) {
+    noteLaunches(1);
+    denseUpdateVelocityKernel<<<dim3(c.node_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, dt);
+}
+void launchDenseCollision(const LaunchCtx& c, float dt) {
+    noteLaunches(1);
+    denseCollisionKernel<<<dim3(c.node_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, dt);
+}
+void launchDensePack(const LaunchCtx& c) {
+    noteLaunches(1);
+    densePackKernel<<<dim3(c.node_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes);
+}
+void launchParticlesCollision(const LaunchCtx& c, int parity, float dt) {
+    noteLaunches(1);
+    particlesCollisionKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, dt);
+}
+void launchAdvect(const LaunchCtx& c, int parity, float dt) {
+    noteLaunches(1);
+    advectKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, dt);
+}
+void launchVolume(const LaunchCtx& c, int parity, int S) {
+    noteLaunches(1);
+    dim3 g(c.particle_blocks, c.nscenes);
+    if (S == 2) volumeKernel<2><<<g, kThreads, 0, c.stream>>>(c.scenes, parity);
+    else if (S == 3) volumeKernel<3><<<g, kThreads, 0, c.stream>>>(c.scenes, parity);
+    else volumeKernel<4><<<g, kThreads, 0, c.stream>>>(c.scenes, parity);
+}
+void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out) {
+    noteLaunches(1);
+    gatherFieldKernel<<<c.particle_blocks, kThreads, 0, c.stream>>>(c.scenes, scene, parity, field, comps, mode, out);
+}
+void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in) {
+    noteLaunches(1);
+    scatterFieldKernel<<<c.particle_blocks, kThreads, 0, c.stream>>>(c.scenes, scene, parity, field, comps, in);
+}
+
+size_t p2gSmemBytes(int S, int mode) {
+#define SM_CASE(SS)                                                          \
+    if (S == SS) {                                                           \
+        switch (mode) {                                                      \
+            case MODE_APIC_FUSED: return P2GLayout<SS, MODE_APIC_FUSED>::smemBytes; \
+            case MODE_FLIP: return P2GLayout<SS, MODE_FLIP>::smemBytes;       \
+            case MODE_SPLIT: return P2GLayout<SS, MODE_SPLIT>::smemBytes;     \
+            default: return P2GLayout<SS, MODE_MASS>::smemBytes;              \
+        }                                                                    \
+    }
+    SM_CASE(2) SM_CASE(3) SM_CASE(4)
+#undef SM_CASE
+    return 0;
+}
+
+}  // namespace mpm

@@ -1,0 +1,258 @@
+// mpm_math.cuh -- per-particle math of the snow step, FP32, register resident.
+//
+// Splines follow Interpolator3D (src/interpolation3d.cu:88-142), the 3x3 SVD
+// follows the method of the reference's 3x3_SVD_CUDA dependency (McAdams,
+// Selle, Tamstorf, Teran, Sifakis, UW-Madison CS TR-1690, 2011), boundary
+// collision follows applyBoundaryCollision (src/collision_object3d.cu:7-54).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace mpm {
+
+constexpr float kFltEps = 1.1920928955078125e-07f;  // std::numeric_limits<float>::epsilon()
+constexpr int kSvdSweeps = 6;
+
+// ---------------------------------------------------------------------------
+// 1D B-spline kernels.  d is the signed distance in cells.  Where the
+// reference's double-literal expression can be reproduced exactly in FP32
+// (linear, quadratic) it is; the cubic forms are within ~2 ulp of it.
+// ---------------------------------------------------------------------------
+template <int S>
+__device__ __forceinline__ float splineN(float d);
+template <int S>
+__device__ __forceinline__ float splineNDot(float d);
+
+template <>
+__device__ __forceinline__ float splineN<2>(float d) {
+    float t = fabsf(d);
+    return t < 1.0f ? 1.0f - t : 0.0f;
+}
+template <>
+__device__ __forceinline__ float splineNDot<2>(float d) {
+    float t = fabsf(d);
+    return (t < 1.0f && t > kFltEps) ? -d / t : 0.0f;
+}
+template <>
+__device__ __forceinline__ float splineN<3>(float d) {
+    float t = fabsf(d);
+    if (t < 0.5f) return __fsub_rn(0.75f, __fmul_rn(t, t));
+    if (t < 1.5f) {
+        float u = 1.5f - t;  // exact
+        return __fmul_rn(0.5f, __fmul_rn(u, u));
+    }
+    return 0.0f;
+}
+template <>
+__device__ __forceinline__ float splineNDot<3>(float d) {
+    float t = fabsf(d);
+    if (t < 0.5f) return -2.0f * d;
+    if (t < 1.5f) return __fsub_rn(d, copysignf(1.5f, d));
+    return 0.0f;
+}
+template <>
+__device__ __forceinline__ float splineN<4>(float d) {
+    float t = fabsf(d);
+    if (t < 1.0f) return fmaf(fmaf(0.5f, t, -1.0f) * t, t, 0.66666666666666667f);
+    if (t < 2.0f) {
+        float u = 2.0f - t;
+        return u * u * u * 0.16666666666666667f;
+    }
+    return 0.0f;
+}
+template <>
+__device__ __forceinline__ float splineNDot<4>(float d) {
+    float t = fabsf(d);
+    if (t < 1.0f) return d * fmaf(1.5f, t, -2.0f);
+    if (t < 2.0f) {
+        float u = 2.0f - t;
+        return -copysignf(0.5f * u * u, d);  // -sign(d) (2-|d|)^2 / 2
+    }
+    return 0.0f;
+}
+
+template <int S>
+__device__ __forceinline__ float splineRange() {
+    return S == 2 ? 1.0f : (S == 3 ? 1.5f : 2.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Small row-major 3x3 helpers.
+// ---------------------------------------------------------------------------
+struct M3 {
+    float a[9];
+};
+
+__device__ __forceinline__ float det3(const float* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+           m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+__device__ __forceinline__ void matmul3(const float* A, const float* B, float* C) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            C[3 * i + j] = fmaf(A[3 * i + 2], B[6 + j], fmaf(A[3 * i + 1], B[3 + j], A[3 * i] * B[j]));
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 SVD, McAdams et al. 2011: Jacobi eigen-analysis of A^T A with
+// approximate Givens rotations, sort of the columns of A V with sign fixes,
+// Givens QR.  The reference's library runs 4 Jacobi sweeps; for nearly equal
+// singular values (Fe close to a rotation, the common case in snow) 4 sweeps
+// leave off-diagonal residues up to ~1e-5, so 6 are run here.  A = U diag(s) V^T, U and V rotations, s sorted by
+// decreasing magnitude, s[2] carrying the sign of det(A).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void jacobiRotate(float (&S)[3][3], float* V, int p, int q) {
+    const float gamma = 5.82842712474619f;  // 3 + 2 sqrt(2)
+    const float cstar = 0.923879532511287f;  // cos(pi/8)
+    const float sstar = 0.382683432365090f;  // sin(pi/8)
+    float ch = 2.0f * (S[p][p] - S[q][q]);
+    float sh = S[p][q];
+    bool b = gamma * sh * sh < ch * ch;
+    float w = rsqrtf(fmaf(ch, ch, sh * sh));
+    ch = b ? w * ch : cstar;
+    sh = b ? w * sh : sstar;
+    float c = fmaf(ch, ch, -sh * sh);
+    float s = 2.0f * ch * sh;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float sp = S[k][p], sq = S[k][q];
+        S[k][p] = fmaf(c, sp, s * sq);
+        S[k][q] = fmaf(-s, sp, c * sq);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float sp = S[p][k], sq = S[q][k];
+        S[p][k] = fmaf(c, sp, s * sq);
+        S[q][k] = fmaf(-s, sp, c * sq);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float vp = V[3 * k + p], vq = V[3 * k + q];
+        V[3 * k + p] = fmaf(c, vp, s * vq);
+        V[3 * k + q] = fmaf(-s, vp, c * vq);
+    }
+}
+
+__device__ __forceinline__ void condSwapNeg(bool cond, float* B, float* V, int i, int j) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float bi = B[3 * k + i], bj = B[3 * k + j];
+        B[3 * k + i] = cond ? bj : bi;
+        B[3 * k + j] = cond ? -bi : bj;
+        float vi = V[3 * k + i], vj = V[3 * k + j];
+        V[3 * k + i] = cond ? vj : vi;
+        V[3 * k + j] = cond ? -vi : vj;
+    }
+}
+
+__device__ __forceinline__ void qrRotate(float* B, float* U, int p, int q) {
+    const float eps = 1e-6f;
+    float a1 = B[3 * p + p], a2 = B[3 * q + p];
+    float rho2 = fmaf(a1, a1, a2 * a2);
+    float rho = sqrtf(rho2);
+    float sh = rho > eps ? a2 : 0.0f;
+    float ch = fabsf(a1) + fmaxf(rho, eps);
+    bool neg = a1 < 0.0f;
+    float t = ch;
+    ch = neg ? sh : ch;
+    sh = neg ? t : sh;
+    float w = rsqrtf(fmaf(ch, ch, sh * sh));
+    ch *= w;
+    sh *= w;
+    float c = fmaf(ch, ch, -sh * sh);
+    float s = 2.0f * ch * sh;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float bp = B[3 * p + k], bq = B[3 * q + k];
+        B[3 * p + k] = fmaf(c, bp, s * bq);
+        B[3 * q + k] = fmaf(-s, bp, c * bq);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float up = U[3 * k + p], uq = U[3 * k + q];
+        U[3 * k + p] = fmaf(c, up, s * uq);
+        U[3 * k + q] = fmaf(-s, up, c * uq);
+    }
+}
+
+__device__ __forceinline__ void svd3(const float* A, float* U, float* s, float* V) {
+    float S[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            S[i][j] = fmaf(A[6 + i], A[6 + j], fmaf(A[3 + i], A[3 + j], A[i] * A[j]));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
+#pragma unroll
+    for (int sweep = 0; sweep < kSvdSweeps; ++sweep) {
+        jacobiRotate(S, V, 0, 1);
+        jacobiRotate(S, V, 1, 2);
+        jacobiRotate(S, V, 0, 2);
+    }
+    float B[9];
+    matmul3(A, V, B);
+    float r0 = fmaf(B[6], B[6], fmaf(B[3], B[3], B[0] * B[0]));
+    float r1 = fmaf(B[7], B[7], fmaf(B[4], B[4], B[1] * B[1]));
+    float r2 = fmaf(B[8], B[8], fmaf(B[5], B[5], B[2] * B[2]));
+    bool c01 = r0 < r1;
+    condSwapNeg(c01, B, V, 0, 1);
+    float t = r0;
+    r0 = c01 ? r1 : r0;
+    r1 = c01 ? t : r1;
+    bool c02 = r0 < r2;
+    condSwapNeg(c02, B, V, 0, 2);
+    t = r0;
+    r0 = c02 ? r2 : r0;
+    r2 = c02 ? t : r2;
+    bool c12 = r1 < r2;
+    condSwapNeg(c12, B, V, 1, 2);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) U[k] = (k % 4 == 0) ? 1.0f : 0.0f;
+    qrRotate(B, U, 0, 1);
+    qrRotate(B, U, 0, 2);
+    qrRotate(B, U, 1, 2);
+    s[0] = B[0];
+    s[1] = B[4];
+    s[2] = B[8];
+}
+
+// ---------------------------------------------------------------------------
+// applyBoundaryCollision (src/collision_object3d.cu:7-54).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void boundaryCollision(const float* pos, float* vel, const float* lo, const float* hi,
+                                                  float friction) {
+    float n[3] = {0.f, 0.f, 0.f};
+    bool collided = false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (pos[i] <= lo[i] + kFltEps) {
+            collided = true;
+            n[i] = 1.0f;
+        }
+        if (pos[i] >= hi[i] - kFltEps) {
+            collided = true;
+            n[i] = -1.0f;
+        }
+    }
+    if (!collided) return;
+    float vn = vel[0] * n[0] + vel[1] * n[1] + vel[2] * n[2];
+    if (vn >= kFltEps) return;
+    float vt[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) vt[i] = vel[i] - vn * n[i];
+    float vtn = sqrtf(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+    if (vtn <= -friction * vn + kFltEps) {
+        vel[0] = vel[1] = vel[2] = 0.0f;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) vel[i] = vt[i] + friction * vn * (vt[i] / vtn);
+    }
+}
+
+}  // namespace mpm

@@ -1,0 +1,250 @@
+// sort.cu -- stable LSD radix sort of particle keys and device-wide scans.
+//
+// Replaces the reference's unordered global atomics (src/mpm_solver3d.cu:
+// 277-286): particles are ordered by (block, cell) key every step so that the
+// P2G scatter can be done per block in a fixed order.  The sort is stable
+// (ties keep their previous order), hence bit-exact and deterministic.
+//
+// Per 8-bit digit: upsweep (per-tile digit histogram), exclusive scan of the
+// digit-major histogram, downsweep (warp match_any ranking, stable scatter).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "engine_host.hpp"
+
+namespace mpm {
+
+namespace {
+
+constexpr int kScanItems = 16;                      // per thread
+constexpr int kScanChunk = kThreads * kScanItems;   // 4096 per CTA
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kThreads * kSortItems;    // 4096 keys per tile
+
+template <class T>
+__device__ __forceinline__ T warpInclusiveScan(T x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Exclusive scan across the 256 threads of a CTA; returns the CTA total in *total.
+template <class T>
+__device__ __forceinline__ T blockExclusiveScan(T x, T* total) {
+    __shared__ T warp_tot[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = warpInclusiveScan(x);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T t = lane < kWarps ? warp_tot[lane] : T(0);
+        T ti = warpInclusiveScan(t);
+        if (lane < kWarps) warp_tot[lane] = ti - t;
+        // CTA total: inclusive value at the last warp
+        T tl = __shfl_sync(0xffffffffu, ti, kWarps - 1);
+        if (lane == 0) *total = tl;
+    }
+    __syncthreads();
+    T r = inc - x + warp_tot[warp];
+    __syncthreads();
+    return r;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) scanReduceKernel(const T* in, size_t n, T* partials) {
+    size_t base = (size_t)blockIdx.x * kScanChunk;
+    T s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        size_t i = base + (size_t)j * kThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    __shared__ T tot;
+    (void)blockExclusiveScan(s, &tot);
+    if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+}
+
+// Single CTA exclusive scan of up to kScanChunk partials; writes the grand
+// total to *total (if non-null).
+template <class T>
+__global__ void __launch_bounds__(kThreads) scanPartialsKernel(T* partials, int m, T* total) {
+    T v[kScanItems];
+    T s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        int i = threadIdx.x * kScanItems + j;
+        v[j] = i < m ? partials[i] : T(0);
+        s += v[j];
+    }
+    __shared__ T tot;
+    T run = blockExclusiveScan(s, &tot);
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        int i = threadIdx.x * kScanItems + j;
+        if (i < m) partials[i] = run;
+        run += v[j];
+    }
+    if (threadIdx.x == 0 && total) *total = tot;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) scanDownsweepKernel(const T* in, T* out, size_t n, const T* partials) {
+    size_t base = (size_t)blockIdx.x * kScanChunk + (size_t)threadIdx.x * kScanItems;
+    T v[kScanItems];
+    T s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        size_t i = base + j;
+        v[j] = i < n ? in[i] : T(0);
+        s += v[j];
+    }
+    __shared__ T tot;
+    T run = blockExclusiveScan(s, &tot) + partials[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        size_t i = base + j;
+        if (i < n) out[i] = run;
+        run += v[j];
+    }
+}
+
+// --- radix sort -------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) radixUpsweepKernel(const uint32_t* __restrict__ keys, uint32_t n,
+                                                                int shift, uint32_t mask, uint32_t* __restrict__ hist,
+                                                                int ntiles) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    size_t base = (size_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int j = 0; j < kSortItems; ++j) {
+        size_t i = base + (size_t)j * kThreads + threadIdx.x;
+        bool valid = i < n;
+        uint32_t d = valid ? (keys[i] >> shift) & mask : 0xffffffffu;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+template <bool kIdentVals>
+__global__ void __launch_bounds__(kThreads) radixDownsweepKernel(const uint32_t* __restrict__ keys_in,
+                                                                  const uint32_t* __restrict__ vals_in,
+                                                                  uint32_t* __restrict__ keys_out,
+                                                                  uint32_t* __restrict__ vals_out,
+                                                                  const uint32_t* __restrict__ offsets, uint32_t n,
+                                                                  int shift, uint32_t mask, int ntiles) {
+    __shared__ uint32_t cnt[kWarps][256];
+    for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const size_t base = (size_t)blockIdx.x * kSortTile + (size_t)warp * 32 * kSortItems;
+    uint32_t k[kSortItems], v[kSortItems], r[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        size_t i = base + (size_t)j * 32 + lane;
+        bool valid = i < n;
+        k[j] = valid ? keys_in[i] : 0u;
+        v[j] = valid ? (kIdentVals ? (uint32_t)i : vals_in[i]) : 0u;
+        uint32_t d = valid ? (k[j] >> shift) & mask : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        int leader = __ffs(peers) - 1;
+        uint32_t before = valid ? cnt[warp][d] : 0u;
+        r[j] = before + __popc(peers & lt);
+        __syncwarp();
+        if (valid && lane == leader) cnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            uint32_t c = cnt[w][threadIdx.x];
+            cnt[w][threadIdx.x] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        size_t i = base + (size_t)j * 32 + lane;
+        if (i < n) {
+            uint32_t d = (k[j] >> shift) & mask;
+            uint32_t pos = offsets[(size_t)d * ntiles + blockIdx.x] + cnt[warp][d] + r[j];
+            keys_out[pos] = k[j];
+            vals_out[pos] = v[j];
+        }
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host wrappers.
+// ---------------------------------------------------------------------------
+size_t scanScratchElems(size_t n) { return (n + kScanChunk - 1) / kScanChunk; }
+
+template <class T>
+cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    size_t chunks = (n + kScanChunk - 1) / kScanChunk;
+    if (chunks > (size_t)kScanChunk) return cudaErrorInvalidValue;
+    noteLaunches(3);
+    scanReduceKernel<T><<<(unsigned)chunks, kThreads, 0, st>>>(in, n, partials);
+    scanPartialsKernel<T><<<1, kThreads, 0, st>>>(partials, (int)chunks, total);
+    scanDownsweepKernel<T><<<(unsigned)chunks, kThreads, 0, st>>>(in, out, n, partials);
+    return cudaGetLastError();
+}
+
+template cudaError_t exclusiveScan<uint32_t>(const uint32_t*, uint32_t*, size_t, uint32_t*, uint32_t*, cudaStream_t);
+template cudaError_t exclusiveScan<unsigned long long>(const unsigned long long*, unsigned long long*, size_t,
+                                                        unsigned long long*, unsigned long long*, cudaStream_t);
+
+size_t radixTiles(size_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+// Sorts (keys_a, identity values) by the low `bits` bits of the keys.
+// Returns in *result_in_b whether the sorted arrays ended in (keys_b, vals_b).
+cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
+                           int bits, uint32_t* hist, uint32_t* scan_partials, bool* result_in_b, cudaStream_t st) {
+    *result_in_b = false;
+    if (n == 0) return cudaSuccess;
+    int ntiles = (int)radixTiles(n);
+    uint32_t *kin = keys_a, *vin = vals_a, *kout = keys_b, *vout = vals_b;
+    bool first = true;
+    for (int shift = 0; shift < bits || first; shift += 8) {
+        int pass_bits = bits - shift < 8 ? bits - shift : 8;
+        if (pass_bits <= 0) pass_bits = 1;
+        uint32_t mask = (1u << pass_bits) - 1u;
+        noteLaunches(2);
+        radixUpsweepKernel<<<ntiles, kThreads, 0, st>>>(kin, (uint32_t)n, shift, mask, hist, ntiles);
+        cudaError_t e = exclusiveScan<uint32_t>(hist, hist, (size_t)256 * ntiles, scan_partials, nullptr, st);
+        if (e != cudaSuccess) return e;
+        if (first)
+            radixDownsweepKernel<true><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, hist, (uint32_t)n, shift, mask,
+                                                                    ntiles);
+        else
+            radixDownsweepKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, hist, (uint32_t)n, shift,
+                                                                     mask, ntiles);
+        first = false;
+        uint32_t* t = kin;
+        kin = kout;
+        kout = t;
+        t = vin;
+        vin = vout;
+        vout = t;
+        *result_in_b = !*result_in_b;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace mpm

@@ -1,0 +1,356 @@
+"""GPU parity: the sm_100a step against the CPU oracle, through the C ABI.
+
+Tolerances (norm-wise relative, max|gpu - oracle| / max|oracle|) follow the
+stated targets: grid mass and momentum 1e-6; particle positions, velocities
+and det(Fe)/det(Fp) 1e-5 after one step; forces and B carry the FP32 SVD's
+error of the stress and use 1e-4.  Integer work (sorting) is bit-exact.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import relerr
+from mpm_b200 import _abi, scenes
+from mpm_b200.solver import APICMPMSolver3D, Material, MPMSolver3D, Particles
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+COMBOS = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2)]  # (transfer, interpolation)
+
+
+def _sort(keys, bits):
+    lib = _abi.load()
+    keys = np.ascontiguousarray(keys, np.uint32)
+    n = keys.size
+    sk = np.empty(n, np.uint32)
+    pm = np.empty(n, np.uint32)
+    P = C.POINTER(C.c_uint32)
+    _abi.check(lib.mpm_sort_keys(keys.ctypes.data_as(P), n, bits, sk.ctypes.data_as(P), pm.ctypes.data_as(P)),
+               "mpm_sort_keys")
+    return sk, pm
+
+
+@pytest.mark.parametrize("n,bits,kind", [(1, 8, "rand"), (4095, 12, "rand"), (4097, 22, "dup"),
+                                         (100_003, 22, "nearly"), (1_000_000, 24, "dup"), (65536, 32, "rand"),
+                                         (50_000, 1, "rand")])
+def test_radix_sort_bit_exact(gpu, n, bits, kind):
+    rng = np.random.default_rng(n + bits)
+    hi = (1 << bits) if bits < 32 else (1 << 32)
+    if kind == "rand":
+        keys = rng.integers(0, hi, n, dtype=np.uint64).astype(np.uint32)
+    elif kind == "dup":
+        keys = rng.integers(0, 64, n, dtype=np.uint64).astype(np.uint32) * (hi // 64 - 1)
+    else:  # nearly sorted with local swaps, like keys between steps
+        keys = np.sort(rng.integers(0, hi, n, dtype=np.uint64)).astype(np.uint32)
+        idx = rng.integers(0, n - 1, n // 20)
+        keys[idx], keys[idx + 1] = keys[idx + 1].copy(), keys[idx].copy()
+    sk, pm = _sort(keys, bits)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(pm, order.astype(np.uint32))
+    assert np.array_equal(sk, keys[order])
+
+
+def _nontrivial_state(sc, seed=0, B_scale=5.0):
+    rng = np.random.default_rng(seed)
+    n = sc.n
+    Fe = np.eye(3)[None] + 0.01 * rng.normal(size=(n, 3, 3))
+    Fp = np.eye(3)[None] + 0.002 * rng.normal(size=(n, 3, 3))
+    B = B_scale * sc.stride ** 2 * rng.normal(size=(n, 3, 3))
+    return Fe.astype(np.float32), Fp.astype(np.float32), B.astype(np.float32)
+
+
+def _pair(sc, seed=0, bits=64):
+    """GPU solver and oracle from the same input, with the same non-trivial Fe/Fp/B."""
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=bits)
+    Fe, Fp, B = _nontrivial_state(sc, seed)
+    for field, val in ((_abi.FIELD_FE, Fe), (_abi.FIELD_FP, Fp)) + (
+            ((_abi.FIELD_B, B),) if sc.transfer == _abi.TRANSFER_APIC else ()):
+        g.upload(field, val.reshape(sc.n, -1))
+        o.set(field, val.reshape(sc.n, -1).astype(np.float64))
+    return g, o
+
+
+@pytest.mark.parametrize("transfer,interp", COMBOS)
+def test_initial_volume_matches_oracle(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=3000, res=24, transfer=transfer, interpolation=interp)
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    assert relerr(g.download(_abi.FIELD_VOLUME0), o.get(_abi.FIELD_VOLUME0)) < 1e-6
+
+
+@pytest.mark.parametrize("transfer,interp", COMBOS)
+def test_p2g_grid_matches_oracle(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=4000, res=24, transfer=transfer, interpolation=interp)
+    g, o = _pair(sc)
+    g.resetGrid()
+    g.particlesToGrid()
+    o.reset_grid()
+    o.particles_to_grid()
+    gm = g.download_grid(_abi.GRID_MASS)
+    om = o.grid(_abi.GRID_MASS)
+    assert relerr(gm, om) < 1e-6
+    # per-node relative error of non-negligible nodes
+    big = om > 1e-3 * om.max()
+    assert np.abs(gm[big] - om[big]).max() / om[big].min() < 1e-3
+    assert np.max(np.abs(gm[big] / om[big] - 1)) < 1e-5
+    assert relerr(g.download_grid(_abi.GRID_VELOCITY), o.grid(_abi.GRID_VELOCITY)) < 1e-6
+    assert relerr(g.download_grid(_abi.GRID_FORCE), o.grid(_abi.GRID_FORCE)) < 1e-4
+    # total mass = total particle mass (partition of unity)
+    assert abs(gm.astype(np.float64).sum() / sc.particles.mass.astype(np.float64).sum() - 1) < 1e-5
+
+
+@pytest.mark.parametrize("transfer,interp", COMBOS)
+def test_grid_update_matches_oracle(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=4000, res=24, transfer=transfer, interpolation=interp)
+    g, o = _pair(sc, seed=1)
+    dt = sc.dt
+    for fn in ("resetGrid", "particlesToGrid", "computeExternalForces"):
+        getattr(g, fn)()
+    g.updateGridVelocities(dt)
+    g.gridCollision(dt)
+    o.reset_grid()
+    o.particles_to_grid()
+    o.gravity()
+    o.update_grid_velocities(dt)
+    o.grid_collision(dt)
+    # v = p/m carries no stress but divides the 1e-6 momentum error by light
+    # node masses; v* = v + dt f/m inherits the FP32 stress error of f (1e-4,
+    # the force tolerance above)
+    assert relerr(g.download_grid(_abi.GRID_VELOCITY), o.grid(_abi.GRID_VELOCITY)) < 1e-5
+    assert relerr(g.download_grid(_abi.GRID_VELOCITY_STAR), o.grid(_abi.GRID_VELOCITY_STAR)) < 1e-4
+
+
+def _particle_fields(transfer):
+    f = [_abi.FIELD_POSITION, _abi.FIELD_VELOCITY, _abi.FIELD_DET_FE, _abi.FIELD_DET_FP, _abi.FIELD_FE, _abi.FIELD_FP]
+    return f + ([_abi.FIELD_B] if transfer == _abi.TRANSFER_APIC else [])
+
+
+TOL = {_abi.FIELD_POSITION: 1e-5, _abi.FIELD_VELOCITY: 1e-5, _abi.FIELD_DET_FE: 1e-5, _abi.FIELD_DET_FP: 1e-5,
+       _abi.FIELD_FE: 1e-5, _abi.FIELD_FP: 1e-5, _abi.FIELD_B: 1e-4}
+
+
+@pytest.mark.parametrize("transfer,interp", COMBOS)
+def test_split_substeps_match_oracle(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=4000, res=24, transfer=transfer, interpolation=interp)
+    g, o = _pair(sc, seed=2)
+    dt = sc.dt
+    g.resetGrid()
+    g.particlesToGrid()
+    g.computeExternalForces()
+    g.updateGridVelocities(dt)
+    g.gridCollision(dt)
+    g.solveLinearSystem(dt)
+    if transfer == _abi.TRANSFER_APIC:
+        g.gridToParticles(dt)
+    else:
+        g.gridToParticles(dt, sc.blend)
+    g.advectParticles(dt)
+    o.reset_grid()
+    o.particles_to_grid()
+    o.gravity()
+    o.update_grid_velocities(dt)
+    o.grid_collision(dt)
+    o.grid_to_particles(dt, sc.blend)
+    o.advect(dt)
+    for f in _particle_fields(transfer):
+        assert relerr(g.download(f), o.get(f)) < TOL[f], f
+
+
+@pytest.mark.parametrize("transfer,interp", COMBOS)
+def test_fused_step_matches_oracle(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=4000, res=24, transfer=transfer, interpolation=interp)
+    g, o = _pair(sc, seed=3)
+    g.step(1)
+    o.step(1)
+    for f in _particle_fields(transfer):
+        assert relerr(g.download(f), o.get(f)) < TOL[f], f
+
+
+@pytest.mark.parametrize("transfer,interp", [(0, 1), (1, 2)])
+def test_hundred_steps_bound(gpu, transfer, interp):
+    """After 100 steps positions stay within 1e-4 of the FP64 oracle and
+    det(Fe), det(Fp) within 1e-3 (chaotic growth of FP32 round-off)."""
+    sc = scenes.tiny_scene(n=3000, res=24, transfer=transfer, interpolation=interp)
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    g.step(100)
+    o.step(100)
+    assert relerr(g.download(_abi.FIELD_POSITION), o.get(_abi.FIELD_POSITION)) < 1e-4
+    assert relerr(g.download(_abi.FIELD_VELOCITY), o.get(_abi.FIELD_VELOCITY)) < 1e-2
+    assert relerr(g.download(_abi.FIELD_DET_FE), o.get(_abi.FIELD_DET_FE)) < 1e-3
+    assert relerr(g.download(_abi.FIELD_DET_FP), o.get(_abi.FIELD_DET_FP)) < 1e-3
+
+
+@pytest.mark.parametrize("transfer,interp", [(0, 1), (1, 2)])
+def test_bitwise_deterministic(gpu, transfer, interp):
+    sc = scenes.tiny_scene(n=20000, res=32, transfer=transfer, interpolation=interp)
+    a, b = sc.solver(), sc.solver()
+    a.step(20)
+    b.step(20)
+    for f in _particle_fields(transfer):
+        assert np.array_equal(a.download(f), b.download(f)), f
+
+
+def test_mass_conserved_exactly(gpu):
+    sc = scenes.snow_cube(n=20000)
+    g = sc.solver()
+    m0 = g.download(_abi.FIELD_MASS)
+    g.step(30)
+    assert np.array_equal(g.download(_abi.FIELD_MASS), m0)
+    assert np.array_equal(m0, sc.particles.mass)
+
+
+def test_apic_momentum_conserved(gpu):
+    sc = scenes.tiny_scene(n=5000, res=32, transfer=1, interpolation=2, gravity=0.0)
+    sc.particles.materials[0].youngs_modulus = 0.0
+    sc.particles.velocities = np.random.default_rng(9).normal(size=(sc.n, 3)).astype(np.float32)
+    sc.particles.mass = np.full(sc.n, 10.0, np.float32)
+    g = sc.solver()
+    m = g.download(_abi.FIELD_MASS).astype(np.float64)
+    p0 = (m[:, None] * g.download(_abi.FIELD_VELOCITY)).sum(0)
+    g.step(5)
+    p1 = (m[:, None] * g.download(_abi.FIELD_VELOCITY)).sum(0)
+    assert np.abs(p1 - p0).max() < 1e-5 * np.abs(p0).max()
+
+
+def test_particles_collision_toggle_matches_oracle(gpu):
+    sc = scenes.tiny_scene(n=2000, res=16, transfer=0, interpolation=1, velocity=(-30.0, 5.0, 0.0))
+    sc.particles.positions[:, 0] -= 0.25  # touch the lower x wall
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    assert not g._enable_particles_collision
+    g.switchIfEnableParticlesCollision()
+    assert g._enable_particles_collision
+    o.set_particles_collision(True)
+    g.step(3)
+    o.step(3)
+    assert relerr(g.download(_abi.FIELD_VELOCITY), o.get(_abi.FIELD_VELOCITY)) < 1e-5
+    assert relerr(g.download(_abi.FIELD_POSITION), o.get(_abi.FIELD_POSITION)) < 1e-5
+
+
+@pytest.mark.parametrize("boundary", [_abi.BOUNDARY_REFERENCE, _abi.BOUNDARY_STICKY])
+def test_boundary_modes_match_oracle(gpu, boundary):
+    sc = scenes.tiny_scene(n=3000, res=16, transfer=1, interpolation=1, boundary=boundary,
+                           velocity=(0.0, -40.0, 0.0))
+    sc.particles.positions[:, 1] -= 0.22  # near the floor
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    g.step(2)
+    o.step(2)
+    assert relerr(g.download(_abi.FIELD_VELOCITY), o.get(_abi.FIELD_VELOCITY)) < 1e-5
+
+
+def test_neo_hookean_and_two_materials_match_oracle(gpu):
+    rng = np.random.default_rng(10)
+    n = 3000
+    x = (0.3 + 0.3 * rng.random((n, 3))).astype(np.float32)
+    mats = [Material(model=_abi.MODEL_NEO_HOOKEAN), Material(critical_compression=5e-2, critical_stretch=9e-3)]
+    p = Particles(x, (0.3, -1.0, 0.2), 0.0036, mats, (np.arange(n) % 2).astype(np.uint16))
+    g = APICMPMSolver3D(p, (0, 0, 0), (24, 24, 24), 1 / 24, 0.9, _abi.INTERP_CUBIC, 1e-4)
+    o = O.OracleSolver(g._desc, p, bits=64)
+    g.step(1)
+    o.step(1)
+    for f in (_abi.FIELD_POSITION, _abi.FIELD_VELOCITY, _abi.FIELD_DET_FE, _abi.FIELD_DET_FP):
+        assert relerr(g.download(f), o.get(f)) < 1e-5, f
+    g.step(2)
+    o.step(2)
+    for f in (_abi.FIELD_POSITION, _abi.FIELD_VELOCITY, _abi.FIELD_DET_FE, _abi.FIELD_DET_FP):
+        assert relerr(g.download(f), o.get(f)) < 5e-5, f
+
+
+def test_particles_outside_the_grid(gpu):
+    # stencils that miss the grid contribute nothing (src/mpm_solver3d.cu:259-264)
+    sc = scenes.tiny_scene(n=1000, res=16, transfer=0, interpolation=2)
+    sc.particles.positions[:10] = np.array([5.0, 5.0, 5.0], np.float32)
+    sc.particles.positions[10:20] = np.array([-3.0, 0.5, 0.5], np.float32)
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    g.step(2)
+    o.step(2)
+    assert relerr(g.download(_abi.FIELD_POSITION), o.get(_abi.FIELD_POSITION)) < 1e-5
+    assert relerr(g.download(_abi.FIELD_VELOCITY), o.get(_abi.FIELD_VELOCITY)) < 1e-5
+
+
+def test_nan_input_reports_numeric_error(gpu):
+    # a non-finite input position is reported by the first device pass over the
+    # particles (the volume initialization inside the constructor)
+    sc = scenes.tiny_scene(n=500, res=16)
+    sc.particles.positions[7] = np.nan
+    with pytest.raises(_abi.MPMError) as e:
+        g = sc.solver()
+        g.step(1)
+        g.synchronize()
+    assert e.value.status == 6
+
+
+def test_nan_during_run_reports_numeric_error(gpu):
+    # a state that turns non-finite mid-run (host-injected NaN velocity) is
+    # reported by synchronize() after the step that produced it
+    sc = scenes.tiny_scene(n=500, res=16)
+    g = sc.solver()
+    g.step(2)
+    v = g.download(_abi.FIELD_VELOCITY)
+    v[11] = np.inf
+    g.upload(_abi.FIELD_VELOCITY, v)
+    g.step(1)
+    with pytest.raises(_abi.MPMError) as e:
+        g.synchronize()
+    assert e.value.status == 6
+    g.synchronize()  # the flag is cleared once reported
+
+
+def test_empty_scene(gpu):
+    p = Particles(np.zeros((0, 3), np.float32), (0, 0, 0), 1.0)
+    g = MPMSolver3D(p, (0, 0, 0), (8, 8, 8), 1 / 8, 0.9, 0.95, 1, 1e-4)
+    g.step(3)
+    g.synchronize()
+    assert g.download(_abi.FIELD_POSITION).shape == (0, 3)
+
+
+def test_position4_and_upload_roundtrip(gpu):
+    sc = scenes.tiny_scene(n=777, res=16)
+    g = sc.solver()
+    g.step(4)
+    x = g.download(_abi.FIELD_POSITION)
+    x4 = g.download(_abi.FIELD_POSITION4)
+    assert np.array_equal(x4[:, :3], x) and np.all(x4[:, 3] == 1.0)
+    v = np.random.default_rng(0).normal(size=(sc.n, 3)).astype(np.float32)
+    g.upload(_abi.FIELD_VELOCITY, v)
+    assert np.array_equal(g.download(_abi.FIELD_VELOCITY), v)
+
+
+def test_golden_fixtures_on_gpu(gpu):
+    """The GPU reproduces the committed FP64 oracle fixtures within tolerance."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "oracle_golden.json")
+    for case in json.load(open(path))["cases"]:
+        if case["bits"] != 64:
+            continue
+        sc = scenes.tiny_scene(seed=case["seed"], n=case["n"], res=case["res"], transfer=case["transfer"],
+                               interpolation=case["interp"])
+        g = sc.solver()
+        g.step(case["steps"])
+        x = g.download(_abi.FIELD_POSITION).reshape(-1)[: len(case["x"])]
+        v = g.download(_abi.FIELD_VELOCITY).reshape(-1)[: len(case["v"])]
+        assert relerr(x, case["x"]) < 1e-5, case["name"]
+        assert relerr(v, case["v"]) < 1e-4, case["name"]
+
+
+@pytest.mark.parametrize("name", ["snow_cube", "two_balls"])
+def test_full_size_configs_properties(gpu, name):
+    """Full benchmark sizes: finite state, exact mass, bounded deformation."""
+    sc = scenes.snow_cube() if name == "snow_cube" else scenes.two_balls()
+    g = sc.solver()
+    g.step(10)
+    g.synchronize()
+    x = g.download(_abi.FIELD_POSITION)
+    assert np.isfinite(x).all()
+    assert np.array_equal(g.download(_abi.FIELD_MASS), sc.particles.mass)
+    dFe = g.download(_abi.FIELD_DET_FE)
+    lo = (1 - 2.5e-2) ** 3 * 0.999
+    hi = (1 + 7.5e-3) ** 3 * 1.001
+    assert dFe.min() >= lo and dFe.max() <= hi

@@ -238,6 +238,25 @@ MPM_API mpm_status mpm_solver_upload(mpm_solver* s, int32_t field, const float* 
 MPM_API mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, uint32_t* sorted_keys,
                                  uint32_t* perm);
 
+/* The same stable sort for callers that cannot allocate device memory: no
+ * counterpart in the reference.  Some callers own all device memory
+ * themselves -- a host application with its own pool or a budget fixed at
+ * start-up, or a loop that must not risk the implicit device synchronization
+ * of cudaMalloc/cudaFree -- and hand the library only buffers they allocated.
+ * Here `keys` (n inputs, only read), `sorted_keys` and `perm` (n outputs)
+ * are device pointers from the caller, `stream` is a cudaStream_t (NULL for
+ * the default stream), and the call is asynchronous on that stream.  The
+ * call allocates nothing: its working memory is one fixed device array
+ * inside the library that every GPU loading the library keeps until the
+ * process exits.  Limits: n <= MPM_SORT_NOALLOC_MAX_KEYS (larger n is
+ * rejected with MPM_ERR_INVALID_ARG); all calls share the array, so calls
+ * that overlap on the GPU race -- keep them on one stream.  The first call on
+ * each device resolves the array's device address (cudaGetSymbolAddress), so
+ * make that first call during set-up. */
+#define MPM_SORT_NOALLOC_MAX_KEYS (1u << 20)
+MPM_API mpm_status mpm_sort_keys_device_noalloc(const uint32_t* keys, uint32_t n, int32_t bits,
+                                                uint32_t* sorted_keys, uint32_t* perm, void* stream);
+
 /* Run nsteps steps bracketed by CUDA events recorded on the solver's own
  * stream and return the device time in *ms (synchronizes).  Used by the
  * benchmark; same work as mpm_solver_step. */

@@ -90,6 +90,8 @@ SIGNATURES = {
     "mpm_solver_profile_read": (C.c_int, [_P, _F, C.POINTER(C.c_int32), C.c_int32]),
     "mpm_sort_keys": (C.c_int, [C.POINTER(C.c_uint32), C.c_size_t, C.c_int32, C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32)]),
+    "mpm_sort_keys_device_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
+                                               C.c_void_p]),
     "mpm_set_device": (C.c_int, [C.c_int32]),
     "mpm_solver_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
     "mpm_batch_stats": (C.c_int, [_P, C.POINTER(StepStats)]),

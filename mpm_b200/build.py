@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xcompiler", "-ffp-contract=off"]
 
-SOURCES = ["sort.cu", "kernels.cu", "engine.cu"]
+SOURCES = ["sort.cu", "kernels.cu", "engine.cu", "sort_noalloc.cu"]
 
 
 def _headers():

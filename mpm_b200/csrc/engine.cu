@@ -31,6 +31,9 @@ static mpm_status fail(mpm_status st, const std::string& msg) {
     return st;
 }
 
+// Error recording for entry points defined in other translation units.
+mpm_status recordError(mpm_status st, const char* msg) { return fail(st, msg ? msg : ""); }
+
 #define CUDA_TRY(call)                                                                                 \
     do {                                                                                               \
         cudaError_t e_ = (call);                                                                       \

@@ -247,4 +247,41 @@ cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b,
     return cudaGetLastError();
 }
 
+// Same sort with every buffer supplied by the caller: `in_keys` is only read,
+// the result always lands in (out_keys, out_vals), and (tmp_keys, tmp_vals)
+// is the other ping-pong pair.  The pass count decides which pair the first
+// pass writes so that the last pass writes the output pair.
+cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint32_t* out_vals, uint32_t* tmp_keys,
+                               uint32_t* tmp_vals, size_t n, int bits, uint32_t* hist, uint32_t* scan_partials,
+                               cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const int ntiles = (int)radixTiles(n);
+    const int passes = bits <= 8 ? 1 : (bits + 7) / 8;
+    uint32_t* dk[2] = {out_keys, tmp_keys};
+    uint32_t* dv[2] = {out_vals, tmp_vals};
+    int dst = (passes % 2 == 1) ? 0 : 1;
+    const uint32_t* kin = in_keys;
+    const uint32_t* vin = nullptr;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        int pass_bits = bits - shift < 8 ? bits - shift : 8;
+        if (pass_bits <= 0) pass_bits = 1;
+        const uint32_t mask = (1u << pass_bits) - 1u;
+        noteLaunches(2);
+        radixUpsweepKernel<<<ntiles, kThreads, 0, st>>>(kin, (uint32_t)n, shift, mask, hist, ntiles);
+        cudaError_t e = exclusiveScan<uint32_t>(hist, hist, (size_t)256 * ntiles, scan_partials, nullptr, st);
+        if (e != cudaSuccess) return e;
+        if (p == 0)
+            radixDownsweepKernel<true><<<ntiles, kThreads, 0, st>>>(kin, nullptr, dk[dst], dv[dst], hist, (uint32_t)n,
+                                                                    shift, mask, ntiles);
+        else
+            radixDownsweepKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, dk[dst], dv[dst], hist, (uint32_t)n,
+                                                                     shift, mask, ntiles);
+        kin = dk[dst];
+        vin = dv[dst];
+        dst ^= 1;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace mpm

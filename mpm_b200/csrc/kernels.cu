@@ -18,6 +18,7 @@
 #include "mpm_math.cuh"
 
 #include <atomic>
+#include <cstdlib>
 
 namespace mpm {
 
@@ -28,6 +29,16 @@ uint64_t kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
 namespace {
 
 __device__ __forceinline__ float ldg(const float* p) { return __ldg(p); }
+
+// Asynchronous 4-byte global -> shared copies (cp.async, L1-allocating).
+__device__ __forceinline__ void cpAsync4(float* smem_dst, const float* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+constexpr int kPreStride = 19;  // odd: rows of consecutive threads fall in different banks
 
 // Stencil base ceil(x/h - r) per axis (src/mpm_solver3d.cu:252-255).  Returns
 // false when the stencil misses the grid in some axis (or x is not finite).
@@ -228,43 +239,54 @@ __global__ void __launch_bounds__(kThreads) stressKernel(const SceneDev* __restr
 
 // ---------------------------------------------------------------------------
 // P2G: one CTA per active 4^3-cell block (persistent loop).  Each warp takes
-// whole cells; its lanes own the S^3 stencil nodes of the cell and accumulate
-// the cell's particles in sorted order in registers.  Cell partial sums are
-// merged into the (S+3)^3 block tile by a fixed-order gather, and the tile is
-// written to scratch.  No floating-point atomics: bitwise deterministic.
+// whole cells (dynamically, cell by cell); its lanes own the S^3 stencil
+// nodes of the cell and accumulate the cell's particles, in sorted order, in
+// registers.  Cell partial sums are merged into the (S+3)^3 block tile by a
+// fixed-order gather, and the tile is written to scratch.  Which warp takes a
+// cell does not matter: every sum has a fixed order, no floating-point
+// atomics, bitwise deterministic.
+//
+// Staged payload of a particle (floats, 16-byte aligned rows):
+//   shared part (one broadcast float4 per 4 values)
+//     APIC / SPLIT : m, q[3] | hC[0..3] | hC[4..7] | hC[8], T[0..2] | T[3..5], -
+//                    q = m v - m C delta, hC = h m C (C = B D^-1), T = stress term
+//     PIC-FLIP     : m, m v[3] | T[0..3] | T[4..5], -, -
+//     MASS         : m, -, -, -
+//   weights: (N(d), N'(d)/h) pairs per axis and stencil offset (float2)
 // ---------------------------------------------------------------------------
-template <int S, int MODE>
+template <int S, int MODE, int STAGE = 16>
 struct P2GLayout {
     static constexpr int F = modeFields(MODE);
     static constexpr int NS = S * S * S;              // stencil nodes
     static constexpr int NJ = (NS + 31) / 32;         // nodes per lane
     static constexpr int TN = tileNodes(S);
     static constexpr int TJ = (TN + kThreads - 1) / kThreads;
-    // staged payload per particle: w[3][S], dw[3][S], then mode extras
-    static constexpr int OW = 0, ODW = 3 * S;
-    static constexpr int OM = (MODE == MODE_MASS) ? 3 * S : 6 * S;
-    static constexpr int OQ = OM + 1;   // q or m v (3)
-    static constexpr int OHC = OQ + 3;  // h m C (9)
-    static constexpr int OT = (MODE == MODE_FLIP) ? OQ + 3 : OHC + 9;  // stress term (6)
-    static constexpr int RAW = (MODE == MODE_MASS) ? OM + 1 : OT + 6;
-    static constexpr int P = RAW | 1;   // odd stride: conflict-free staging writes
-    static constexpr int kCells = 32;   // cells per half-block
-    static constexpr size_t smemFloats = (size_t)kWarps * 32 * P + (size_t)kCells * F * 64;
-    static constexpr size_t smemBytes = smemFloats * 4 + 3 * 64 * 4;
+    static constexpr int SH = (MODE == MODE_MASS) ? 4 : (MODE == MODE_FLIP ? 12 : 20);  // shared floats
+    static constexpr int WB = SH;                     // weight pairs start
+    static constexpr int P = ((SH + 6 * S) + 3) / 4 * 4;
+    static constexpr int kStage = STAGE;              // particles staged per warp round
+    static constexpr int kCells = 32;                 // cells per half-block
+    static constexpr size_t smemFloats = (size_t)kWarps * kStage * P + (size_t)kCells * F * 64;
+    static constexpr size_t smemBytes = smemFloats * 4 + 4 * 64 * 4;
 };
 
-template <int S, int MODE>
-__global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_transfer) {
-    using L = P2GLayout<S, MODE>;
+template <int S, int MODE, int STAGE>
+__global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want_transfer) {
+    using L = P2GLayout<S, MODE, STAGE>;
     constexpr int F = L::F;
-    extern __shared__ float smem[];
-    float* stage = smem;                                     // [warp][32][P]
-    float* partial = smem + (size_t)kWarps * 32 * L::P;      // [cell][F][64]
+    extern __shared__ float4 smem4[];
+    float* smem = reinterpret_cast<float*>(smem4);
+    float* stage = smem;                                        // [warp][kStage][P]
+    float* partial = smem + (size_t)kWarps * L::kStage * L::P;  // [cell][F][64]
     int* cellBeg = (int*)(partial + (size_t)L::kCells * F * 64);
     int* cellEnd = cellBeg + 64;
     int* cellNonEmpty = cellEnd + 64;
+    int* nextCell = cellNonEmpty + 64;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // lane -> stencil node(s): (a, b, c) and, for S = 4, (a, b, c + 2)
+    const int na = lane % S, nb = (lane / S) % S, nc = lane / (S * S);
+    const bool lane_on = lane < L::NS;
     const uint32_t nact = args.counters[0];
     for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
         const BlockItem it = args.active[w];
@@ -272,14 +294,10 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
         const float* pf = sc.buf[args.parity].f;
         const size_t cap = sc.cap;
-        const uint32_t lb = it.block - sc.block_base;
-        const int bx = (int)(lb % (uint32_t)sc.nb[0]);
-        const int by = (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]);
-        const int bz = (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]));
-        const int t0[3] = {4 * bx - 4, 4 * by - 4, 4 * bz - 4};
 
         // Cell ranges inside the block (keys are sorted by cell).
         for (int c = threadIdx.x; c < 64; c += kThreads) cellBeg[c] = cellEnd[c] = 0;
+        if (threadIdx.x < 2) nextCell[threadIdx.x] = 0;
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
             uint32_t g = it.start + i;
@@ -296,20 +314,25 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
 #pragma unroll
             for (int f = 0; f < F; ++f) tacc[j][f] = 0.f;
 
-        const float dt = sc.dt, h = sc.h;
+        const float dt = sc.dt, h = sc.h, inv_h = sc.inv_h;
         for (int half = 0; half < 2; ++half) {
-            // ---- particle phase: warp per cell ----
-            for (int cl = warp; cl < L::kCells; cl += kWarps) {
+            // ---- particle phase: warps take cells dynamically ----
+            float* st = stage + (size_t)warp * L::kStage * L::P;
+            while (true) {
+                int cl = 0;
+                if (lane == 0) cl = atomicAdd(&nextCell[half], 1);
+                cl = __shfl_sync(0xffffffffu, cl, 0);
+                if (cl >= L::kCells) break;
                 const int cell = half * 32 + cl;
                 const int beg = cellBeg[cell], end = cellEnd[cell];
+                if (end <= beg) continue;
                 float acc[L::NJ][F];
 #pragma unroll
                 for (int j = 0; j < L::NJ; ++j)
 #pragma unroll
                     for (int f = 0; f < F; ++f) acc[j][f] = 0.f;
-                float* st = stage + (size_t)warp * 32 * L::P;
-                for (int g0 = beg; g0 < end; g0 += 32) {
-                    const int np = min(32, end - g0);
+                for (int g0 = beg; g0 < end; g0 += L::kStage) {
+                    const int np = min(L::kStage, end - g0);
                     if (lane < np) {
                         float* my = st + lane * L::P;
                         const uint32_t gs = it.start + (uint32_t)(g0 + lane);
@@ -326,30 +349,40 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
                         float delta[3];
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
-                            float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
+                            const float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
                             delta[a] = x[a] - gp0;
+                            // node distances as the reference forms them, (x_p - (o + h i)) / h
+                            float dk[S], wk[S], dwk[S];
 #pragma unroll
                             for (int k = 0; k < S; ++k) {
-                                float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
-                                float d = __fdiv_rn(__fsub_rn(x[a], gp), h);
-                                my[L::OW + a * S + k] = splineN<S>(d);
-                                if (MODE != MODE_MASS) my[L::ODW + a * S + k] = __fdiv_rn(splineNDot<S>(d), h);
+                                const float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                                dk[k] = __fdiv_rn(__fsub_rn(x[a], gp), h);
+                            }
+                            splineWeights<S>(dk, wk, dwk);
+#pragma unroll
+                            for (int k = 0; k < S; ++k) {
+                                if (MODE == MODE_MASS) {
+                                    my[L::WB + a * S + k] = wk[k];
+                                } else {
+                                    my[L::WB + 2 * (a * S + k)] = wk[k];
+                                    my[L::WB + 2 * (a * S + k) + 1] = dwk[k] * inv_h;
+                                }
                             }
                         }
                         const float m = bad ? 0.f : ldg(pf + F_MASS * cap + old);
-                        my[L::OM] = m;
+                        my[0] = m;
                         if (MODE != MODE_MASS) {
                             float v[3] = {ldg(pf + (F_V + 0) * cap + old), ldg(pf + (F_V + 1) * cap + old),
                                           ldg(pf + (F_V + 2) * cap + old)};
-                            float tau[6];
-#pragma unroll
-                            for (int k = 0; k < 6; ++k) tau[k] = ldg(pf + (F_TAU + k) * cap + old);
                             const float ts = bad ? 0.f : ((MODE == MODE_APIC_FUSED) ? -dt : -1.0f);
+                            float T[6];
 #pragma unroll
-                            for (int k = 0; k < 6; ++k) my[L::OT + k] = ts * tau[k];
+                            for (int k = 0; k < 6; ++k) T[k] = ts * ldg(pf + (F_TAU + k) * cap + old);
                             if (MODE == MODE_FLIP) {
 #pragma unroll
-                                for (int a = 0; a < 3; ++a) my[L::OQ + a] = m * v[a];
+                                for (int a = 0; a < 3; ++a) my[1 + a] = m * v[a];
+#pragma unroll
+                                for (int k = 0; k < 6; ++k) my[4 + k] = T[k];
                             } else {
                                 float mC[9];
                                 if (sc.transfer == MPM_TRANSFER_APIC) {
@@ -361,61 +394,80 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
                                     for (int k = 0; k < 9; ++k) mC[k] = 0.f;
                                 }
 #pragma unroll
-                                for (int a = 0; a < 3; ++a) {
-                                    my[L::OQ + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
-                                                                mC[3 * a + 2] * delta[2]);
+                                for (int a = 0; a < 3; ++a)
+                                    my[1 + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
+                                                            mC[3 * a + 2] * delta[2]);
 #pragma unroll
-                                    for (int b = 0; b < 3; ++b) my[L::OHC + 3 * a + b] = h * mC[3 * a + b];
-                                }
+                                for (int k = 0; k < 9; ++k) my[4 + k] = h * mC[k];
+#pragma unroll
+                                for (int k = 0; k < 6; ++k) my[13 + k] = T[k];
                             }
                         }
                     }
                     __syncwarp();
-                    for (int q = 0; q < np; ++q) {
-                        const float* pq = st + q * L::P;
-                        const float m = pq[L::OM];
+                    if (lane_on) {
+                        const float fa = (float)na, fb = (float)nb, fc = (float)nc;
+                        for (int q = 0; q < np; ++q) {
+                            const float* pq = st + q * L::P;
+                            const float4 s0 = *reinterpret_cast<const float4*>(pq);
+                            const float m = s0.x;
+                            if (MODE == MODE_MASS) {
+                                const float w = pq[L::WB + na] * pq[L::WB + S + nb];
 #pragma unroll
-                        for (int j = 0; j < L::NJ; ++j) {
-                            const int k = lane + 32 * j;
-                            if (k < L::NS) {
-                                const int a = k % S, b = (k / S) % S, c = k / (S * S);
-                                const float wa = pq[L::OW + a], wb = pq[L::OW + S + b], wc = pq[L::OW + 2 * S + c];
-                                const float wab = wa * wb;
-                                const float wgt = wab * wc;
+                                for (int j = 0; j < L::NJ; ++j)
+                                    acc[j][0] = fmaf(m * w, pq[L::WB + 2 * S + nc + 2 * j], acc[j][0]);
+                                continue;
+                            }
+                            const float2 xa = *reinterpret_cast<const float2*>(pq + L::WB + 2 * na);
+                            const float2 yb = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (S + nb));
+                            const float wab = xa.x * yb.x, dawb = xa.y * yb.x, wadb = xa.x * yb.y;
+                            float T[6], u[3], hc2[3];
+                            float hC[9];
+                            if (MODE == MODE_FLIP) {
+                                const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
+                                const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
+                                T[0] = s1.x; T[1] = s1.y; T[2] = s1.z; T[3] = s1.w; T[4] = s2.x; T[5] = s2.y;
+                                u[0] = s0.y; u[1] = s0.z; u[2] = s0.w;
+                            } else {
+                                const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
+                                const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
+                                const float4 s3 = *reinterpret_cast<const float4*>(pq + 12);
+                                const float4 s4 = *reinterpret_cast<const float4*>(pq + 16);
+                                hC[0] = s1.x; hC[1] = s1.y; hC[2] = s1.z; hC[3] = s1.w;
+                                hC[4] = s2.x; hC[5] = s2.y; hC[6] = s2.z; hC[7] = s2.w; hC[8] = s3.x;
+                                T[0] = s3.y; T[1] = s3.z; T[2] = s3.w; T[3] = s4.x; T[4] = s4.y; T[5] = s4.z;
+                                const float qv[3] = {s0.y, s0.z, s0.w};
+#pragma unroll
+                                for (int i = 0; i < 3; ++i) {
+                                    u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, fmaf(hC[3 * i + 2], fc, qv[i])));
+                                    hc2[i] = 2.0f * hC[3 * i + 2];
+                                }
+                            }
+#pragma unroll
+                            for (int j = 0; j < L::NJ; ++j) {
+                                if (j > 0 && lane + 32 * j >= L::NS) break;
+                                const float2 zc = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (2 * S + nc + 2 * j));
+                                const float wgt = wab * zc.x;
+                                const float gx = dawb * zc.x, gy = wadb * zc.x, gz = wab * zc.y;
+                                const float tg0 = fmaf(T[0], gx, fmaf(T[3], gy, T[4] * gz));
+                                const float tg1 = fmaf(T[3], gx, fmaf(T[1], gy, T[5] * gz));
+                                const float tg2 = fmaf(T[4], gx, fmaf(T[5], gy, T[2] * gz));
                                 acc[j][0] = fmaf(m, wgt, acc[j][0]);
-                                if (MODE != MODE_MASS) {
-                                    const float da = pq[L::ODW + a], db = pq[L::ODW + S + b], dc = pq[L::ODW + 2 * S + c];
-                                    const float gx = da * wb * wc, gy = wa * db * wc, gz = wab * dc;
-                                    const float* T = pq + L::OT;  // xx yy zz xy xz yz
-                                    const float tg0 = fmaf(T[0], gx, fmaf(T[3], gy, T[4] * gz));
-                                    const float tg1 = fmaf(T[3], gx, fmaf(T[1], gy, T[5] * gz));
-                                    const float tg2 = fmaf(T[4], gx, fmaf(T[5], gy, T[2] * gz));
-                                    if (MODE == MODE_FLIP) {
-                                        acc[j][1] = fmaf(wgt, pq[L::OQ + 0], acc[j][1]);
-                                        acc[j][2] = fmaf(wgt, pq[L::OQ + 1], acc[j][2]);
-                                        acc[j][3] = fmaf(wgt, pq[L::OQ + 2], acc[j][3]);
-                                        acc[j][4] += tg0;
-                                        acc[j][5] += tg1;
-                                        acc[j][6] += tg2;
-                                    } else {
-                                        const float fa = (float)a, fb = (float)b, fc = (float)c;
-                                        const float* hC = pq + L::OHC;
-                                        float u0 = fmaf(hC[0], fa, fmaf(hC[1], fb, fmaf(hC[2], fc, pq[L::OQ + 0])));
-                                        float u1 = fmaf(hC[3], fa, fmaf(hC[4], fb, fmaf(hC[5], fc, pq[L::OQ + 1])));
-                                        float u2 = fmaf(hC[6], fa, fmaf(hC[7], fb, fmaf(hC[8], fc, pq[L::OQ + 2])));
-                                        if (MODE == MODE_APIC_FUSED) {
-                                            acc[j][1] += fmaf(wgt, u0, tg0);
-                                            acc[j][2] += fmaf(wgt, u1, tg1);
-                                            acc[j][3] += fmaf(wgt, u2, tg2);
-                                        } else {  // MODE_SPLIT
-                                            acc[j][1] = fmaf(wgt, u0, acc[j][1]);
-                                            acc[j][2] = fmaf(wgt, u1, acc[j][2]);
-                                            acc[j][3] = fmaf(wgt, u2, acc[j][3]);
-                                            acc[j][4] += tg0;
-                                            acc[j][5] += tg1;
-                                            acc[j][6] += tg2;
-                                        }
-                                    }
+                                if (j > 0 && MODE != MODE_FLIP) {
+#pragma unroll
+                                    for (int i = 0; i < 3; ++i) u[i] += hc2[i];
+                                }
+                                if (MODE == MODE_APIC_FUSED) {
+                                    acc[j][1] += fmaf(wgt, u[0], tg0);
+                                    acc[j][2] += fmaf(wgt, u[1], tg1);
+                                    acc[j][3] += fmaf(wgt, u[2], tg2);
+                                } else {  // PIC-FLIP and SPLIT keep p and f apart
+                                    acc[j][1] = fmaf(wgt, u[0], acc[j][1]);
+                                    acc[j][2] = fmaf(wgt, u[1], acc[j][2]);
+                                    acc[j][3] = fmaf(wgt, u[2], acc[j][3]);
+                                    acc[j][4] += tg0;
+                                    acc[j][5] += tg1;
+                                    acc[j][6] += tg2;
                                 }
                             }
                         }
@@ -451,6 +503,7 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
                                 const int cell = (cz * 4 + cy) * 4 + cx;
                                 if (!cellNonEmpty[cell]) continue;
                                 const int cl = cell - half * 32;
+                                // stencil node index of the lane layout: a + S (b + S c)
                                 const int k = dx + S * (dy + S * dz);
                                 const float* pc = partial + (size_t)cl * F * 64 + k;
 #pragma unroll
@@ -470,9 +523,9 @@ __global__ void __launch_bounds__(kThreads) p2gKernel(StepArgs args, int want_tr
 #pragma unroll
                 for (int f = 0; f < F; ++f) tile[f * L::TN + tn] = tacc[j][f];
         }
-        (void)t0;
     }
 }
+
 
 // ---------------------------------------------------------------------------
 // Grid pass: merge the <= 8 overlapping tiles of every node in fixed order,
@@ -590,7 +643,8 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
 // ---------------------------------------------------------------------------
 template <int S, bool APIC>
 __device__ __forceinline__ void particleUpdate(const StepArgs& args, const SceneDev& sc, uint32_t gs,
-                                               const float4* tvs, const float4* tvo, const int* t0, bool fused) {
+                                               const float4* tvs, const float4* tvo, const int* t0, bool fused,
+                                               float* pre) {
     constexpr int T = S + 3;
     const float* pf = sc.buf[args.parity].f;
     float* nf = sc.buf[args.parity ^ 1].f;
@@ -601,6 +655,15 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
         atomicOr(args.err, ERR_INDEX);
         return;
     }
+    // Fe, Fp and V0 are needed only after the gather: start their copies into
+    // this thread's shared-memory row now so the loads overlap the gather.
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        cpAsync4(pre + k, pf + (F_FE + k) * cap + old);
+        cpAsync4(pre + 9 + k, pf + (F_FP + k) * cap + old);
+    }
+    cpAsync4(pre + 18, pf + F_VOL * cap + old);
+    cpAsyncCommit();
     const float h = sc.h, dt = sc.dt;
     float x[3], v[3];
 #pragma unroll
@@ -629,12 +692,14 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
             lo[a] = base[a] - t0[a];
             float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
             delta[a] = x[a] - gp0;
+            float dk[S];
+            dk[0] = __fdiv_rn(delta[a], h);
+#pragma unroll
+            for (int k = 1; k < S; ++k) dk[k] = dk[0] - (float)k;  // exact subtraction
+            splineWeights<S>(dk, w[a], dw[a]);
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-                float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
-                float d = __fdiv_rn(__fsub_rn(x[a], gp), h);
-                w[a][k] = splineN<S>(d);
-                dw[a][k] = __fdiv_rn(splineNDot<S>(d), h);
+                dw[a][k] *= sc.inv_h;
             }
         }
 #pragma unroll
@@ -693,10 +758,11 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
     }
     // Fe <- (I + dt grad v) Fe ; F = Fe Fp ; SVD clamp (src/material_point3d.cu:53-70).
     float Fe[9], Fp[9], A[9], Fn[9];
+    cpAsyncWaitAll();
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        Fe[k] = ldg(pf + (F_FE + k) * cap + old);
-        Fp[k] = ldg(pf + (F_FP + k) * cap + old);
+        Fe[k] = pre[k];
+        Fp[k] = pre[9 + k];
         A[k] = dt * gv[k] + ((k % 4 == 0) ? 1.0f : 0.0f);
     }
     matmul3(A, Fe, Fn);
@@ -739,7 +805,7 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
         for (int k = 0; k < 9; ++k) Fe[k] = Fn[k];
     }
     // Next step's stress from the clamped SVD (Fe = U S V^T exactly).
-    const float V0 = ldg(pf + F_VOL * cap + old);
+    const float V0 = pre[18];
     float mu, la, tau[6];
     plasticLame(m, Fp, mu, la);
     if (m.model == MPM_MODEL_NEO_HOOKEAN) {
@@ -797,11 +863,12 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
 }
 
 template <int S, bool APIC>
-__global__ void __launch_bounds__(kThreads) g2pKernel(StepArgs args, int fused) {
+__global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fused) {
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
     __shared__ float4 tvs[TN];
     __shared__ float4 tvo[APIC ? 1 : TN];
+    __shared__ float pre[kThreads * kPreStride];  // per-thread prefetch row: Fe, Fp, V0
     const int want = APIC ? MPM_TRANSFER_APIC : MPM_TRANSFER_PIC_FLIP;
     const uint32_t nact = args.counters[0];
     const uint32_t nout = args.counters[1];
@@ -828,7 +895,7 @@ __global__ void __launch_bounds__(kThreads) g2pKernel(StepArgs args, int fused) 
         }
         for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
             particleUpdate<S, APIC>(args, sc, it.start + i, inside ? tvs : nullptr, APIC ? nullptr : tvo, t0,
-                                    fused != 0);
+                                    fused != 0, pre + threadIdx.x * kPreStride);
         __syncthreads();
     }
 }
@@ -1021,20 +1088,37 @@ void launchStress(const LaunchCtx& c, int parity) {
     stressKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity);
 }
 
-template <int S, int MODE>
+template <int S, int MODE, int STAGE>
 static void setP2GAttr() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(p2gKernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)P2GLayout<S, MODE>::smemBytes);
+        cudaFuncSetAttribute(p2gKernel<S, MODE, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)P2GLayout<S, MODE, STAGE>::smemBytes);
         done = true;
     }
 }
 
+// Particles staged per warp round in P2G: 32 (default: all lanes stage, half
+// the per-particle staging cost; measured 0.212 vs 0.221 ms on the 1M-particle
+// cubic APIC scene) or 16 (smaller shared-memory footprint).  MPM_P2G_STAGE=16
+// selects the latter.
+static int p2gStage() {
+    static int v = [] {
+        const char* e = getenv("MPM_P2G_STAGE");
+        return (e && atoi(e) == 16) ? 16 : 32;
+    }();
+    return v;
+}
+
 template <int S, int MODE>
 static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
-    setP2GAttr<S, MODE>();
-    p2gKernel<S, MODE><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE>::smemBytes, c.stream>>>(a, want);
+    if (p2gStage() == 32) {
+        setP2GAttr<S, MODE, 32>();
+        p2gKernel<S, MODE, 32><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, 32>::smemBytes, c.stream>>>(a, want);
+    } else {
+        setP2GAttr<S, MODE, 16>();
+        p2gKernel<S, MODE, 16><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, 16>::smemBytes, c.stream>>>(a, want);
+    }
 }
 
 void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer) {

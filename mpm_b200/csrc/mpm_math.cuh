@@ -13,7 +13,7 @@
 namespace mpm {
 
 constexpr float kFltEps = 1.1920928955078125e-07f;  // std::numeric_limits<float>::epsilon()
-constexpr int kSvdSweeps = 6;
+constexpr int kSvdSweeps = 5;
 
 // ---------------------------------------------------------------------------
 // 1D B-spline kernels.  d is the signed distance in cells.  Where the
@@ -78,6 +78,59 @@ __device__ __forceinline__ float splineRange() {
     return S == 2 ? 1.0f : (S == 3 ? 1.5f : 2.0f);
 }
 
+// All S weights (and derivatives, in cells) of one axis for a stencil that
+// starts at base = ceil(x/h - r), so that d0 = x/h - base lies in (r-1, r].
+// Node k sits at distance d0 - k, whose sign and spline piece are known in
+// advance, so the piecewise kernels need no branches.  The values are those of
+// splineN / splineNDot (the pieces agree at their junctions); the linear
+// kernel keeps the branchy form for the reference's zero derivative at
+// |d| = 0 and |d| = 1.
+// d[k] is the distance (in cells) of stencil node k; pass d[k] = d[0] - k
+// when the per-node rounding of (x - o - h i)/h is not needed.
+template <int S>
+__device__ __forceinline__ void splineWeights(const float* d, float* w, float* dw);
+
+template <>
+__device__ __forceinline__ void splineWeights<2>(const float* d, float* w, float* dw) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        w[k] = splineN<2>(d[k]);
+        dw[k] = splineNDot<2>(d[k]);
+    }
+}
+
+template <>
+__device__ __forceinline__ void splineWeights<3>(const float* d, float* w, float* dw) {
+    // d0 in (0.5, 1.5] (outer piece), d1 in (-0.5, 0.5] (inner), d2 in (-1.5, -0.5] (outer)
+    const float u0 = 1.5f - d[0];        // >= 0
+    const float d1 = d[1];
+    const float u2 = 1.5f + d[2];        // 1.5 - |d2|, >= 0
+    w[0] = 0.5f * u0 * u0;
+    w[1] = 0.75f - d1 * d1;
+    w[2] = 0.5f * u2 * u2;
+    dw[0] = -u0;                          // d - 1.5 sign(d), d > 0
+    dw[1] = -2.0f * d1;
+    dw[2] = u2;                           // d + 1.5, d < 0
+}
+
+template <>
+__device__ __forceinline__ void splineWeights<4>(const float* d, float* w, float* dw) {
+    // d0 in (1, 2] (outer), d1 in (0, 1] (inner), d2 in (-1, 0] (inner), d3 in (-2, -1] (outer)
+    const float u0 = 2.0f - d[0];        // >= 0
+    const float t1 = d[1];               // |d1|
+    const float t2 = -d[2];              // |d2|
+    const float u3 = 2.0f + d[3];        // 2 - |d3|
+    const float sixth = 0.16666666666666667f, twothirds = 0.66666666666666667f;
+    w[0] = u0 * u0 * u0 * sixth;
+    w[1] = fmaf(fmaf(0.5f, t1, -1.0f) * t1, t1, twothirds);
+    w[2] = fmaf(fmaf(0.5f, t2, -1.0f) * t2, t2, twothirds);
+    w[3] = u3 * u3 * u3 * sixth;
+    dw[0] = -0.5f * u0 * u0;             // d > 0 outer: -(2-|d|)^2 / 2
+    dw[1] = t1 * fmaf(1.5f, t1, -2.0f);  // d > 0 inner: d (1.5|d| - 2)
+    dw[2] = -t2 * fmaf(1.5f, t2, -2.0f); // d <= 0 inner
+    dw[3] = 0.5f * u3 * u3;              // d < 0 outer: +(2-|d|)^2 / 2
+}
+
 // ---------------------------------------------------------------------------
 // Small row-major 3x3 helpers.
 // ---------------------------------------------------------------------------
@@ -103,7 +156,8 @@ __device__ __forceinline__ void matmul3(const float* A, const float* B, float* C
 // approximate Givens rotations, sort of the columns of A V with sign fixes,
 // Givens QR.  The reference's library runs 4 Jacobi sweeps; for nearly equal
 // singular values (Fe close to a rotation, the common case in snow) 4 sweeps
-// leave off-diagonal residues up to ~1e-5, so 6 are run here.  A = U diag(s) V^T, U and V rotations, s sorted by
+// can leave off-diagonal residues up to ~1e-5, so 5 are run here (the FP32
+// floor of the method, ~5e-7 reconstruction error, is reached by then).  A = U diag(s) V^T, U and V rotations, s sorted by
 // decreasing magnitude, s[2] carrying the sign of det(A).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void jacobiRotate(float (&S)[3][3], float* V, int p, int q) {
@@ -189,7 +243,7 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* s, float* 
             S[i][j] = fmaf(A[6 + i], A[6 + j], fmaf(A[3 + i], A[3 + j], A[i] * A[j]));
 #pragma unroll
     for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
-#pragma unroll
+#pragma unroll 1
     for (int sweep = 0; sweep < kSvdSweeps; ++sweep) {
         jacobiRotate(S, V, 0, 1);
         jacobiRotate(S, V, 1, 2);

@@ -78,7 +78,9 @@ def test_initial_volume_matches_oracle(gpu, transfer, interp):
     sc = scenes.tiny_scene(n=3000, res=24, transfer=transfer, interpolation=interp)
     g = sc.solver()
     o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
-    assert relerr(g.download(_abi.FIELD_VOLUME0), o.get(_abi.FIELD_VOLUME0)) < 1e-6
+    # V0 = m / (sum_i m_i w_ip / h^3) is a ratio of FP32 sums of up to ~100
+    # terms each (about 10 ulp): 3e-6
+    assert relerr(g.download(_abi.FIELD_VOLUME0), o.get(_abi.FIELD_VOLUME0)) < 3e-6
 
 
 @pytest.mark.parametrize("transfer,interp", COMBOS)

@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--workload", default="two_balls", choices=WORKLOADS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served legs")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-scale", type=float, default=0.02)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     return ap.parse_args()
 
@@ -256,6 +259,10 @@ def run_ours(args, ws, rank, local):
     if not args.no_e2e:
         e2e = run_e2e(sc, args.steps, ws)
 
+    forms = None
+    if not args.no_forms:
+        forms = run_forms(args, ws, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, threads, k, dt = cpu_rate(sc, args.cpu_budget_s)
@@ -268,9 +275,68 @@ def run_ours(args, ws, rank, local):
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                "config": config_of(sc, ws), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(launches1.value - launches0.value), "clocks": clk.summary(),
-               "stats": stats}
+               "stats": stats, "forms": forms}
         print(json.dumps(out), flush=True)
     g.close()
+
+
+def run_forms(args, ws, local):
+    """Batched vs plain on the 64-scene workload, and a served stream.
+
+    batched: the 64 seeded scenes (10k-500k particles, 32^3-128^3 grids,
+             half APIC / half PIC-FLIP, quadratic, dt 1e-4) in one Batch;
+    plain:   the same 64 scenes as 64 separate solvers stepped round-robin
+             (each on its own stream), i.e. the reference's API used per scene;
+    served:  a Poisson stream of scene requests (rate 20/s) replayed for
+             --serve-seconds with particle counts scaled by --serve-scale."""
+    from mpm_b200 import scenes
+    from mpm_b200.batch import Batch
+    from mpm_b200.serving import Server
+    out = {}
+    steps = min(args.steps, 100)
+    scs = scenes.batched_scenes()
+    ntot = sum(s.n for s in scs)
+    with Batch(device=local) as b:
+        for s in scs:
+            b.add(s)
+        b.step(3)
+        b.synchronize()
+        b.profile(True)
+        barrier(ws)
+        ms = b.timed_step(steps)
+        prof = b.profile_read()
+        st = b.stats()
+    t = allmax(ws, ms) / 1e3
+    out["batched"] = {"workload": "64 scenes, %d particles" % ntot, "steps": steps,
+                      "value": allsum(ws, float(ntot * steps)) / t, "ms_per_step": t / steps * 1e3,
+                      "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st}
+    solvers = [s.solver() for s in scs]
+    for g in solvers:
+        g.step(3)
+    for g in solvers:
+        g.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for g in solvers:
+            g.step(1)
+    for g in solvers:
+        g.synchronize()
+    t = allmax(ws, time.perf_counter() - t0)
+    for g in solvers:
+        g.close()
+    out["plain"] = {"workload": "same 64 scenes as 64 solvers", "steps": steps,
+                    "value": allsum(ws, float(ntot * steps)) / t, "ms_per_step": t / steps * 1e3}
+    out["batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
+    reqs = scenes.serving_requests(rate=20.0, duration=args.serve_seconds, scale=args.serve_scale)
+    srv = Server(budget_bytes=150e9, device=local, keep_state=False)
+    rep = srv.run(reqs, time_scale=1.0)
+    srv.close()
+    s = rep.summary()
+    s["stream"] = ("Poisson 20 req/s for %.0f s, particles log-uniform in [%d, %d], 100-500 steps each"
+                   % (args.serve_seconds, max(1, int(5000 * args.serve_scale)), int(2_000_000 * args.serve_scale)))
+    out["served"] = s
+    return out
 
 
 def run_e2e(sc, steps, ws):

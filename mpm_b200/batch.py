@@ -1,0 +1,105 @@
+"""Batched scenes over the C ABI of include/mpm_b200_batch.h.
+
+A Batch advances many independent scenes -- different particle counts,
+grids, transfers, splines and materials -- with one launch sequence per step
+(sort, block compaction, P2G, grid pass, G2P over the active blocks of every
+scene).  Scenes can be added and removed between steps; the serving loop
+(mpm_b200.serving) uses that for continuous batching.  The reference has no
+batching; each scene's result is bitwise the result of solving it alone.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+
+class Batch:
+    def __init__(self, device: int | None = None):
+        self._lib = _abi.load()
+        if _abi.device_count() < 1:
+            raise RuntimeError("mpm_b200 needs a CUDA device; there is no CPU fallback")
+        if device is not None:
+            check(self._lib.mpm_set_device(int(device)), "mpm_set_device")
+        h = C.c_void_p()
+        check(self._lib.mpm_batch_create(C.byref(h)), "mpm_batch_create")
+        self._h = h
+        self._n: Dict[int, int] = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mpm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, scene) -> int:
+        """Add a mpm_b200.scenes.Scene; returns its id."""
+        desc = scene.desc()
+        pin, keep = scene.particles.to_c()
+        sid = C.c_int32()
+        check(self._lib.mpm_batch_add_scene(self._h, C.byref(desc), C.byref(pin), C.byref(sid)),
+              "mpm_batch_add_scene")
+        del keep
+        self._n[int(sid.value)] = scene.n
+        return int(sid.value)
+
+    def remove(self, sid: int):
+        check(self._lib.mpm_batch_remove_scene(self._h, int(sid)), "mpm_batch_remove_scene")
+        self._n.pop(int(sid), None)
+
+    @property
+    def num_scenes(self) -> int:
+        return len(self._n)
+
+    @property
+    def num_particles(self) -> int:
+        return int(sum(self._n.values()))
+
+    def step(self, nsteps: int = 1):
+        check(self._lib.mpm_batch_step(self._h, int(nsteps)), "mpm_batch_step")
+
+    def synchronize(self):
+        check(self._lib.mpm_batch_synchronize(self._h), "mpm_batch_synchronize")
+
+    def timed_step(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(self._lib.mpm_batch_timed_step(self._h, int(nsteps), C.byref(ms)), "mpm_batch_timed_step")
+        return float(ms.value)
+
+    def download(self, sid: int, field: int) -> np.ndarray:
+        n = self._n[int(sid)]
+        comps = _abi.FIELD_COMPONENTS[field]
+        out = np.empty((n, comps), np.float32)
+        check(self._lib.mpm_batch_download(self._h, int(sid), int(field), out.ctypes.data_as(C.POINTER(C.c_float))),
+              "mpm_batch_download")
+        return out.reshape(n, 3, 3) if comps == 9 else (out[:, 0] if comps == 1 else out)
+
+    def stats(self) -> dict:
+        st = _abi.StepStats()
+        check(self._lib.mpm_batch_stats(self._h, C.byref(st)), "mpm_batch_stats")
+        return dict(active_blocks=st.active_blocks, outside_blocks=st.outside_blocks, active_nodes=st.active_nodes)
+
+    def profile(self, enable: bool = True):
+        check(self._lib.mpm_batch_profile(self._h, 1 if enable else 0), "mpm_batch_profile")
+
+    def profile_read(self) -> dict:
+        nf = len(_abi.KERNEL_FAMILIES)
+        ms = (C.c_float * nf)()
+        cnt = (C.c_int32 * nf)()
+        check(self._lib.mpm_batch_profile_read(self._h, ms, cnt, nf), "mpm_batch_profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_abi.KERNEL_FAMILIES)}

@@ -96,6 +96,7 @@ struct SceneHost {
     DevMem vstar, vold, dbg, mats;
     int nmat = 1;
     bool need_init = true;
+    bool stress_stale = true;  // cached tau must be recomputed from Fe/Fp
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
 };
 
@@ -236,10 +237,10 @@ public:
         sc->need_init = true;
         sc->id = next_id_++;
         *out_id = sc->id;
+        sc->stress_stale = true;
         scenes_.push_back(std::move(sc));
         dirty_ = true;
         keys_valid_ = false;
-        stress_valid_ = false;
         sorted_valid_ = false;
         return MPM_OK;
     }
@@ -352,9 +353,10 @@ public:
         MPM_TRY(total64_.alloc(sizeof(unsigned long long), "block scan total"));
         MPM_TRY(sbb_.alloc(sizeof(uint32_t) * (ns + 1), "scene block bases"));
         CUDA_TRY(cudaMemcpyAsync(sbb_.p, sbb.data(), sizeof(uint32_t) * (ns + 1), cudaMemcpyHostToDevice, stream_));
-        max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk));
+        // work items: one per non-empty block plus one per further kBlockChunk particles
+        max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
         MPM_TRY(active_.alloc(sizeof(BlockItem) * max_active_, "active blocks"));
-        MPM_TRY(outside_.alloc(sizeof(BlockItem) * std::max(ns, 1), "outside blocks"));
+        MPM_TRY(outside_.alloc(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
         MPM_TRY(counters_.alloc(sizeof(uint32_t) * 4, "counters"));
         CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 4, stream_));
         MPM_TRY(block_slot_.alloc(sizeof(int32_t) * tb, "block slots"));
@@ -543,21 +545,39 @@ public:
             CUDA_TRY(cudaGetLastError());
             keys_valid_ = false;  // block counts were consumed by the compaction
         }
-        for (auto& s : scenes_) s->need_init = false;
-        stress_valid_ = false;
+        for (auto& s : scenes_) {
+            if (all || s->need_init) s->stress_stale = true;  // V0 changed
+            s->need_init = false;
+        }
+        return MPM_OK;
+    }
+
+    // tau from Fe/Fp for the scenes whose cached stress is stale (new scenes,
+    // uploads, re-initialization).  Scenes whose tau came from the last G2P
+    // keep it, so a scene's trajectory does not depend on its batch-mates.
+    mpm_status refreshStress() {
+        bool any = false;
+        for (auto& s : scenes_) any |= s->stress_stale;
+        if (!any) return MPM_OK;
+        mark(KF_STRESS, 0);
+        LaunchCtx c = ctx();
+        for (size_t i = 0; i < scenes_.size(); ++i) {
+            if (!scenes_[i]->stress_stale) continue;
+            LaunchCtx one = c;
+            one.scenes = scenes_dev_.as<SceneDev>() + i;
+            one.nscenes = 1;
+            launchStress(one, parity_);
+            scenes_[i]->stress_stale = false;
+        }
+        mark(KF_STRESS, 1);
+        CUDA_TRY(cudaGetLastError());
         return MPM_OK;
     }
 
     // One fused simulateOneStep over every scene of the batch.
     mpm_status stepOnce() {
         MPM_TRY(sortLive());
-        if (!stress_valid_) {
-            mark(KF_STRESS, 0);
-            launchStress(ctx(), parity_);
-            mark(KF_STRESS, 1);
-            collect(KF_STRESS);
-            stress_valid_ = true;
-        }
+        MPM_TRY(refreshStress());
         const int next = 1 - sorted_;
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
         LaunchCtx c = ctx();
@@ -579,8 +599,7 @@ public:
         CUDA_TRY(cudaGetLastError());
         parity_ ^= 1;
         kcur_ = next;
-        keys_valid_ = true;   // G2P wrote next step's keys and block counts
-        stress_valid_ = true; // and next step's stress
+        keys_valid_ = true;   // G2P wrote next step's keys and block counts (and stress)
         sorted_valid_ = false;
         return MPM_OK;
     }
@@ -668,10 +687,7 @@ public:
         MPM_TRY(ensureReady());
         MPM_TRY(ensureDbg());
         MPM_TRY(sortLive());
-        if (!stress_valid_) {
-            launchStress(ctx(), parity_);
-            stress_valid_ = true;
-        }
+        MPM_TRY(refreshStress());
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
         LaunchCtx c = ctx();
         for (int S : stencilSizes()) {
@@ -707,10 +723,7 @@ public:
         MPM_TRY(ensureReady());
         MPM_TRY(ensureDbg());
         if (!sorted_valid_) MPM_TRY(sortLive());
-        if (!stress_valid_) {
-            launchStress(ctx(), parity_);
-            stress_valid_ = true;
-        }
+        MPM_TRY(refreshStress());
         launchDensePack(ctx());
         std::vector<SceneDev> saved = host_scenes_;
         for (auto& d : host_scenes_) {
@@ -727,7 +740,6 @@ public:
         parity_ ^= 1;
         keys_valid_ = false;
         sorted_valid_ = false;
-        stress_valid_ = true;
         return MPM_OK;
     }
     mpm_status particlesCollision(float dt) {
@@ -802,7 +814,7 @@ public:
         launchScatterField(ctx(), idx, parity_, base, comps, tmp_.as<float>());
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaStreamSynchronize(stream_));
-        stress_valid_ = false;
+        s.stress_stale = true;
         if (field == MPM_FIELD_POSITION) {
             keys_valid_ = false;
             sorted_valid_ = false;
@@ -880,7 +892,7 @@ private:
     std::vector<std::unique_ptr<SceneHost>> scenes_;
     std::vector<SceneDev> host_scenes_;
     int next_id_ = 0;
-    bool dirty_ = true, keys_valid_ = false, stress_valid_ = false, sorted_valid_ = false;
+    bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     int parity_ = 0, kcur_ = 0, sorted_ = 0;
     size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
     uint32_t total_blocks_ = 0;

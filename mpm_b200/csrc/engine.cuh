@@ -21,6 +21,10 @@ namespace mpm {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// Largest particle count of one P2G/G2P work item: denser blocks are split
+// into several items (each with its own P2G tile, merged in item order), so
+// one crowded block cannot serialize a whole step.
+constexpr uint32_t kBlockChunk = 4096;
 
 enum Field : int {
     F_X = 0,

@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(kThreads) packBlocksKernel(const uint32_t* __r
         uint32_t c = block_count[b];
         int s = sceneOfBlock(scene_block_base, nscenes, b);
         bool outside = (b == scene_block_base[s + 1] - 1);
-        unsigned long long flag = (c > 0 && !outside) ? 1ull : 0ull;
-        packed[b] = (flag << 32) | (unsigned long long)c;
+        // work items of at most kBlockChunk particles each
+        unsigned long long items = (c > 0 && !outside) ? (unsigned long long)((c + kBlockChunk - 1) / kBlockChunk) : 0ull;
+        packed[b] = (items << 32) | (unsigned long long)c;
     }
 }
 
@@ -197,15 +198,24 @@ __global__ void __launch_bounds__(kThreads) compactBlocksKernel(
         uint32_t count = (uint32_t)(v & 0xffffffffull);
         uint32_t start = (uint32_t)(s & 0xffffffffull);
         int scene = sceneOfBlock(scene_block_base, nscenes, b);
-        if (v >> 32) {
-            uint32_t slot = (uint32_t)(s >> 32);
-            active[slot] = BlockItem{b, start, count, (uint32_t)scene};
+        const uint32_t items = (uint32_t)(v >> 32);
+        if (items) {
+            // consecutive work items (and tile slots) of one block, in particle order
+            const uint32_t slot = (uint32_t)(s >> 32);
+            for (uint32_t j = 0; j < items; ++j) {
+                const uint32_t off = j * kBlockChunk;
+                active[slot + j] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
+            }
             block_slot[b] = (int32_t)slot;
         } else {
             block_slot[b] = -1;
             if (count > 0) {
-                uint32_t o = atomicAdd(&counters[1], 1u);
-                outside[o] = BlockItem{b, start, count, (uint32_t)scene};
+                const uint32_t nitems = (count + kBlockChunk - 1) / kBlockChunk;
+                const uint32_t o = atomicAdd(&counters[1], nitems);
+                for (uint32_t j = 0; j < nitems; ++j) {
+                    const uint32_t off = j * kBlockChunk;
+                    outside[o + j] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
+                }
             }
         }
         block_count[b] = 0;
@@ -265,9 +275,12 @@ struct P2GLayout {
     static constexpr int WB = SH;                     // weight pairs start
     static constexpr int P = ((SH + 6 * S) + 3) / 4 * 4;
     static constexpr int kStage = STAGE;              // particles staged per warp round
-    static constexpr int kCells = 32;                 // cells per half-block
-    static constexpr size_t smemFloats = (size_t)kWarps * kStage * P + (size_t)kCells * F * 64;
-    static constexpr size_t smemBytes = smemFloats * 4 + 4 * 64 * 4;
+    static constexpr int kSlots = 32;                 // segment partials per round
+    static constexpr int kSeg = 96;                   // particles per segment (at most)
+    static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg
+    static constexpr size_t smemFloats = (size_t)kWarps * kStage * P + (size_t)kSlots * F * 64;
+    static constexpr size_t smemBytes = smemFloats * 4 + (2 * 64 + 3 * kMaxSeg + 4) * 4;
+    static_assert(kMaxSeg >= 64 + (int)(kBlockChunk / kSeg) + 1, "segment list too small");
 };
 
 template <int S, int MODE, int STAGE>
@@ -277,11 +290,13 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
     extern __shared__ float4 smem4[];
     float* smem = reinterpret_cast<float*>(smem4);
     float* stage = smem;                                        // [warp][kStage][P]
-    float* partial = smem + (size_t)kWarps * L::kStage * L::P;  // [cell][F][64]
-    int* cellBeg = (int*)(partial + (size_t)L::kCells * F * 64);
+    float* partial = smem + (size_t)kWarps * L::kStage * L::P;  // [slot][F][64]
+    int* cellBeg = (int*)(partial + (size_t)L::kSlots * F * 64);
     int* cellEnd = cellBeg + 64;
-    int* cellNonEmpty = cellEnd + 64;
-    int* nextCell = cellNonEmpty + 64;
+    int* segCell = cellEnd + 64;                                // segment list, in cell order
+    int* segBeg = segCell + L::kMaxSeg;
+    int* segEnd = segBeg + L::kMaxSeg;
+    int* ctl = segEnd + L::kMaxSeg;                             // [0] segments, [1] next segment
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // lane -> stencil node(s): (a, b, c) and, for S = 4, (a, b, c + 2)
@@ -295,9 +310,8 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
         const float* pf = sc.buf[args.parity].f;
         const size_t cap = sc.cap;
 
-        // Cell ranges inside the block (keys are sorted by cell).
+        // Cell ranges inside the work item (keys are sorted by cell).
         for (int c = threadIdx.x; c < 64; c += kThreads) cellBeg[c] = cellEnd[c] = 0;
-        if (threadIdx.x < 2) nextCell[threadIdx.x] = 0;
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
             uint32_t g = it.start + i;
@@ -306,7 +320,37 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
             if (i == it.count - 1 || (args.sorted_keys[g + 1] & 63u) != c) cellEnd[c] = (int)i + 1;
         }
         __syncthreads();
-        for (int c = threadIdx.x; c < 64; c += kThreads) cellNonEmpty[c] = cellEnd[c] > cellBeg[c];
+        // Segment list: every non-empty cell cut into runs of at most kSeg
+        // particles, in cell order (warp 0; lane l owns cells 2l and 2l+1).
+        if (warp == 0) {
+            const int c0 = 2 * lane, c1 = 2 * lane + 1;
+            const int b0 = cellBeg[c0], e0 = cellEnd[c0], b1 = cellBeg[c1], e1 = cellEnd[c1];
+            const int n0 = e0 > b0 ? (e0 - b0 + L::kSeg - 1) / L::kSeg : 0;
+            const int n1 = e1 > b1 ? (e1 - b1 + L::kSeg - 1) / L::kSeg : 0;
+            int x = n0 + n1;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            int off = x - (n0 + n1);
+            for (int j = 0; j < n0; ++j, ++off) {
+                segCell[off] = c0;
+                segBeg[off] = b0 + j * L::kSeg;
+                segEnd[off] = min(e0, b0 + (j + 1) * L::kSeg);
+            }
+            for (int j = 0; j < n1; ++j, ++off) {
+                segCell[off] = c1;
+                segBeg[off] = b1 + j * L::kSeg;
+                segEnd[off] = min(e1, b1 + (j + 1) * L::kSeg);
+            }
+            if (lane == 31) {
+                ctl[0] = x;
+                ctl[1] = 0;
+            }
+        }
+        __syncthreads();
+        const int nseg = ctl[0];
 
         float tacc[L::TJ][F];
 #pragma unroll
@@ -315,17 +359,17 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
             for (int f = 0; f < F; ++f) tacc[j][f] = 0.f;
 
         const float dt = sc.dt, h = sc.h, inv_h = sc.inv_h;
-        for (int half = 0; half < 2; ++half) {
-            // ---- particle phase: warps take cells dynamically ----
+        for (int r0 = 0; r0 < nseg; r0 += L::kSlots) {
+            const int rend = min(nseg, r0 + L::kSlots);
+            // ---- particle phase: warps take segments of this round dynamically ----
             float* st = stage + (size_t)warp * L::kStage * L::P;
             while (true) {
-                int cl = 0;
-                if (lane == 0) cl = atomicAdd(&nextCell[half], 1);
-                cl = __shfl_sync(0xffffffffu, cl, 0);
-                if (cl >= L::kCells) break;
-                const int cell = half * 32 + cl;
-                const int beg = cellBeg[cell], end = cellEnd[cell];
-                if (end <= beg) continue;
+                int sg = 0;
+                if (lane == 0) sg = r0 + atomicAdd(&ctl[1], 1);
+                sg = __shfl_sync(0xffffffffu, sg, 0);
+                if (sg >= rend) break;
+                const int cl = sg - r0;  // partial slot
+                const int beg = segBeg[sg], end = segEnd[sg];
                 float acc[L::NJ][F];
 #pragma unroll
                 for (int j = 0; j < L::NJ; ++j)
@@ -484,32 +528,22 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                 }
             }
             __syncthreads();
-            // ---- gather phase: fixed-order merge of this half's cells ----
+            if (threadIdx.x == 0) ctl[1] = 0;  // next round's dynamic counter (no warp reads it until the barrier below)
+            // ---- gather phase: fixed-order merge of this round's segments ----
 #pragma unroll
             for (int j = 0; j < L::TJ; ++j) {
                 const int tn = threadIdx.x + j * kThreads;
                 if (tn < L::TN) {
                     const int tx = tn % (S + 3), ty = (tn / (S + 3)) % (S + 3), tz = tn / ((S + 3) * (S + 3));
+                    for (int sg = r0; sg < rend; ++sg) {
+                        const int cell = segCell[sg];
+                        const int dx = tx - (cell & 3), dy = ty - ((cell >> 2) & 3), dz = tz - (cell >> 4);
+                        if ((unsigned)dx >= (unsigned)S || (unsigned)dy >= (unsigned)S || (unsigned)dz >= (unsigned)S)
+                            continue;
+                        // stencil node index of the lane layout: a + S (b + S c)
+                        const float* pc = partial + (size_t)(sg - r0) * F * 64 + dx + S * (dy + S * dz);
 #pragma unroll
-                    for (int czl = 0; czl < 2; ++czl) {
-                        const int cz = half * 2 + czl, dz = tz - cz;
-                        if (dz < 0 || dz >= S) continue;
-                        for (int cy = 0; cy < 4; ++cy) {
-                            const int dy = ty - cy;
-                            if (dy < 0 || dy >= S) continue;
-                            for (int cx = 0; cx < 4; ++cx) {
-                                const int dx = tx - cx;
-                                if (dx < 0 || dx >= S) continue;
-                                const int cell = (cz * 4 + cy) * 4 + cx;
-                                if (!cellNonEmpty[cell]) continue;
-                                const int cl = cell - half * 32;
-                                // stencil node index of the lane layout: a + S (b + S c)
-                                const int k = dx + S * (dy + S * dz);
-                                const float* pc = partial + (size_t)cl * F * 64 + k;
-#pragma unroll
-                                for (int f = 0; f < F; ++f) tacc[j][f] += pc[f * 64];
-                            }
-                        }
+                        for (int f = 0; f < F; ++f) tacc[j][f] += pc[f * 64];
                     }
                 }
             }
@@ -548,6 +582,7 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
+        if (args.block_slot[it.block] != (int32_t)w) continue;  // a block's first work item does its nodes
         const uint32_t lb = it.block - sc.block_base;
         const int B[3] = {(int)(lb % (uint32_t)sc.nb[0]), (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]),
                           (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]))};
@@ -576,9 +611,13 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
                 if (ix >= T || iy >= T || iz >= T) continue;
                 const int slot = blockSlotAt(args, sc, N[0] - de[0], N[1] - de[1], N[2] - de[2]);
                 if (slot < 0) continue;
-                const float* tile = args.tiles + (size_t)slot * args.tile_stride + ix + T * (iy + T * iz);
+                // every work item (tile) of that block, in item order
+                const uint32_t blk = args.active[slot].block;
+                for (uint32_t s2 = (uint32_t)slot; s2 < nact && args.active[s2].block == blk; ++s2) {
+                    const float* tile = args.tiles + (size_t)s2 * args.tile_stride + ix + T * (iy + T * iz);
 #pragma unroll
-                for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+                    for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+                }
             }
             const size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);
             const size_t nodes = (size_t)sc.res[0] * sc.res[1] * sc.res[2];

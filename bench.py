@@ -292,9 +292,12 @@ def run_forms(args, ws, local):
     from mpm_b200 import scenes
     from mpm_b200.batch import Batch
     from mpm_b200.serving import Server
+    from mpm_b200.sharding import scenes_for_rank
     out = {}
     steps = min(args.steps, 100)
-    scs = scenes.batched_scenes()
+    # with several GPUs the 64 scenes are split across ranks (scene-parallel)
+    rank = int(os.environ.get("RANK", "0"))
+    scs = scenes_for_rank(scenes.batched_scenes(), rank, ws)
     ntot = sum(s.n for s in scs)
     with Batch(device=local) as b:
         for s in scs:
@@ -307,7 +310,8 @@ def run_forms(args, ws, local):
         prof = b.profile_read()
         st = b.stats()
     t = allmax(ws, ms) / 1e3
-    out["batched"] = {"workload": "64 scenes, %d particles" % ntot, "steps": steps,
+    out["batched"] = {"workload": "64 seeded scenes split over %d GPU(s); %d particles on rank %d" % (ws, ntot, rank),
+                      "steps": steps,
                       "value": allsum(ws, float(ntot * steps)) / t, "ms_per_step": t / steps * 1e3,
                       "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st}
     solvers = [s.solver() for s in scs]

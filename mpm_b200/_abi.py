@@ -52,6 +52,19 @@ class ParticlesIn(C.Structure):
                 ("volume", C.POINTER(C.c_float)), ("materials", C.POINTER(Material)), ("nmaterials", C.c_int32)]
 
 
+class ConfigGroup(C.Structure):
+    _fields_ = [("file", C.c_char * 1024), ("mass", C.c_float), ("velocity", C.c_float * 3),
+                ("material", Material)]
+
+
+class Config(C.Structure):
+    _fields_ = [("ngroups", C.c_int32), ("groups", C.POINTER(ConfigGroup)), ("origin", C.c_float * 3),
+                ("resolution", C.c_int32 * 3), ("stride", C.c_float), ("friction", C.c_float), ("blend", C.c_float),
+                ("interpolation", C.c_int32), ("dt", C.c_float), ("offline", C.c_int32),
+                ("particle_frag_shader", C.c_char * 1024), ("gravity", C.c_float), ("transfer", C.c_int32),
+                ("boundary", C.c_int32), ("sticky_cells", C.c_int32), ("base_dir", C.c_char * 1024)]
+
+
 class StepStats(C.Structure):
     _fields_ = [("active_blocks", C.c_uint32), ("outside_blocks", C.c_uint32), ("active_nodes", C.c_uint32),
                 ("reserved", C.c_uint32)]
@@ -93,6 +106,13 @@ SIGNATURES = {
     "mpm_sort_keys_device_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),
     "mpm_set_device": (C.c_int, [C.c_int32]),
+    "mpm_config_parse_yaml": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Config))]),
+    "mpm_config_parse_yaml_string": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.POINTER(Config))]),
+    "mpm_config_free": (C.c_int, [C.POINTER(Config)]),
+    "mpm_read_xyz": (C.c_int, [C.c_char_p, C.c_char_p, C.c_float, C.POINTER(C.POINTER(C.c_float)),
+                               C.POINTER(C.c_size_t)]),
+    "mpm_free": (None, [C.c_void_p]),
+    "mpm_solver_create_from_config": (C.c_int, [C.POINTER(Config), C.c_int32, C.POINTER(_P), C.POINTER(C.c_int32)]),
     "mpm_solver_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
     "mpm_batch_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
     "mpm_solver_timed_step": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_float)]),

@@ -18,13 +18,16 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpm_b200.so")
+CLI = os.path.join(HERE, "mpm-run")
+# The image's default CXX (/opt/gcc) lacks parts of the runtime; the system g++ is complete.
+HOSTCXX = os.environ.get("MPM_HOSTCXX", "/usr/bin/g++")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xcompiler", "-ffp-contract=off"]
 
-SOURCES = ["sort.cu", "kernels.cu", "engine.cu", "sort_noalloc.cu"]
+SOURCES = ["sort.cu", "kernels.cu", "engine.cu", "sort_noalloc.cu", "config.cpp"]
 
 
 def _headers():
@@ -59,7 +62,7 @@ def build(verbose: bool = False) -> str:
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if _stale(o, [s] + headers):
             jobs.append([NVCC, *ARCH, *FLAGS, "-c", s, "-o", o])
@@ -68,6 +71,11 @@ def build(verbose: bool = False) -> str:
             list(ex.map(lambda c: _run(c, verbose), jobs))
     if _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], verbose)
+    # headless driver over the C++ facade (include/chains/mpm_b200.hpp)
+    src = os.path.join(CSRC, "mpm_run.cpp")
+    if _stale(CLI, [src, LIB] + headers):
+        _run([HOSTCXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", CLI, "-L", HERE,
+              "-lmpm_b200", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <memory>
 #include <string>
@@ -105,6 +106,7 @@ public:
     Engine() {}
     ~Engine() {
         if (stream_) cudaStreamSynchronize(stream_);
+        dropGraphs();
         for (int k = 0; k < KF_COUNT; ++k) {
             if (ev_[k][0]) cudaEventDestroy(ev_[k][0]);
             if (ev_[k][1]) cudaEventDestroy(ev_[k][1]);
@@ -273,6 +275,8 @@ public:
     // set of scenes changed.
     mpm_status rebuild() {
         if (!dirty_) return MPM_OK;
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        dropGraphs();  // graphs hold pointers into buffers that may move below
         const int ns = (int)scenes_.size();
         host_scenes_.assign(ns, SceneDev{});
         std::vector<uint32_t> sbb(ns + 1, 0);
@@ -574,10 +578,59 @@ public:
         return MPM_OK;
     }
 
-    // One fused simulateOneStep over every scene of the batch.
+    // One fused simulateOneStep over every scene of the batch.  In steady state
+    // (keys and stress produced by the previous G2P, no profiling) the step is
+    // replayed from a CUDA graph captured once per (particle buffer, key
+    // buffer) state; the launch sequence and its arguments only depend on it.
     mpm_status stepOnce() {
+        bool stale = false;
+        for (auto& s : scenes_) stale |= s->stress_stale;
+        const bool steady = use_graphs_ && keys_valid_ && !stale && !profiling_ && !dirty_;
+        if (!steady) return stepBody();
+        GraphSlot& g = graphs_[parity_][kcur_];
+        const int p0 = parity_, k0 = kcur_;
+        if (!g.exec) {
+            const uint64_t l0 = kernelLaunches();
+            CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            mpm_status st = stepBody();
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+            // the capture only recorded the launches: restore the host state
+            parity_ = p0;
+            kcur_ = k0;
+            keys_valid_ = true;
+            if (st != MPM_OK || e != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                use_graphs_ = false;  // fall back to direct launches for this engine
+                return stepBody();
+            }
+            e = cudaGraphInstantiate(&g.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                g.exec = nullptr;
+                cudaGetLastError();
+                use_graphs_ = false;
+                return stepBody();
+            }
+            g.launches = kernelLaunches() - l0;
+            noteLaunches(0 - g.launches);  // captured, not run: counted at each replay instead
+        }
+        CUDA_TRY(cudaGraphLaunch(g.exec, stream_));
+        noteLaunches(g.launches);
+        // host state after the step, as stepBody() leaves it
+        sorted_ = graph_sorted_[p0][k0];
+        parity_ = p0 ^ 1;
+        kcur_ = 1 - sorted_;
+        keys_valid_ = true;
+        sorted_valid_ = false;
+        return MPM_OK;
+    }
+
+    mpm_status stepBody() {
         MPM_TRY(sortLive());
         MPM_TRY(refreshStress());
+        graph_sorted_[parity_][kcur_] = sorted_;
         const int next = 1 - sorted_;
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
         LaunchCtx c = ctx();
@@ -900,6 +953,20 @@ private:
     DevMem keys_[2], vals_[2], hist_, scan32_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    };
+    GraphSlot graphs_[2][2];          // [particle buffer parity][unsorted key buffer]
+    int graph_sorted_[2][2] = {};     // sorted key buffer after the sort of that state
+    bool use_graphs_ = getenv("MPM_NO_GRAPHS") == nullptr;
+    void dropGraphs() {
+        for (auto& row : graphs_)
+            for (auto& g : row) {
+                if (g.exec) cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+    }
     cudaEvent_t ev_[KF_COUNT][2] = {};
     struct Record {
         int fam;

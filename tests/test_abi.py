@@ -12,7 +12,7 @@ from mpm_b200 import _abi
 from mpm_b200.solver import Material, Particles, scene_desc
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADERS = [os.path.join(ROOT, "include", h) for h in ("mpm_b200.h", "mpm_b200_batch.h")]
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("mpm_b200.h", "mpm_b200_batch.h", "mpm_b200_config.h")]
 
 
 def declared_symbols():

@@ -349,6 +349,9 @@ public:
         const size_t tiles = radixTiles(nk);
         MPM_TRY(hist_.alloc(sizeof(uint32_t) * 256 * tiles, "radix histogram"));
         MPM_TRY(scan32_.alloc(sizeof(uint32_t) * (scanScratchElems(256 * tiles) + 1), "scan scratch"));
+        MPM_TRY(sort_scratch_.alloc(sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
+        MPM_TRY(compact_scratch_.alloc(sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
+                                       "compaction scratch"));
         MPM_TRY(block_count_.alloc(sizeof(uint32_t) * tb, "block counts"));
         CUDA_TRY(cudaMemsetAsync(block_count_.p, 0, sizeof(uint32_t) * tb, stream_));
         MPM_TRY(packed_.alloc(sizeof(unsigned long long) * tb, "block scan"));
@@ -477,14 +480,15 @@ public:
         }
         bool inB = false;
         mark(KF_SORT, 0);
-        CUDA_TRY(radixSortPairs(keys_[kcur_].as<uint32_t>(), vals_[kcur_].as<uint32_t>(),
-                                keys_[1 - kcur_].as<uint32_t>(), vals_[1 - kcur_].as<uint32_t>(), ntot_, key_bits_,
-                                hist_.as<uint32_t>(), scan32_.as<uint32_t>(), &inB, stream_));
+        CUDA_TRY(radixSortOnesweep(keys_[kcur_].as<uint32_t>(), vals_[kcur_].as<uint32_t>(),
+                                   keys_[1 - kcur_].as<uint32_t>(), vals_[1 - kcur_].as<uint32_t>(), ntot_, key_bits_,
+                                   sort_scratch_.as<uint32_t>(), err_.as<uint32_t>(), &inB, stream_));
         mark(KF_SORT, 1);
         collect(KF_SORT);
         sorted_ = inB ? 1 - kcur_ : kcur_;
         mark(KF_COMPACT, 0);
-        launchCompact(ctx(), blockBuffers(), total_blocks_);
+        launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(),
+                              err_.as<uint32_t>());
         mark(KF_COMPACT, 1);
         collect(KF_COMPACT);
         CUDA_TRY(cudaGetLastError());
@@ -950,7 +954,7 @@ private:
     size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
-    DevMem keys_[2], vals_[2], hist_, scan32_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
+    DevMem keys_[2], vals_[2], hist_, scan32_, sort_scratch_, compact_scratch_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
     struct GraphSlot {
@@ -1187,22 +1191,25 @@ mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, uint32_t*
         cudaGetLastError();
         return mpm::fail(MPM_ERR_CUDA, "mpm_sort_keys: no CUDA device");
     }
-    mpm::DevMem k[2], v[2], hist, part;
+    mpm::DevMem k[2], v[2], scratch, err;
     mpm_status s = MPM_OK;
     for (int i = 0; i < 2 && s == MPM_OK; ++i) {
         s = k[i].alloc(sizeof(uint32_t) * n, "keys");
         if (s == MPM_OK) s = v[i].alloc(sizeof(uint32_t) * n, "values");
     }
-    const size_t tiles = mpm::radixTiles(n);
-    if (s == MPM_OK) s = hist.alloc(sizeof(uint32_t) * 256 * tiles, "histogram");
-    if (s == MPM_OK) s = part.alloc(sizeof(uint32_t) * (mpm::scanScratchElems(256 * tiles) + 1), "scan scratch");
+    if (s == MPM_OK) s = scratch.alloc(sizeof(uint32_t) * mpm::onesweepScratchWords(n, bits), "sort scratch");
+    if (s == MPM_OK) s = err.alloc(sizeof(uint32_t), "error flag");
     bool inB = false;
+    uint32_t flag = 0;
     cudaError_t e = cudaSuccess;
     if (s == MPM_OK) {
-        e = cudaMemcpyAsync(k[0].p, keys, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st);
+        e = cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(k[0].p, keys, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
-            e = mpm::radixSortPairs(k[0].as<uint32_t>(), v[0].as<uint32_t>(), k[1].as<uint32_t>(), v[1].as<uint32_t>(),
-                                    n, bits, hist.as<uint32_t>(), part.as<uint32_t>(), &inB, st);
+            e = mpm::radixSortOnesweep(k[0].as<uint32_t>(), v[0].as<uint32_t>(), k[1].as<uint32_t>(),
+                                       v[1].as<uint32_t>(), n, bits, scratch.as<uint32_t>(), err.as<uint32_t>(), &inB,
+                                       st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         const int r = inB ? 1 : 0;
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(sorted_keys, k[r].p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
@@ -1213,6 +1220,7 @@ mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, uint32_t*
     cudaStreamDestroy(st);
     if (s != MPM_OK) return s;
     if (e != cudaSuccess) return mpm::fail(MPM_ERR_CUDA, std::string("mpm_sort_keys: ") + cudaGetErrorString(e));
+    if (flag) return mpm::fail(MPM_ERR_TIMEOUT, "mpm_sort_keys: a look-back wait gave up");
     return MPM_OK;
 }
 

@@ -46,6 +46,9 @@ cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, 
 size_t radixTiles(size_t n);
 cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n, int bits,
                            uint32_t* hist, uint32_t* scan_partials, bool* result_in_b, cudaStream_t st);
+size_t onesweepScratchWords(size_t n, int bits);
+cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
+                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st);
 cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint32_t* out_vals, uint32_t* tmp_keys,
                                uint32_t* tmp_vals, size_t n, int bits, uint32_t* hist, uint32_t* scan_partials,
                                cudaStream_t st);
@@ -53,6 +56,9 @@ cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint
 // kernels.cu
 void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err);
 void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks);
+size_t compactScratchWords64(uint32_t total_blocks);
+void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
+                           unsigned long long* scratch, uint32_t* err);
 void launchStress(const LaunchCtx& c, int parity);
 void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
 void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);

@@ -222,6 +222,134 @@ __global__ void __launch_bounds__(kThreads) compactBlocksKernel(
     }
 }
 
+// Block compaction in one kernel: each CTA scans a tile of 1024 block counts,
+// publishes the tile's (work items, particles) sums and looks back over the
+// earlier tiles' published words (single-pass scan, dynamic tile ids, every
+// wait bounded), then writes the work items, slots and outside items of its
+// blocks and clears their counts.  Word layout: [63:62] flag, [61:32] items,
+// [31:0] particles.
+constexpr int kCompactPer = 4;
+constexpr int kCompactTile = kThreads * kCompactPer;
+constexpr unsigned long long kCFlagAgg = 1ull << 62, kCFlagPrefix = 2ull << 62, kCFlagMask = 3ull << 62;
+
+__device__ __forceinline__ unsigned long long blockExclusiveScanU64(unsigned long long x, unsigned long long* total) {
+    __shared__ unsigned long long wt[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wt[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = lane < kWarps ? wt[lane] : 0ull, ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += y;
+        }
+        if (lane < kWarps) wt[lane] = ti - t;
+        const unsigned long long tl = __shfl_sync(0xffffffffu, ti, kWarps - 1);
+        if (lane == 0) *total = tl;
+    }
+    __syncthreads();
+    const unsigned long long r = inc - x + wt[warp];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
+    uint32_t* __restrict__ block_count, uint32_t total_blocks, const uint32_t* __restrict__ scene_block_base,
+    int nscenes, BlockItem* __restrict__ active, BlockItem* __restrict__ outside, uint32_t* __restrict__ counters,
+    int32_t* __restrict__ block_slot, unsigned long long* __restrict__ status, uint32_t* __restrict__ tile_counter,
+    uint32_t ntiles, uint32_t* __restrict__ err) {
+    __shared__ uint32_t tile_s;
+    __shared__ unsigned long long tot, excl_s;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = tile_s;
+    const uint32_t b0 = tile * kCompactTile + threadIdx.x * kCompactPer;
+    unsigned long long packed[kCompactPer];
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int j = 0; j < kCompactPer; ++j) {
+        const uint32_t b = b0 + j;
+        unsigned long long v = 0;
+        if (b < total_blocks) {
+            const uint32_t c = block_count[b];
+            const int s = sceneOfBlock(scene_block_base, nscenes, b);
+            const bool out = (b == scene_block_base[s + 1] - 1);
+            const unsigned long long items = (c > 0 && !out) ? (unsigned long long)((c + kBlockChunk - 1) / kBlockChunk) : 0ull;
+            v = (items << 32) | (unsigned long long)c;
+        }
+        packed[j] = v;
+        sum += v;
+    }
+    unsigned long long run = blockExclusiveScanU64(sum, &tot);
+    if (threadIdx.x == 0) {
+        unsigned long long excl = 0;
+        if (tile == 0) {
+            atomicExch(&status[0], kCFlagPrefix | tot);
+        } else {
+            atomicExch(&status[tile], kCFlagAgg | tot);
+            int t = (int)tile - 1;
+            int polls = 0;
+            while (t >= 0) {
+                const unsigned long long w = *(volatile const unsigned long long*)(status + t);
+                const unsigned long long f = w & kCFlagMask;
+                if (f == 0) {
+                    if (++polls > (1 << 22)) {  // never expected: give up instead of hanging
+                        atomicOr(err, 16u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += w & ~kCFlagMask;
+                if (f == kCFlagPrefix) break;
+                --t;
+            }
+            atomicExch(&status[tile], kCFlagPrefix | (excl + tot));
+        }
+        excl_s = excl;
+        if (tile == ntiles - 1) counters[0] = (uint32_t)((excl + tot) >> 32);
+    }
+    __syncthreads();
+    run += excl_s;
+#pragma unroll
+    for (int j = 0; j < kCompactPer; ++j) {
+        const uint32_t b = b0 + j;
+        if (b >= total_blocks) break;
+        const unsigned long long v = packed[j];
+        const uint32_t count = (uint32_t)(v & 0xffffffffull);
+        const uint32_t items = (uint32_t)(v >> 32);
+        const uint32_t start = (uint32_t)(run & 0xffffffffull);
+        const int scene = sceneOfBlock(scene_block_base, nscenes, b);
+        if (items) {
+            const uint32_t slot = (uint32_t)(run >> 32);
+            for (uint32_t q = 0; q < items; ++q) {
+                const uint32_t off = q * kBlockChunk;
+                active[slot + q] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
+            }
+            block_slot[b] = (int32_t)slot;
+        } else {
+            block_slot[b] = -1;
+            if (count > 0) {
+                const uint32_t nitems = (count + kBlockChunk - 1) / kBlockChunk;
+                const uint32_t o = atomicAdd(&counters[1], nitems);
+                for (uint32_t q = 0; q < nitems; ++q) {
+                    const uint32_t off = q * kBlockChunk;
+                    outside[o + q] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
+                }
+            }
+        }
+        block_count[b] = 0;
+        run += v;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // tau from Fe/Fp for the live order (first step, after uploads).
 // ---------------------------------------------------------------------------
@@ -1108,6 +1236,21 @@ __global__ void scatterFieldKernel(const SceneDev* __restrict__ scenes, int scen
 void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err) {
     noteLaunches(1);
     keyKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, keys, block_count, err);
+}
+
+size_t compactScratchWords64(uint32_t total_blocks) {
+    return (size_t)(total_blocks + kCompactTile - 1) / kCompactTile + 1;  // + the tile counter
+}
+
+void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
+                           unsigned long long* scratch, uint32_t* err) {
+    const uint32_t ntiles = (uint32_t)((total_blocks + kCompactTile - 1) / kCompactTile);
+    cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * compactScratchWords64(total_blocks), c.stream);
+    cudaMemsetAsync(bb.counters, 0, sizeof(uint32_t) * 4, c.stream);
+    noteLaunches(1);
+    compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
+        bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,
+        bb.block_slot, scratch + 1, reinterpret_cast<uint32_t*>(scratch), ntiles, err);
 }
 
 void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks) {

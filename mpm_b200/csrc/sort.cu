@@ -187,11 +187,184 @@ __global__ void __launch_bounds__(kThreads) radixDownsweepKernel(const uint32_t*
     }
 }
 
+// --- single-pass ("onesweep") radix passes -----------------------------------
+//
+// One kernel counts the digits of every pass over all keys; then each pass is
+// one kernel: a CTA takes the next tile (dynamic tile ids, so tile t only
+// ever waits on tiles that started earlier), ranks its keys stably, publishes
+// its per-digit count, and finds the count of every earlier tile with the
+// same digit by looking back over their published words.  A word holds a
+// 2-bit flag (aggregate / inclusive prefix) and a 30-bit count.  Every wait
+// is bounded: after kLookbackLimit polls the kernel raises an error flag and
+// goes on instead of spinning forever.
+
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagPrefix = 2u << 30, kCountMask = (1u << 30) - 1u;
+constexpr int kLookbackLimit = 1 << 22;
+
+__global__ void __launch_bounds__(kThreads) onesweepHistKernel(const uint32_t* __restrict__ keys, uint32_t n,
+                                                                int passes, int bits, uint32_t* __restrict__ ghist) {
+    __shared__ uint32_t h[4][256];
+    for (int i = threadIdx.x; i < 4 * 256; i += kThreads) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const size_t stride = (size_t)gridDim.x * kThreads;
+    const size_t n_round = ((size_t)n + 31) / 32 * 32;  // whole warps iterate together
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n_round; i += stride) {
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys[i] : 0u;
+        for (int p = 0; p < passes; ++p) {
+            const int shift = 8 * p;
+            const int pb = bits - shift < 8 ? bits - shift : 8;
+            const uint32_t mask = (1u << (pb > 0 ? pb : 1)) - 1u;
+            const uint32_t d = valid ? (key >> shift) & mask : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads)
+        if ((&h[0][0])[i]) atomicAdd(&ghist[i], (&h[0][0])[i]);
+}
+
+template <bool kIdentVals>
+__global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* __restrict__ keys_in,
+                                                                const uint32_t* __restrict__ vals_in,
+                                                                uint32_t* __restrict__ keys_out,
+                                                                uint32_t* __restrict__ vals_out, uint32_t n,
+                                                                int shift, uint32_t mask,
+                                                                const uint32_t* __restrict__ ghist,
+                                                                uint32_t* __restrict__ tile_counter,
+                                                                uint32_t* __restrict__ status,
+                                                                uint32_t* __restrict__ err) {
+    __shared__ uint32_t cnt[kWarps][256];
+    __shared__ uint32_t base[256];
+    __shared__ uint32_t tile_s;
+    __shared__ uint32_t tot;
+    for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) (&cnt[0][0])[i] = 0;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+    {   // global start of every digit: exclusive scan of this pass's digit counts
+        const uint32_t g = ghist[threadIdx.x];
+        base[threadIdx.x] = blockExclusiveScan(g, &tot);
+    }
+    __syncthreads();
+    const uint32_t tile = tile_s;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const size_t tbase = (size_t)tile * kSortTile + (size_t)warp * 32 * kSortItems;
+    uint32_t k[kSortItems], v[kSortItems], r[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const size_t i = tbase + (size_t)j * 32 + lane;
+        const bool valid = i < n;
+        k[j] = valid ? keys_in[i] : 0u;
+        v[j] = valid ? (kIdentVals ? (uint32_t)i : vals_in[i]) : 0u;
+        const uint32_t d = valid ? (k[j] >> shift) & mask : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        const uint32_t before = valid ? cnt[warp][d] : 0u;
+        r[j] = before + __popc(peers & lt);
+        __syncwarp();
+        if (valid && lane == leader) cnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = cnt[w][d];
+            cnt[w][d] = run;
+            run += c;
+        }
+        uint32_t* mine = status + (size_t)tile * 256 + d;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            atomicExch(mine, kFlagPrefix | run);
+        } else {
+            atomicExch(mine, kFlagAgg | run);
+            int t = (int)tile - 1;
+            int polls = 0;
+            while (t >= 0) {
+                const uint32_t w = *(volatile const uint32_t*)(status + (size_t)t * 256 + d);
+                const uint32_t f = w & ~kCountMask;
+                if (f == 0) {
+                    if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
+                        atomicOr(err, 8u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += w & kCountMask;
+                if (f == kFlagPrefix) break;
+                --t;
+            }
+            atomicExch(mine, kFlagPrefix | (excl + run));
+        }
+        base[d] += excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const size_t i = tbase + (size_t)j * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (k[j] >> shift) & mask;
+            const uint32_t pos = base[d] + cnt[warp][d] + r[j];
+            keys_out[pos] = k[j];
+            vals_out[pos] = v[j];
+        }
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Host wrappers.
 // ---------------------------------------------------------------------------
+size_t onesweepScratchWords(size_t n, int bits) {
+    const int passes = bits <= 8 ? 1 : (bits + 7) / 8;
+    return (size_t)passes * 256 + 32 + (size_t)passes * radixTiles(n) * 256;
+}
+
+// Stable sort of (keys_a, identity values) by the low `bits` bits, one kernel
+// per 8-bit pass.  `scratch` holds onesweepScratchWords(n, bits) words and is
+// cleared here.  `err` receives bit 8 if a look-back wait gave up.
+cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
+                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st) {
+    *result_in_b = false;
+    if (n == 0) return cudaSuccess;
+    if (n > kCountMask) return cudaErrorInvalidValue;
+    const int passes = bits <= 8 ? 1 : (bits + 7) / 8;
+    const int ntiles = (int)radixTiles(n);
+    uint32_t* ghist = scratch;
+    uint32_t* counters = scratch + (size_t)passes * 256;
+    uint32_t* status = counters + 32;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * onesweepScratchWords(n, bits), st);
+    if (e != cudaSuccess) return e;
+    const int hblocks = (int)std::min<size_t>((n + kThreads * 16 - 1) / (kThreads * 16), 148 * 4);
+    noteLaunches(1 + passes);
+    onesweepHistKernel<<<hblocks, kThreads, 0, st>>>(keys_a, (uint32_t)n, passes, bits, ghist);
+    uint32_t *kin = keys_a, *vin = vals_a, *kout = keys_b, *vout = vals_b;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        int pass_bits = bits - shift < 8 ? bits - shift : 8;
+        if (pass_bits <= 0) pass_bits = 1;
+        const uint32_t mask = (1u << pass_bits) - 1u;
+        uint32_t* stat = status + (size_t)p * ntiles * 256;
+        if (p == 0)
+            onesweepPassKernel<true><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, shift, mask,
+                                                                  ghist + 256 * p, counters + p, stat, err);
+        else
+            onesweepPassKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, shift, mask,
+                                                                   ghist + 256 * p, counters + p, stat, err);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+        *result_in_b = !*result_in_b;
+    }
+    return cudaGetLastError();
+}
+
 size_t scanScratchElems(size_t n) { return (n + kScanChunk - 1) / kScanChunk; }
 
 template <class T>

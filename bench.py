@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-scale", type=float, default=0.02)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    ap.add_argument("--no-naive", action="store_true", help="skip the reference-naive GPU baseline leg")
+    ap.add_argument("--naive-budget-s", type=float, default=10.0)
     return ap.parse_args()
 
 
@@ -203,6 +205,25 @@ def cpu_rate(sc, budget_s, steps_hint=None):
     return sc.n * k / dt, threads, k, dt
 
 
+def naive_rate(sc, budget_s):
+    """The reference-naive GPU restatement (baseline/naive) on the same scene
+    and GPU: AoS state, float atomics, per-node spline evaluation, one
+    synchronised launch per sub-step.  Steps timed with CUDA events on the
+    legacy stream, as many as fit the budget (at least 3)."""
+    sys.path.insert(0, os.path.join(ROOT, "baseline", "naive"))
+    import naive as NV
+    g = NV.NaiveSolver(sc.desc(), sc.particles)
+    g.step(2)
+    t1 = g.timed_step(2) / 2e3
+    k = int(max(3, min(1000, budget_s / max(t1, 1e-6))))
+    ms = g.timed_step(k)
+    g.close()
+    return {"value": sc.n * k / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / k, "steps": k,
+            "kind": "reference-naive CUDA restatement on the same B200 (AoS 236 B APIC / 128 B FLIP points, "
+                    "52 B nodes, 7 float atomics per particle-node, per-node FP64-literal splines, "
+                    "2 SVDs per particle, synchronised launch per sub-step)"}
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -263,6 +284,11 @@ def run_ours(args, ws, rank, local):
     if not args.no_forms:
         forms = run_forms(args, ws, local)
 
+    naive = None
+    if rank == 0 and ws == 1 and not args.no_naive:
+        naive = naive_rate(sc, args.naive_budget_s)
+        naive["speedup"] = value / naive["value"]
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, threads, k, dt = cpu_rate(sc, args.cpu_budget_s)
@@ -275,7 +301,7 @@ def run_ours(args, ws, rank, local):
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                "config": config_of(sc, ws), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(launches1.value - launches0.value), "clocks": clk.summary(),
-               "stats": stats, "forms": forms}
+               "stats": stats, "naive_gpu": naive, "forms": forms}
         print(json.dumps(out), flush=True)
     g.close()
 
@@ -346,7 +372,9 @@ def run_forms(args, ws, local):
 def run_e2e(sc, steps, ws):
     """Same metric through the public API with host buffers: construct the
     solver from pinned host arrays (H2D), then every step download the
-    (x, y, z, 1) positions into pinned host memory (D2H)."""
+    (x, y, z, 1) positions into pinned host memory (D2H, asynchronous, into
+    two alternating buffers, so the copy of step k overlaps step k + 1); the
+    clock stops after the last copy has landed."""
     import torch
     from mpm_b200 import _abi
     from mpm_b200.solver import APICMPMSolver3D, MPMSolver3D, Particles
@@ -354,7 +382,7 @@ def run_e2e(sc, steps, ws):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     p = Particles(pin(sc.particles.positions), pin(sc.particles.velocities), pin(sc.particles.mass),
                   sc.particles.materials, None, None)
-    out = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    outs = [torch.empty((n, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
     opts = dict(gravity=sc.gravity, boundary=sc.boundary, sticky_cells=sc.sticky_cells, volume_mode=sc.volume_mode)
     barrier(ws)
     t0 = time.perf_counter()
@@ -363,9 +391,12 @@ def run_e2e(sc, steps, ws):
     else:
         g = MPMSolver3D(p, sc.origin, sc.resolution, sc.stride, sc.friction, sc.blend, sc.interpolation, sc.dt,
                         **opts)
-    for _ in range(steps):
+    for k in range(steps):
         g.step(1)
-        g.download_into(_abi.FIELD_POSITION4, out.data_ptr())
+        # this step's positions into alternating pinned buffers; the copy
+        # overlaps the next step (download_async)
+        g.download_async(_abi.FIELD_POSITION4, outs[k % 2].data_ptr())
+    g.download_wait()
     dt = time.perf_counter() - t0
     g.close()
     barrier(ws)
@@ -373,7 +404,8 @@ def run_e2e(sc, steps, ws):
     h2d = n * (3 + 3 + 1) * 4
     return {"value": allsum(ws, float(n * steps)) / t, "unit": METRIC, "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": 16 * n, "timed": "solver construction (H2D of the particles) + per step: "
-            "step + download of float4 positions into pinned host memory"}
+            "step + asynchronous download of float4 positions into pinned host memory, "
+            "until the last copy has landed"}
 
 
 def main():

@@ -221,6 +221,18 @@ MPM_API mpm_status mpm_solver_get_desc(const mpm_solver* s, mpm_scene_desc* desc
  * holds n * floats-per-particle floats.  MPM_FIELD_POSITION4 replaces the
  * GL buffer export (src/mpm_solver3d.cu:447-508). */
 MPM_API mpm_status mpm_solver_download(mpm_solver* s, int32_t field, float* host_out);
+/* Asynchronous download of the current state (same layout as
+ * mpm_solver_download): the device gather runs in the solver's stream order,
+ * the copy into host_out runs on a copy stream and overlaps later steps.
+ * Returns at once; host_out (pinned memory for the copy to overlap) must stay
+ * valid and unread until mpm_solver_download_wait or mpm_solver_synchronize
+ * returns.  Two staging buffers alternate, so any number of downloads may be
+ * queued; the third waits on the device for the first one's copy.  No
+ * counterpart in the reference, whose per-frame export
+ * (updateGLBufferWithCUDA, src/mpm_solver3d.cu:447-508) copies synchronously. */
+MPM_API mpm_status mpm_solver_download_async(mpm_solver* s, int32_t field, float* host_out);
+/* Wait for every asynchronous download issued so far. */
+MPM_API mpm_status mpm_solver_download_wait(mpm_solver* s);
 /* Download a dense grid field (res^3 * components floats).  Valid after
  * particles_to_grid() and the grid sub-steps of the split API, or after
  * mpm_solver_step when the solver keeps the dense debug grid. */

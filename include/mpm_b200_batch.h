@@ -32,6 +32,9 @@ MPM_API mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps);
 MPM_API mpm_status mpm_batch_synchronize(mpm_batch* b);
 /* Download a particle field of one scene in its original particle order. */
 MPM_API mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
+/* Asynchronous form (see mpm_solver_download_async) and its wait. */
+MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
+MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
 MPM_API mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out);
 /* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */

@@ -89,6 +89,15 @@ class Batch:
               "mpm_batch_download")
         return out.reshape(n, 3, 3) if comps == 9 else (out[:, 0] if comps == 1 else out)
 
+    def download_async(self, sid: int, field: int, ptr: int):
+        """Queue a download of one scene's current state into caller memory at
+        address ptr; complete after download_wait() or synchronize()."""
+        check(self._lib.mpm_batch_download_async(self._h, int(sid), int(field), C.c_void_p(ptr)),
+              "mpm_batch_download_async")
+
+    def download_wait(self):
+        check(self._lib.mpm_batch_download_wait(self._h), "mpm_batch_download_wait")
+
     def stats(self) -> dict:
         st = _abi.StepStats()
         check(self._lib.mpm_batch_stats(self._h, C.byref(st)), "mpm_batch_stats")

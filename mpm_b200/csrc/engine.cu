@@ -106,6 +106,14 @@ public:
     Engine() {}
     ~Engine() {
         if (stream_) cudaStreamSynchronize(stream_);
+        if (copy_stream_) {
+            cudaStreamSynchronize(copy_stream_);
+            for (int k = 0; k < 2; ++k) {
+                if (stage_ready_[k]) cudaEventDestroy(stage_ready_[k]);
+                if (stage_done_[k]) cudaEventDestroy(stage_done_[k]);
+            }
+            cudaStreamDestroy(copy_stream_);
+        }
         dropGraphs();
         for (int k = 0; k < KF_COUNT; ++k) {
             if (ev_[k][0]) cudaEventDestroy(ev_[k][0]);
@@ -211,30 +219,31 @@ public:
         MPM_TRY(sc->mats.alloc(sizeof(MaterialDev) * mats.size(), "materials"));
         CUDA_TRY(cudaMemcpyAsync(sc->mats.p, mats.data(), sizeof(MaterialDev) * mats.size(), cudaMemcpyHostToDevice,
                                  stream_));
-        // Particle state in the caller's order (Fe = Fp = I, B = 0).
+        // Particle state in the caller's order: the caller's arrays are copied
+        // as they are (x, v interleaved; m; V0 if prescribed) into a staging
+        // buffer and a kernel writes the SoA planes (Fe = Fp = I, B = 0).
         if (p.n > 0) {
-            std::vector<float> host((size_t)NFIELDS * p.n, 0.f);
-            for (size_t i = 0; i < p.n; ++i) {
-                for (int a = 0; a < 3; ++a) {
-                    host[(F_X + a) * p.n + i] = p.position[3 * i + a];
-                    host[(F_V + a) * p.n + i] = p.velocity[3 * i + a];
-                }
-                for (int k = 0; k < 9; k += 4) {
-                    host[(F_FE + k) * p.n + i] = 1.f;
-                    host[(F_FP + k) * p.n + i] = 1.f;
-                }
-                host[F_MASS * p.n + i] = p.mass[i];
-                host[F_VOL * p.n + i] = (d.volume_mode == MPM_VOLUME_PRESCRIBED) ? p.volume[i] : 0.f;
-            }
-            std::vector<uint32_t> pid(p.n);
-            for (size_t i = 0; i < p.n; ++i) pid[i] = (uint32_t)i;
+            const bool has_vol = d.volume_mode == MPM_VOLUME_PRESCRIBED;
+            const size_t n = p.n;
+            MPM_TRY(tmp_.alloc(sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
+            float* staged = tmp_.as<float>();
+            CUDA_TRY(cudaMemcpyAsync(staged, p.position, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
+            CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
+                                     stream_));
+            CUDA_TRY(cudaMemcpyAsync(staged + 6 * n, p.mass, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+            if (has_vol)
+                CUDA_TRY(cudaMemcpyAsync(staged + 7 * n, p.volume, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
             const int b = parity_;
-            CUDA_TRY(cudaMemcpy(sc->buf_f[b].p, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice));
-            CUDA_TRY(cudaMemcpy(sc->buf_pid[b].p, pid.data(), sizeof(uint32_t) * p.n, cudaMemcpyHostToDevice));
+            launchInitState(stream_, num_sms_, sc->buf_f[b].as<float>(), sc->buf_pid[b].as<uint32_t>(), cap, staged, n,
+                            has_vol);
+            CUDA_TRY(cudaGetLastError());
             if (p.material)
-                CUDA_TRY(cudaMemcpy(sc->buf_mat[b].p, p.material, sizeof(uint16_t) * p.n, cudaMemcpyHostToDevice));
+                CUDA_TRY(cudaMemcpyAsync(sc->buf_mat[b].p, p.material, sizeof(uint16_t) * n, cudaMemcpyHostToDevice,
+                                         stream_));
             else
-                CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * p.n, stream_));
+                CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * n, stream_));
+            // the caller's arrays may be freed once this returns
+            CUDA_TRY(cudaStreamSynchronize(stream_));
         }
         sc->need_init = true;
         sc->id = next_id_++;
@@ -709,6 +718,7 @@ public:
 
     mpm_status synchronize() {
         CUDA_TRY(cudaStreamSynchronize(stream_));
+        MPM_TRY(downloadWait());
         uint32_t e = 0;
         CUDA_TRY(cudaMemcpy(&e, err_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
         if (e) {
@@ -854,6 +864,57 @@ public:
         return MPM_OK;
     }
 
+    // Asynchronous download: the gather into one of two device staging
+    // buffers runs in stream order (it reads the current state), the copy to
+    // the host runs on a separate copy stream, so it overlaps the steps that
+    // follow (they write the other particle buffer and never the staging
+    // buffers).  A staging buffer is reused only after its previous copy has
+    // finished (the compute stream waits for that copy's event).
+    mpm_status downloadAsync(int id, int field, float* host) {
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!host) return fail(MPM_ERR_INVALID_ARG, "null output pointer");
+        int base, comps, mode;
+        int per = fieldInfo(field, &base, &comps, &mode);
+        if (!per) return fail(MPM_ERR_INVALID_ARG, "unknown particle field");
+        SceneHost& s = *scenes_[idx];
+        if (field == MPM_FIELD_B && s.desc.transfer != MPM_TRANSFER_APIC)
+            return fail(MPM_ERR_INVALID_ARG, "B is only defined for APIC scenes");
+        if (s.n == 0) return MPM_OK;
+        if (!copy_stream_) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; ++k) {
+                CUDA_TRY(cudaEventCreateWithFlags(&stage_ready_[k], cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&stage_done_[k], cudaEventDisableTiming));
+            }
+        }
+        const int k = stage_next_;
+        stage_next_ ^= 1;
+        const size_t bytes = sizeof(float) * per * s.n;
+        if (stage_[k].bytes < bytes) {
+            if (stage_pending_[k]) CUDA_TRY(cudaEventSynchronize(stage_done_[k]));
+            MPM_TRY(stage_[k].alloc(bytes, "download staging buffer"));
+        }
+        if (stage_pending_[k]) CUDA_TRY(cudaStreamWaitEvent(stream_, stage_done_[k], 0));
+        launchGatherField(ctx(), idx, parity_, base, comps, mode, stage_[k].as<float>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(stage_ready_[k], stream_));
+        CUDA_TRY(cudaStreamWaitEvent(copy_stream_, stage_ready_[k], 0));
+        CUDA_TRY(cudaMemcpyAsync(host, stage_[k].p, bytes, cudaMemcpyDeviceToHost, copy_stream_));
+        CUDA_TRY(cudaEventRecord(stage_done_[k], copy_stream_));
+        stage_pending_[k] = true;
+        return MPM_OK;
+    }
+
+    // Waits for every asynchronous download issued so far.
+    mpm_status downloadWait() {
+        if (!copy_stream_) return MPM_OK;
+        CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+        stage_pending_[0] = stage_pending_[1] = false;
+        return MPM_OK;
+    }
+
     mpm_status upload(int id, int field, const float* host) {
         MPM_TRY(ensureReady());
         int idx = sceneIndex(id);
@@ -957,6 +1018,12 @@ private:
     DevMem keys_[2], vals_[2], hist_, scan32_, sort_scratch_, compact_scratch_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
+    // asynchronous downloads (downloadAsync)
+    cudaStream_t copy_stream_ = nullptr;
+    DevMem stage_[2];
+    cudaEvent_t stage_ready_[2] = {}, stage_done_[2] = {};
+    bool stage_pending_[2] = {};
+    int stage_next_ = 0;
     struct GraphSlot {
         cudaGraphExec_t exec = nullptr;
         uint64_t launches = 0;
@@ -1138,6 +1205,14 @@ mpm_status mpm_solver_download(mpm_solver* s, int32_t field, float* host_out) {
     MPM_TRY(check(s));
     return s->eng.download(s->scene, field, host_out);
 }
+mpm_status mpm_solver_download_async(mpm_solver* s, int32_t field, float* host_out) {
+    MPM_TRY(check(s));
+    return s->eng.downloadAsync(s->scene, field, host_out);
+}
+mpm_status mpm_solver_download_wait(mpm_solver* s) {
+    MPM_TRY(check(s));
+    return s->eng.downloadWait();
+}
 mpm_status mpm_solver_download_grid(mpm_solver* s, int32_t field, float* host_out) {
     MPM_TRY(check(s));
     if (!host_out) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -1263,6 +1338,14 @@ mpm_status mpm_batch_synchronize(mpm_batch* b) {
 mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.download(scene_id, field, host_out);
+}
+mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.downloadAsync(scene_id, field, host_out);
+}
+mpm_status mpm_batch_download_wait(mpm_batch* b) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.downloadWait();
 }
 mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
     if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");

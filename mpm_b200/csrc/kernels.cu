@@ -396,7 +396,8 @@ template <int S, int MODE, int STAGE = 16>
 struct P2GLayout {
     static constexpr int F = modeFields(MODE);
     static constexpr int NS = S * S * S;              // stencil nodes
-    static constexpr int NJ = (NS + 31) / 32;         // nodes per lane
+    static constexpr int PAIRS = S * S;               // (a, b) columns; a lane owns one column of S nodes
+    static constexpr int G = 32 / PAIRS;              // particle groups per warp (one particle each per pass)
     static constexpr int TN = tileNodes(S);
     static constexpr int TJ = (TN + kThreads - 1) / kThreads;
     static constexpr int SH = (MODE == MODE_MASS) ? 4 : (MODE == MODE_FLIP ? 12 : 20);  // shared floats
@@ -427,9 +428,11 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
     int* ctl = segEnd + L::kMaxSeg;                             // [0] segments, [1] next segment
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // lane -> stencil node(s): (a, b, c) and, for S = 4, (a, b, c + 2)
-    const int na = lane % S, nb = (lane / S) % S, nc = lane / (S * S);
-    const bool lane_on = lane < L::NS;
+    // lane -> particle group grp and stencil column (na, nb): the lane
+    // accumulates nodes (na, nb, 0..S-1) for the group's particles
+    // grp, grp + G, grp + 2G, ... of each staged batch.
+    const int grp = lane / L::PAIRS, na = (lane % L::PAIRS) % S, nb = (lane % L::PAIRS) / S;
+    const bool lane_on = grp < L::G;
     const uint32_t nact = args.counters[0];
     for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
         const BlockItem it = args.active[w];
@@ -498,11 +501,11 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                 if (sg >= rend) break;
                 const int cl = sg - r0;  // partial slot
                 const int beg = segBeg[sg], end = segEnd[sg];
-                float acc[L::NJ][F];
+                float acc[S][F];
 #pragma unroll
-                for (int j = 0; j < L::NJ; ++j)
+                for (int c = 0; c < S; ++c)
 #pragma unroll
-                    for (int f = 0; f < F; ++f) acc[j][f] = 0.f;
+                    for (int f = 0; f < F; ++f) acc[c][f] = 0.f;
                 for (int g0 = beg; g0 < end; g0 += L::kStage) {
                     const int np = min(L::kStage, end - g0);
                     if (lane < np) {
@@ -523,12 +526,22 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                         for (int a = 0; a < 3; ++a) {
                             const float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
                             delta[a] = x[a] - gp0;
-                            // node distances as the reference forms them, (x_p - (o + h i)) / h
+                            // Node distances.  The linear kernel's weights
+                            // have relative error ~ulp(d)/w near |d| = 1, so it
+                            // forms each one as the reference does,
+                            // (x_p - (o + h i)) / h; the B-splines are smooth
+                            // there and use d0 - k (exact subtraction).
                             float dk[S], wk[S], dwk[S];
+                            if (S == 2) {
 #pragma unroll
-                            for (int k = 0; k < S; ++k) {
-                                const float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
-                                dk[k] = __fdiv_rn(__fsub_rn(x[a], gp), h);
+                                for (int k = 0; k < S; ++k) {
+                                    const float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                                    dk[k] = __fdiv_rn(__fsub_rn(x[a], gp), h);
+                                }
+                            } else {
+                                dk[0] = __fdiv_rn(delta[a], h);
+#pragma unroll
+                                for (int k = 1; k < S; ++k) dk[k] = dk[0] - (float)k;
                             }
                             splineWeights<S>(dk, wk, dwk);
 #pragma unroll
@@ -578,81 +591,90 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                     }
                     __syncwarp();
                     if (lane_on) {
-                        const float fa = (float)na, fb = (float)nb, fc = (float)nc;
-                        for (int q = 0; q < np; ++q) {
+                        const float fa = (float)na, fb = (float)nb;
+                        for (int q = grp; q < np; q += L::G) {
                             const float* pq = st + q * L::P;
                             const float4 s0 = *reinterpret_cast<const float4*>(pq);
                             const float m = s0.x;
                             if (MODE == MODE_MASS) {
-                                const float w = pq[L::WB + na] * pq[L::WB + S + nb];
+                                const float mw = m * (pq[L::WB + na] * pq[L::WB + S + nb]);
 #pragma unroll
-                                for (int j = 0; j < L::NJ; ++j)
-                                    acc[j][0] = fmaf(m * w, pq[L::WB + 2 * S + nc + 2 * j], acc[j][0]);
+                                for (int c = 0; c < S; ++c) acc[c][0] = fmaf(mw, pq[L::WB + 2 * S + c], acc[c][0]);
                                 continue;
                             }
+                            // column factors: w = wab Z_c and
+                            // T grad w = Z_c A + Z'_c Bz with A = T (X'Y, XY', 0), Bz = T (0, 0, XY)
                             const float2 xa = *reinterpret_cast<const float2*>(pq + L::WB + 2 * na);
                             const float2 yb = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (S + nb));
-                            const float wab = xa.x * yb.x, dawb = xa.y * yb.x, wadb = xa.x * yb.y;
+                            const float wab = xa.x * yb.x, dab = xa.y * yb.x, adb = xa.x * yb.y;
                             float T[6], u[3], hc2[3];
-                            float hC[9];
                             if (MODE == MODE_FLIP) {
                                 const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
                                 const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
                                 T[0] = s1.x; T[1] = s1.y; T[2] = s1.z; T[3] = s1.w; T[4] = s2.x; T[5] = s2.y;
                                 u[0] = s0.y; u[1] = s0.z; u[2] = s0.w;
+                                hc2[0] = hc2[1] = hc2[2] = 0.f;
                             } else {
                                 const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
                                 const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
                                 const float4 s3 = *reinterpret_cast<const float4*>(pq + 12);
                                 const float4 s4 = *reinterpret_cast<const float4*>(pq + 16);
-                                hC[0] = s1.x; hC[1] = s1.y; hC[2] = s1.z; hC[3] = s1.w;
-                                hC[4] = s2.x; hC[5] = s2.y; hC[6] = s2.z; hC[7] = s2.w; hC[8] = s3.x;
+                                const float hC[9] = {s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, s2.w, s3.x};
                                 T[0] = s3.y; T[1] = s3.z; T[2] = s3.w; T[3] = s4.x; T[4] = s4.y; T[5] = s4.z;
                                 const float qv[3] = {s0.y, s0.z, s0.w};
 #pragma unroll
                                 for (int i = 0; i < 3; ++i) {
-                                    u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, fmaf(hC[3 * i + 2], fc, qv[i])));
-                                    hc2[i] = 2.0f * hC[3 * i + 2];
+                                    u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, qv[i]));
+                                    hc2[i] = hC[3 * i + 2];
                                 }
                             }
+                            const float A[3] = {fmaf(T[0], dab, T[3] * adb), fmaf(T[3], dab, T[1] * adb),
+                                                fmaf(T[4], dab, T[5] * adb)};
+                            const float Bz[3] = {T[4] * wab, T[5] * wab, T[2] * wab};
 #pragma unroll
-                            for (int j = 0; j < L::NJ; ++j) {
-                                if (j > 0 && lane + 32 * j >= L::NS) break;
-                                const float2 zc = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (2 * S + nc + 2 * j));
+                            for (int c = 0; c < S; ++c) {
+                                const float2 zc = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (2 * S + c));
                                 const float wgt = wab * zc.x;
-                                const float gx = dawb * zc.x, gy = wadb * zc.x, gz = wab * zc.y;
-                                const float tg0 = fmaf(T[0], gx, fmaf(T[3], gy, T[4] * gz));
-                                const float tg1 = fmaf(T[3], gx, fmaf(T[1], gy, T[5] * gz));
-                                const float tg2 = fmaf(T[4], gx, fmaf(T[5], gy, T[2] * gz));
-                                acc[j][0] = fmaf(m, wgt, acc[j][0]);
-                                if (j > 0 && MODE != MODE_FLIP) {
+                                acc[c][0] = fmaf(m, wgt, acc[c][0]);
+                                if (c > 0 && MODE != MODE_FLIP) {
 #pragma unroll
                                     for (int i = 0; i < 3; ++i) u[i] += hc2[i];
                                 }
                                 if (MODE == MODE_APIC_FUSED) {
-                                    acc[j][1] += fmaf(wgt, u[0], tg0);
-                                    acc[j][2] += fmaf(wgt, u[1], tg1);
-                                    acc[j][3] += fmaf(wgt, u[2], tg2);
+#pragma unroll
+                                    for (int i = 0; i < 3; ++i)
+                                        acc[c][1 + i] = fmaf(zc.y, Bz[i], fmaf(zc.x, A[i], fmaf(wgt, u[i], acc[c][1 + i])));
                                 } else {  // PIC-FLIP and SPLIT keep p and f apart
-                                    acc[j][1] = fmaf(wgt, u[0], acc[j][1]);
-                                    acc[j][2] = fmaf(wgt, u[1], acc[j][2]);
-                                    acc[j][3] = fmaf(wgt, u[2], acc[j][3]);
-                                    acc[j][4] += tg0;
-                                    acc[j][5] += tg1;
-                                    acc[j][6] += tg2;
+#pragma unroll
+                                    for (int i = 0; i < 3; ++i) {
+                                        acc[c][1 + i] = fmaf(wgt, u[i], acc[c][1 + i]);
+                                        acc[c][4 + i] = fmaf(zc.y, Bz[i], fmaf(zc.x, A[i], acc[c][4 + i]));
+                                    }
                                 }
                             }
                         }
                     }
                     __syncwarp();
                 }
-                float* pc = partial + (size_t)cl * F * 64;
+                // Sum the groups' columns in group order into group 0 (fixed
+                // order, so the partial does not depend on timing).
 #pragma unroll
-                for (int j = 0; j < L::NJ; ++j) {
-                    const int k = lane + 32 * j;
-                    if (k < L::NS)
+                for (int c = 0; c < S; ++c)
 #pragma unroll
-                        for (int f = 0; f < F; ++f) pc[f * 64 + k] = acc[j][f];
+                    for (int f = 0; f < F; ++f) {
+                        const float mine = acc[c][f];
+                        float sum = mine;
+#pragma unroll
+                        for (int g = 1; g < L::G; ++g)
+                            sum += __shfl_sync(0xffffffffu, mine, min(lane + g * L::PAIRS, 31));
+                        acc[c][f] = sum;
+                    }
+                if (grp == 0) {
+                    float* pc = partial + (size_t)cl * F * 64 + na + S * nb;
+#pragma unroll
+                    for (int c = 0; c < S; ++c)
+#pragma unroll
+                        for (int f = 0; f < F; ++f) pc[f * 64 + L::PAIRS * c] = acc[c][f];
                 }
             }
             __syncthreads();
@@ -1155,6 +1177,32 @@ __global__ void advectKernel(const SceneDev* __restrict__ scenes, int parity, fl
         for (int a = 0; a < 3; ++a) f[(F_X + a) * cap + i] += dt * f[(F_V + a) * cap + i];
 }
 
+// Particle state of a new scene from the caller's arrays staged on the device
+// as [x: 3n interleaved][v: 3n interleaved][m: n][V0: n, prescribed only]:
+// SoA planes with Fe = Fp = I, B = tau = 0 and V0 = 0 unless prescribed
+// (the reference's MaterialPoint3D constructor, src/material_point3d.cu:10-30).
+__global__ void initStateKernel(float* __restrict__ f, uint32_t* __restrict__ pid, size_t cap,
+                                const float* __restrict__ staged, size_t n, int has_volume) {
+    for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            f[(F_X + a) * cap + i] = staged[3 * i + a];
+            f[(F_V + a) * cap + i] = staged[3 * n + 3 * i + a];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            f[(F_FE + k) * cap + i] = (k % 4 == 0) ? 1.f : 0.f;
+            f[(F_FP + k) * cap + i] = (k % 4 == 0) ? 1.f : 0.f;
+            f[(F_B + k) * cap + i] = 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) f[(F_TAU + k) * cap + i] = 0.f;
+        f[F_MASS * cap + i] = staged[6 * n + i];
+        f[F_VOL * cap + i] = has_volume ? staged[7 * n + i] : 0.f;
+        pid[i] = (uint32_t)i;
+    }
+}
+
 // initialize(): V0 = m / (sum_i m_i w_ip / h^3) with node masses in vstar.w
 // (src/mpm_solver3d.cu:173-214).  Live order, dense node reads.
 template <int S>
@@ -1367,6 +1415,13 @@ void launchParticlesCollision(const LaunchCtx& c, int parity, float dt) {
 void launchAdvect(const LaunchCtx& c, int parity, float dt) {
     noteLaunches(1);
     advectKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, dt);
+}
+void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, size_t cap, const float* staged, size_t n,
+                     bool has_volume) {
+    if (n == 0) return;
+    noteLaunches(1);
+    const unsigned blocks = (unsigned)std::min<size_t>((n + kThreads - 1) / kThreads, (size_t)num_sms * 8);
+    initStateKernel<<<blocks, kThreads, 0, st>>>(f, pid, cap, staged, n, has_volume ? 1 : 0);
 }
 void launchVolume(const LaunchCtx& c, int parity, int S) {
     noteLaunches(1);

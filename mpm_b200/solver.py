@@ -259,6 +259,15 @@ class _SolverBase:
         check(self._lib.mpm_solver_download(self._h, int(field), C.cast(C.c_void_p(ptr), C.POINTER(C.c_float))),
               "download")
 
+    def download_async(self, field: int, ptr: int):
+        """Queue a download of the current state into caller memory at address
+        ptr (pinned host memory to overlap later steps); the data is complete
+        after download_wait() or synchronize()."""
+        check(self._lib.mpm_solver_download_async(self._h, int(field), C.c_void_p(ptr)), "download_async")
+
+    def download_wait(self):
+        check(self._lib.mpm_solver_download_wait(self._h), "download_wait")
+
     def profile(self, enable: bool = True):
         check(self._lib.mpm_solver_profile(self._h, 1 if enable else 0), "profile")
 

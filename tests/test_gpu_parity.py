@@ -398,3 +398,27 @@ def test_batch_add_remove_between_steps(gpu):
         assert np.array_equal(b.download(ia, _abi.FIELD_POSITION), ga.download(_abi.FIELD_POSITION))
         assert np.array_equal(b.download(ic, _abi.FIELD_POSITION), gc.download(_abi.FIELD_POSITION))
         assert np.array_equal(b.download(ic, _abi.FIELD_FE), gc.download(_abi.FIELD_FE))
+
+
+def test_download_async_matches_sync(gpu):
+    """Queued asynchronous downloads (more than the two staging buffers, and of
+    different sizes) deliver the same bytes as synchronous downloads of the
+    same states."""
+    import torch
+    sc = scenes.snow_cube()
+    a, b = sc.solver(), sc.solver()
+    fields = [_abi.FIELD_POSITION4, _abi.FIELD_FE, _abi.FIELD_POSITION4, _abi.FIELD_VELOCITY, _abi.FIELD_POSITION4]
+    outs, expect = [], []
+    for f in fields:
+        a.step(1)
+        b.step(1)
+        comps = _abi.FIELD_COMPONENTS[f]
+        buf = torch.full((sc.n, comps), float("nan"), dtype=torch.float32).pin_memory()
+        a.download_async(f, buf.data_ptr())
+        outs.append(buf)
+        expect.append(b.download(f).reshape(sc.n, comps))
+    a.download_wait()
+    for f, got, ref in zip(fields, outs, expect):
+        assert np.array_equal(got.numpy(), ref), f
+    a.close()
+    b.close()

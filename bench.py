@@ -3,20 +3,25 @@
 
 Workload (default): the two-ball collision -- 1,048,576 particles in two
 spheres, 128^3 grid, cubic B-spline APIC, dt 5e-5 (seeded synthetic input).
-A "step" is one simulateOneStep of the whole scene.
+A "step" is one simulateOneStep of the whole scene.  `--workload batch64`
+times the 64-scene batch (8.56M particles, quadratic, half APIC / half
+PIC-FLIP) as one batched step; `snow_cube` (65,536 particles, 64^3) and
+`large_slab` (8,388,608 particles, 256^3) are the other single scenes.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpm_b200|reference]
 
 N > 1 runs one process per GPU (torchrun); every rank advances its own
-replica of the scene (scene-parallel, no data-path collective), and the value
-is the whole-job particle-steps/s over the max-over-ranks device time.
-`--impl reference` times the reference's step math restated on the host CPU
-(oracle/, FP32, OpenMP on every host core) on the same workload.
+replica of the scene (batch64: its share of the 64 scenes; scene-parallel,
+no data-path collective), and the value is the whole-job particle-steps/s
+over the max-over-ranks device time.  `--impl reference` times the
+reference's step math restated on the host CPU (oracle/, FP32, OpenMP on
+every host core) on the same workload.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes as C
+import dataclasses
 import json
 import os
 import subprocess
@@ -30,7 +35,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s"
-WORKLOADS = ("two_balls", "snow_cube", "large_slab")
+WORKLOADS = ("two_balls", "snow_cube", "large_slab", "batch64")
+NAIVE_KIND = ("reference-naive CUDA restatement on the same B200 (AoS 236 B APIC / 128 B FLIP points, 52 B nodes, "
+              "7 float atomics per particle-node, per-node FP64-literal splines, 2 SVDs per particle, "
+              "synchronised launch per sub-step)")
 
 
 def parse():
@@ -48,21 +56,52 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-naive", action="store_true", help="skip the reference-naive GPU baseline leg")
     ap.add_argument("--naive-budget-s", type=float, default=10.0)
+    ap.add_argument("--batch-scenes", type=int, default=64,
+                    help="batch64: use only the first K scenes (small cases for profiling)")
     return ap.parse_args()
 
 
-def make_scene(name):
-    from mpm_b200 import scenes
-    return {"two_balls": scenes.two_balls, "snow_cube": scenes.snow_cube, "large_slab": scenes.large_slab}[name]()
+# --- workloads --------------------------------------------------------------
+class Work:
+    """The scenes one rank advances: a single scene (one solver) or a share of
+    the 64-scene batch (one Batch)."""
 
+    def __init__(self, name, rank=0, ws=1, batch_scenes=64):
+        from mpm_b200 import scenes
+        from mpm_b200.sharding import scenes_for_rank
+        self.name = name
+        self.batched = name == "batch64"
+        if self.batched:
+            self.scenes = scenes_for_rank(scenes.batched_scenes()[:batch_scenes], rank, ws)
+        else:
+            self.scenes = [{"two_balls": scenes.two_balls, "snow_cube": scenes.snow_cube,
+                            "large_slab": scenes.large_slab}[name]()]
+        self.n = sum(s.n for s in self.scenes)
+        self.nscenes = min(batch_scenes, 64) if self.batched else 1
 
-def config_of(sc, n_gpus):
-    from mpm_b200 import _abi
-    return {"workload": sc.name, "particles_per_gpu": sc.n, "grid": list(sc.resolution),
-            "transfer": "APIC" if sc.transfer == _abi.TRANSFER_APIC else "PIC-FLIP",
-            "interpolation": ["linear", "quadratic", "cubic"][sc.interpolation], "dt": sc.dt,
-            "parallelism": f"scene-replicas x{n_gpus}",
-            "l2": "inputs larger than L2 (particle state %.0f MB)" % (sc.n * 41 * 4 * 2 / 1e6)}
+    def engine(self, device=None, scenes=None):
+        scenes = scenes if scenes is not None else self.scenes
+        if not self.batched:
+            return scenes[0].solver(device=device)
+        from mpm_b200.batch import Batch
+        b = Batch(device=device)
+        b.scene_ids = [b.add(s) for s in scenes]
+        return b
+
+    def config(self, ws):
+        from mpm_b200 import _abi
+        if not self.batched:
+            sc = self.scenes[0]
+            return {"workload": sc.name, "particles_per_gpu": sc.n, "grid": list(sc.resolution),
+                    "transfer": "APIC" if sc.transfer == _abi.TRANSFER_APIC else "PIC-FLIP",
+                    "interpolation": ["linear", "quadratic", "cubic"][sc.interpolation], "dt": sc.dt,
+                    "parallelism": f"scene-replicas x{ws}",
+                    "l2": "inputs larger than L2 (particle state %.0f MB)" % (sc.n * 41 * 4 * 2 / 1e6)}
+        return {"workload": "batch64: %d of the 64 seeded scenes (N log-uniform 10k-500k, grids 32-128^3, "
+                            "quadratic, half APIC / half PIC-FLIP, dt 1e-4) in one batched step" % self.nscenes,
+                "scenes_on_rank0": len(self.scenes), "particles_on_rank0": self.n,
+                "parallelism": f"scenes split over {ws} GPU(s)",
+                "l2": "inputs larger than L2 (particle state %.0f MB)" % (self.n * 41 * 4 * 2 / 1e6)}
 
 
 # --- distributed plumbing ---------------------------------------------------
@@ -156,20 +195,33 @@ class ClockSampler:
 
 
 # --- roofline ---------------------------------------------------------------
-def algorithmic_bytes(sc, family, stats):
-    """Algorithmic bytes of one launch: per particle-step SoA FP32 state read
-    once and written once, plus per active grid node (m and momentum/force
-    into the grid, v* out of it)."""
+# Algorithmic bytes per particle-step and per active grid node, (APIC, PIC-FLIP):
+# the SoA FP32 state read once and written once.
+PARTICLE_BYTES = {
+    "p2g": (140, 104),            # x v Fe Fp m V0 (+B) in
+    "g2p": (132 + 132, 96 + 96),  # state in (no m, V0), state out
+    "grid": (0, 0),
+}
+NODE_BYTES = {
+    "p2g": (16, 28),              # m, p + dt f (or p, f) out
+    "g2p": (12, 24),              # v* (and v) gathered
+    "grid": (16 + 12, 28 + 24),   # tile sums in, v* (v) out
+}
+
+
+def algorithmic_bytes(scenes, family, stats):
+    """Algorithmic bytes of one launch family.  Active nodes are counted over
+    all scenes; their per-node bytes are weighted by the APIC / PIC-FLIP
+    particle split."""
     from mpm_b200 import _abi
-    apic = sc.transfer == _abi.TRANSFER_APIC
-    n, nodes = sc.n, stats["active_nodes"]
-    if family == "p2g":  # x v Fe Fp m V0 (+B) in; m, p(+dt f) (or p, f) out
-        return n * (140 if apic else 104) + nodes * (16 if apic else 28)
-    if family == "g2p":  # state in (no m, V0), state out, v* (v) gathered
-        return n * ((132 + 132) if apic else (96 + 96)) + nodes * (12 if apic else 24)
-    if family == "grid":  # tile sums in, v* (v) out
-        return nodes * ((16 + 12) if apic else (28 + 24))
-    return 0
+    if family not in PARTICLE_BYTES:
+        return 0
+    n_apic = sum(s.n for s in scenes if s.transfer == _abi.TRANSFER_APIC)
+    n_flip = sum(s.n for s in scenes) - n_apic
+    pa, pf = PARTICLE_BYTES[family]
+    na, nf = NODE_BYTES[family]
+    frac = n_apic / max(n_apic + n_flip, 1)
+    return n_apic * pa + n_flip * pf + stats["active_nodes"] * (frac * na + (1 - frac) * nf)
 
 
 def peaks():
@@ -188,54 +240,71 @@ def traffic_of(family, workload):
     return d.get(workload, {}).get(family)
 
 
-# --- CPU baseline -------------------------------------------------------------
-def cpu_rate(sc, budget_s, steps_hint=None):
+# --- CPU and naive-GPU baselines --------------------------------------------------
+def cpu_rate(work, budget_s, steps_hint=None):
     """Reference step math (oracle, FP32 restatement) on all host cores: full
-    steps of the same scene, as many as fit the time budget (at least one)."""
+    steps of the workload's scenes, as many as fit the time budget.
+    Returns (rate, threads, sample description, steps, seconds)."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    o = O.OracleSolver(sc.desc(), sc.particles, bits=32, threads=threads)
-    t0 = time.perf_counter()
-    o.step(1)
-    t1 = time.perf_counter() - t0
-    k = max(1, min(int(budget_s / max(t1, 1e-9)), steps_hint or 10 ** 9))
-    t0 = time.perf_counter()
-    o.step(k)
-    dt = time.perf_counter() - t0
-    return sc.n * k / dt, threads, k, dt
+    if len(work.scenes) == 1:
+        sc = work.scenes[0]
+        o = O.OracleSolver(sc.desc(), sc.particles, bits=32, threads=threads)
+        t0 = time.perf_counter()
+        o.step(1)
+        t1 = time.perf_counter() - t0
+        k = max(1, min(int(budget_s / max(t1, 1e-9)), steps_hint or 10 ** 9))
+        t0 = time.perf_counter()
+        o.step(k)
+        dt = time.perf_counter() - t0
+        return sc.n * k / dt, threads, f"{k} full steps of the {sc.n}-particle scene", k, dt
+    done, dt, used = 0, 0.0, 0
+    for sc in work.scenes:  # one step of each scene in turn, within the budget
+        o = O.OracleSolver(sc.desc(), sc.particles, bits=32, threads=threads)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(1)
+        dt += time.perf_counter() - t0
+        done += sc.n
+        used += 1
+        if dt > budget_s:
+            break
+    return done / dt, threads, f"1 step of each of the first {used} scenes ({done} particle-steps)", 1, dt
 
 
-def naive_rate(sc, budget_s):
-    """The reference-naive GPU restatement (baseline/naive) on the same scene
+def naive_rate(work, budget_s):
+    """The reference-naive GPU restatement (baseline/naive) on the same scenes
     and GPU: AoS state, float atomics, per-node spline evaluation, one
-    synchronised launch per sub-step.  Steps timed with CUDA events on the
-    legacy stream, as many as fit the budget (at least 3)."""
+    synchronised launch per sub-step, scenes stepped one after the other.
+    Steps timed with CUDA events, as many as fit the budget (at least 3)."""
     sys.path.insert(0, os.path.join(ROOT, "baseline", "naive"))
     import naive as NV
-    g = NV.NaiveSolver(sc.desc(), sc.particles)
-    g.step(2)
-    t1 = g.timed_step(2) / 2e3
+    gs = [NV.NaiveSolver(s.desc(), s.particles) for s in work.scenes]
+    for g in gs:
+        g.step(2)
+    t1 = sum(g.timed_step(1) for g in gs) / 1e3
     k = int(max(3, min(1000, budget_s / max(t1, 1e-6))))
-    ms = g.timed_step(k)
-    g.close()
-    return {"value": sc.n * k / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / k, "steps": k,
-            "kind": "reference-naive CUDA restatement on the same B200 (AoS 236 B APIC / 128 B FLIP points, "
-                    "52 B nodes, 7 float atomics per particle-node, per-node FP64-literal splines, "
-                    "2 SVDs per particle, synchronised launch per sub-step)"}
+    ms = 0.0
+    for _ in range(k):
+        ms += sum(g.timed_step(1) for g in gs)
+    for g in gs:
+        g.close()
+    return {"value": work.n * k / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / k, "steps": k, "kind": NAIVE_KIND}
 
 
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    sc = make_scene(args.workload)
+    work = Work(args.workload, batch_scenes=args.batch_scenes)
     # budget: the whole --steps/--warmup run finishes within a few minutes
-    value, threads, k, dt = cpu_rate(sc, budget_s=min(150.0, 1.5 * (args.steps + args.warmup)), steps_hint=args.steps)
+    value, threads, sample, k, dt = cpu_rate(work, budget_s=min(150.0, 1.5 * (args.steps + args.warmup)),
+                                             steps_hint=args.steps)
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": k,
            "warmup": 1, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
-           "config": config_of(sc, 1),
+           "config": work.config(1),
            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                            "sample": f"{k} full steps of the {sc.n}-particle scene after 1 untimed step"},
+                            "sample": sample + " after 1 untimed step"},
            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -245,8 +314,8 @@ def run_ours(args, ws, rank, local):
     from mpm_b200 import _abi
     lib = _abi.load()
     _abi.check(lib.mpm_set_device(local), "mpm_set_device")
-    sc = make_scene(args.workload)
-    g = sc.solver()
+    work = Work(args.workload, rank, ws, args.batch_scenes)
+    g = work.engine()
     g.step(args.warmup)
     g.synchronize()
     launches0 = C.c_uint64()
@@ -261,49 +330,49 @@ def run_ours(args, ws, rank, local):
     prof = g.profile_read()
     g.profile(False)
     stats = g.stats()
+    g.close()
     t_max = allmax(ws, ms) / 1e3
-    total = allsum(ws, float(sc.n * args.steps))
+    total = allsum(ws, float(work.n * args.steps))
     value = total / t_max
 
     fams = {k: v for k, v in prof.items() if k in ("p2g", "g2p", "grid", "sort")}
     dom = max(fams, key=lambda k: fams[k][0] * fams[k][1])
     dur = fams[dom][0] * 1e-3
-    byt = algorithmic_bytes(sc, dom, stats)
+    byt = algorithmic_bytes(work.scenes, dom, stats)
     peak, peak_kind = peaks()
     achieved = byt / dur / 1e9 if dur > 0 and byt > 0 else None
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": traffic_of(dom, sc.name), "algorithmic_bytes": byt, "avg_launch_ms": fams[dom][0],
+            "traffic": traffic_of(dom, work.name), "algorithmic_bytes": byt, "avg_launch_ms": fams[dom][0],
             "kernel_ms": {k: v[0] for k, v in prof.items()}}
 
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(sc, args.steps, ws)
-
-    forms = None
-    if not args.no_forms:
-        forms = run_forms(args, ws, local)
+        e2e = run_e2e(work, args.steps, ws)
 
     naive = None
     if rank == 0 and ws == 1 and not args.no_naive:
-        naive = naive_rate(sc, args.naive_budget_s)
+        naive = naive_rate(work, args.naive_budget_s)
         naive["speedup"] = value / naive["value"]
+
+    forms = None
+    if not args.no_forms and not work.batched:
+        forms = run_forms(args, ws, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, threads, k, dt = cpu_rate(sc, args.cpu_budget_s)
+        v, threads, sample, k, dt = cpu_rate(work, args.cpu_budget_s)
         cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
-               "sample": f"{k} full steps of the {sc.n}-particle scene (oracle FP32, OpenMP)"}
+               "sample": sample + " (oracle FP32, OpenMP)"}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-               "config": config_of(sc, ws), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+               "config": work.config(ws), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(launches1.value - launches0.value), "clocks": clk.summary(),
                "stats": stats, "naive_gpu": naive, "forms": forms}
         print(json.dumps(out), flush=True)
-    g.close()
 
 
 def run_forms(args, ws, local):
@@ -316,18 +385,12 @@ def run_forms(args, ws, local):
     served:  a Poisson stream of scene requests (rate 20/s) replayed for
              --serve-seconds with particle counts scaled by --serve-scale."""
     from mpm_b200 import scenes
-    from mpm_b200.batch import Batch
     from mpm_b200.serving import Server
-    from mpm_b200.sharding import scenes_for_rank
     out = {}
     steps = min(args.steps, 100)
-    # with several GPUs the 64 scenes are split across ranks (scene-parallel)
     rank = int(os.environ.get("RANK", "0"))
-    scs = scenes_for_rank(scenes.batched_scenes(), rank, ws)
-    ntot = sum(s.n for s in scs)
-    with Batch(device=local) as b:
-        for s in scs:
-            b.add(s)
+    work = Work("batch64", rank, ws)  # with several GPUs the 64 scenes are split across ranks
+    with work.engine(device=local) as b:
         b.step(3)
         b.synchronize()
         b.profile(True)
@@ -336,11 +399,11 @@ def run_forms(args, ws, local):
         prof = b.profile_read()
         st = b.stats()
     t = allmax(ws, ms) / 1e3
-    out["batched"] = {"workload": "64 seeded scenes split over %d GPU(s); %d particles on rank %d" % (ws, ntot, rank),
+    out["batched"] = {"workload": "64 seeded scenes split over %d GPU(s); %d particles on rank %d" % (ws, work.n, rank),
                       "steps": steps,
-                      "value": allsum(ws, float(ntot * steps)) / t, "ms_per_step": t / steps * 1e3,
+                      "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3,
                       "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st}
-    solvers = [s.solver() for s in scs]
+    solvers = [s.solver(device=local) for s in work.scenes]
     for g in solvers:
         g.step(3)
     for g in solvers:
@@ -356,7 +419,7 @@ def run_forms(args, ws, local):
     for g in solvers:
         g.close()
     out["plain"] = {"workload": "same 64 scenes as 64 solvers", "steps": steps,
-                    "value": allsum(ws, float(ntot * steps)) / t, "ms_per_step": t / steps * 1e3}
+                    "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3}
     out["batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
     reqs = scenes.serving_requests(rate=20.0, duration=args.serve_seconds, scale=args.serve_scale)
     srv = Server(budget_bytes=150e9, device=local, keep_state=False)
@@ -369,43 +432,44 @@ def run_forms(args, ws, local):
     return out
 
 
-def run_e2e(sc, steps, ws):
+def run_e2e(work, steps, ws):
     """Same metric through the public API with host buffers: construct the
-    solver from pinned host arrays (H2D), then every step download the
-    (x, y, z, 1) positions into pinned host memory (D2H, asynchronous, into
-    two alternating buffers, so the copy of step k overlaps step k + 1); the
-    clock stops after the last copy has landed."""
+    solver (or batch) from pinned host arrays (H2D), then every step download
+    every scene's (x, y, z, 1) positions into pinned host memory (D2H,
+    asynchronous, into two alternating buffers per scene, so the copy of step
+    k overlaps step k + 1); the clock stops after the last copy has landed."""
     import torch
     from mpm_b200 import _abi
-    from mpm_b200.solver import APICMPMSolver3D, MPMSolver3D, Particles
-    n = sc.n
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    p = Particles(pin(sc.particles.positions), pin(sc.particles.velocities), pin(sc.particles.mass),
-                  sc.particles.materials, None, None)
-    outs = [torch.empty((n, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
-    opts = dict(gravity=sc.gravity, boundary=sc.boundary, sticky_cells=sc.sticky_cells, volume_mode=sc.volume_mode)
+    from mpm_b200.solver import Particles
+    pin = lambda a: torch.from_numpy(np.array(a, copy=True)).pin_memory().numpy()
+    pinned = []
+    for sc in work.scenes:
+        p = sc.particles
+        pp = Particles(pin(p.positions), pin(p.velocities), pin(p.mass), p.materials,
+                       None if p.material is None else pin(p.material), None if p.volume is None else pin(p.volume))
+        pinned.append(dataclasses.replace(sc, particles=pp))
+    outs = [[torch.empty((sc.n, 4), dtype=torch.float32).pin_memory() for _ in range(2)] for sc in work.scenes]
     barrier(ws)
     t0 = time.perf_counter()
-    if sc.transfer == _abi.TRANSFER_APIC:
-        g = APICMPMSolver3D(p, sc.origin, sc.resolution, sc.stride, sc.friction, sc.interpolation, sc.dt, **opts)
-    else:
-        g = MPMSolver3D(p, sc.origin, sc.resolution, sc.stride, sc.friction, sc.blend, sc.interpolation, sc.dt,
-                        **opts)
+    g = work.engine(scenes=pinned)
     for k in range(steps):
         g.step(1)
-        # this step's positions into alternating pinned buffers; the copy
-        # overlaps the next step (download_async)
-        g.download_async(_abi.FIELD_POSITION4, outs[k % 2].data_ptr())
+        if work.batched:
+            for j, sid in enumerate(g.scene_ids):
+                g.download_async(sid, _abi.FIELD_POSITION4, outs[j][k % 2].data_ptr())
+        else:
+            g.download_async(_abi.FIELD_POSITION4, outs[0][k % 2].data_ptr())
     g.download_wait()
     dt = time.perf_counter() - t0
     g.close()
     barrier(ws)
     t = allmax(ws, dt)
-    h2d = n * (3 + 3 + 1) * 4
-    return {"value": allsum(ws, float(n * steps)) / t, "unit": METRIC, "h2d_bytes_per_step": h2d / steps,
-            "d2h_bytes_per_step": 16 * n, "timed": "solver construction (H2D of the particles) + per step: "
-            "step + asynchronous download of float4 positions into pinned host memory, "
-            "until the last copy has landed"}
+    h2d = sum(sc.n * (7 + (1 if sc.particles.volume is not None else 0)) * 4 +
+              (2 * sc.n if sc.particles.material is not None else 0) for sc in work.scenes)
+    return {"value": allsum(ws, float(work.n * steps)) / t, "unit": METRIC, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": 16 * work.n, "timed": "construction from pinned host arrays (H2D of the "
+            "particles) + per step: step + asynchronous download of every scene's float4 positions into pinned "
+            "host memory, until the last copy has landed"}
 
 
 def main():

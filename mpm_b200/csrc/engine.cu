@@ -98,7 +98,22 @@ struct SceneHost {
     int nmat = 1;
     bool need_init = true;
     bool stress_stale = true;  // cached tau must be recomputed from Fe/Fp
+    // asynchronous downloads: two staging buffers, each with the event of its
+    // gather (ready) and of its copy to the host (done)
+    DevMem stage[2];
+    cudaEvent_t stage_ready[2] = {}, stage_done[2] = {};
+    bool stage_pending[2] = {};
+    int stage_next = 0;
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
+    ~SceneHost() {
+        for (int k = 0; k < 2; ++k) {
+            if (stage_done[k]) {
+                cudaEventSynchronize(stage_done[k]);  // no copy may still read the staging buffer
+                cudaEventDestroy(stage_done[k]);
+            }
+            if (stage_ready[k]) cudaEventDestroy(stage_ready[k]);
+        }
+    }
 };
 
 class Engine {
@@ -106,14 +121,9 @@ public:
     Engine() {}
     ~Engine() {
         if (stream_) cudaStreamSynchronize(stream_);
-        if (copy_stream_) {
-            cudaStreamSynchronize(copy_stream_);
-            for (int k = 0; k < 2; ++k) {
-                if (stage_ready_[k]) cudaEventDestroy(stage_ready_[k]);
-                if (stage_done_[k]) cudaEventDestroy(stage_done_[k]);
-            }
-            cudaStreamDestroy(copy_stream_);
-        }
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+        scenes_.clear();  // their staging events before the copy stream
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
         dropGraphs();
         for (int k = 0; k < KF_COUNT; ++k) {
             if (ev_[k][0]) cudaEventDestroy(ev_[k][0]);
@@ -373,8 +383,9 @@ public:
         max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
         MPM_TRY(active_.alloc(sizeof(BlockItem) * max_active_, "active blocks"));
         MPM_TRY(outside_.alloc(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
-        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 4, "counters"));
-        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 4, stream_));
+        // [0] work items, [1] outside items, [2] active nodes, [8..13] item schedulers
+        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 16, "counters"));
+        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 16, stream_));
         MPM_TRY(block_slot_.alloc(sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
         for (auto& s : scenes_) maxS = std::max(maxS, s->S);
@@ -428,6 +439,7 @@ public:
         a.block_count = block_count_.as<uint32_t>();
         a.err = err_.as<uint32_t>();
         a.stats = counters_.as<uint32_t>();
+        a.sched = counters_.as<uint32_t>() + 8;
         return a;
     }
 
@@ -864,12 +876,12 @@ public:
         return MPM_OK;
     }
 
-    // Asynchronous download: the gather into one of two device staging
-    // buffers runs in stream order (it reads the current state), the copy to
-    // the host runs on a separate copy stream, so it overlaps the steps that
-    // follow (they write the other particle buffer and never the staging
-    // buffers).  A staging buffer is reused only after its previous copy has
-    // finished (the compute stream waits for that copy's event).
+    // Asynchronous download: the gather into one of the scene's two device
+    // staging buffers runs in stream order (it reads the current state), the
+    // copy to the host runs on a separate copy stream, so it overlaps the
+    // steps that follow (they write the other particle buffer and never the
+    // staging buffers).  A staging buffer is reused only after its previous
+    // copy has finished (the compute stream waits for that copy's event).
     mpm_status downloadAsync(int id, int field, float* host) {
         MPM_TRY(ensureReady());
         int idx = sceneIndex(id);
@@ -882,28 +894,27 @@ public:
         if (field == MPM_FIELD_B && s.desc.transfer != MPM_TRANSFER_APIC)
             return fail(MPM_ERR_INVALID_ARG, "B is only defined for APIC scenes");
         if (s.n == 0) return MPM_OK;
-        if (!copy_stream_) {
-            CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+        if (!copy_stream_) CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+        if (!s.stage_ready[0])
             for (int k = 0; k < 2; ++k) {
-                CUDA_TRY(cudaEventCreateWithFlags(&stage_ready_[k], cudaEventDisableTiming));
-                CUDA_TRY(cudaEventCreateWithFlags(&stage_done_[k], cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&s.stage_ready[k], cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&s.stage_done[k], cudaEventDisableTiming));
             }
-        }
-        const int k = stage_next_;
-        stage_next_ ^= 1;
+        const int k = s.stage_next;
+        s.stage_next ^= 1;
         const size_t bytes = sizeof(float) * per * s.n;
-        if (stage_[k].bytes < bytes) {
-            if (stage_pending_[k]) CUDA_TRY(cudaEventSynchronize(stage_done_[k]));
-            MPM_TRY(stage_[k].alloc(bytes, "download staging buffer"));
+        if (s.stage[k].bytes < bytes) {
+            if (s.stage_pending[k]) CUDA_TRY(cudaEventSynchronize(s.stage_done[k]));
+            MPM_TRY(s.stage[k].alloc(bytes, "download staging buffer"));
         }
-        if (stage_pending_[k]) CUDA_TRY(cudaStreamWaitEvent(stream_, stage_done_[k], 0));
-        launchGatherField(ctx(), idx, parity_, base, comps, mode, stage_[k].as<float>());
+        if (s.stage_pending[k]) CUDA_TRY(cudaStreamWaitEvent(stream_, s.stage_done[k], 0));
+        launchGatherField(ctx(), idx, parity_, base, comps, mode, s.stage[k].as<float>());
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaEventRecord(stage_ready_[k], stream_));
-        CUDA_TRY(cudaStreamWaitEvent(copy_stream_, stage_ready_[k], 0));
-        CUDA_TRY(cudaMemcpyAsync(host, stage_[k].p, bytes, cudaMemcpyDeviceToHost, copy_stream_));
-        CUDA_TRY(cudaEventRecord(stage_done_[k], copy_stream_));
-        stage_pending_[k] = true;
+        CUDA_TRY(cudaEventRecord(s.stage_ready[k], stream_));
+        CUDA_TRY(cudaStreamWaitEvent(copy_stream_, s.stage_ready[k], 0));
+        CUDA_TRY(cudaMemcpyAsync(host, s.stage[k].p, bytes, cudaMemcpyDeviceToHost, copy_stream_));
+        CUDA_TRY(cudaEventRecord(s.stage_done[k], copy_stream_));
+        s.stage_pending[k] = true;
         return MPM_OK;
     }
 
@@ -911,7 +922,7 @@ public:
     mpm_status downloadWait() {
         if (!copy_stream_) return MPM_OK;
         CUDA_TRY(cudaStreamSynchronize(copy_stream_));
-        stage_pending_[0] = stage_pending_[1] = false;
+        for (auto& s : scenes_) s->stage_pending[0] = s->stage_pending[1] = false;
         return MPM_OK;
     }
 
@@ -1018,12 +1029,7 @@ private:
     DevMem keys_[2], vals_[2], hist_, scan32_, sort_scratch_, compact_scratch_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
-    // asynchronous downloads (downloadAsync)
-    cudaStream_t copy_stream_ = nullptr;
-    DevMem stage_[2];
-    cudaEvent_t stage_ready_[2] = {}, stage_done_[2] = {};
-    bool stage_pending_[2] = {};
-    int stage_next_ = 0;
+    cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)
     struct GraphSlot {
         cudaGraphExec_t exec = nullptr;
         uint64_t launches = 0;

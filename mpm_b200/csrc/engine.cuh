@@ -100,7 +100,26 @@ struct StepArgs {
     uint32_t* block_count;       // dense per block
     uint32_t* err;               // error flags
     uint32_t* stats;             // [2]: nodes with mass written by the grid pass
+    uint32_t* sched;             // work-item schedulers: [0..1] P2G, [4..5] G2P (zero between launches)
 };
+
+// Dynamic work-item scheduler of the persistent block kernels: sched[0]
+// hands out item indices, sched[1] counts the CTAs that have run out; the
+// last of those clears both, so every launch starts from zero without a
+// memset.  Call from all threads of the CTA; returns the CTA's next item.
+__device__ __forceinline__ uint32_t nextWorkItem(uint32_t* sched, uint32_t total, uint32_t* slot) {
+    __syncthreads();  // the previous item's shared memory is no longer read
+    if (threadIdx.x == 0) {
+        const uint32_t w = atomicAdd(&sched[0], 1u);
+        if (w >= total && atomicAdd(&sched[1], 1u) == gridDim.x - 1) {
+            sched[0] = 0u;
+            sched[1] = 0u;
+        }
+        *slot = w;
+    }
+    __syncthreads();
+    return *slot;
+}
 
 // P2G/grid-pass variants.
 enum P2GMode : int {

@@ -434,7 +434,10 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
     const int grp = lane / L::PAIRS, na = (lane % L::PAIRS) % S, nb = (lane % L::PAIRS) / S;
     const bool lane_on = grp < L::G;
     const uint32_t nact = args.counters[0];
-    for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
+    __shared__ uint32_t item_s;
+    for (;;) {
+        const uint32_t w = nextWorkItem(args.sched, nact, &item_s);
+        if (w >= nact) break;
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
@@ -1024,7 +1027,11 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
         for (int a = 0; a < 3; ++a) x[a] += dt * vn[a];  // advectParticles (:381-391)
         const uint32_t key = particleKey(sc, x, args.err);
         args.next_keys[gs] = key;
-        atomicAdd(&args.block_count[key >> 6], 1u);
+        // one atomic per distinct block among the converged lanes (sorted
+        // particles: a warp's lanes nearly always share their next block)
+        const uint32_t blk = key >> 6;
+        const uint32_t peers = __match_any_sync(__activemask(), blk);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&args.block_count[blk], (uint32_t)__popc(peers));
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -1061,7 +1068,10 @@ __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fuse
     const int want = APIC ? MPM_TRANSFER_APIC : MPM_TRANSFER_PIC_FLIP;
     const uint32_t nact = args.counters[0];
     const uint32_t nout = args.counters[1];
-    for (uint32_t w = blockIdx.x; w < nact + nout; w += gridDim.x) {
+    __shared__ uint32_t item_s;
+    for (;;) {
+        const uint32_t w = nextWorkItem(args.sched + 4, nact + nout, &item_s);
+        if (w >= nact + nout) break;
         const bool inside = w < nact;
         const BlockItem it = inside ? args.active[w] : args.outside[w - nact];
         const SceneDev& sc = args.scenes[it.scene];
@@ -1085,7 +1095,6 @@ __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fuse
         for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
             particleUpdate<S, APIC>(args, sc, it.start + i, inside ? tvs : nullptr, APIC ? nullptr : tvo, t0,
                                     fused != 0, pre + threadIdx.x * kPreStride);
-        __syncthreads();
     }
 }
 

@@ -172,18 +172,17 @@ __device__ __forceinline__ void jacobiRotate(float (&S)[3][3], float* V, int p, 
     sh = b ? w * sh : sstar;
     float c = fmaf(ch, ch, -sh * sh);
     float s = 2.0f * ch * sh;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float sp = S[k][p], sq = S[k][q];
-        S[k][p] = fmaf(c, sp, s * sq);
-        S[k][q] = fmaf(-s, sp, c * sq);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float sp = S[p][k], sq = S[q][k];
-        S[p][k] = fmaf(c, sp, s * sq);
-        S[q][k] = fmaf(-s, sp, c * sq);
-    }
+    // S <- G^T S G with G the (p, q) rotation; S is symmetric, so only its
+    // upper triangle is formed (r is the third index; S[r][r] is unchanged).
+    const int r = 3 - p - q;
+    const float spp = S[p][p], sqq = S[q][q], spq = S[p][q], spr = S[p][r], sqr = S[q][r];
+    const float cc = c * c, ss = s * s, cs = c * s;
+    const float t = 2.0f * cs * spq;
+    S[p][p] = fmaf(cc, spp, fmaf(ss, sqq, t));
+    S[q][q] = fmaf(ss, spp, fmaf(cc, sqq, -t));
+    S[p][q] = S[q][p] = fmaf(cc - ss, spq, cs * (sqq - spp));
+    S[p][r] = S[r][p] = fmaf(c, spr, s * sqr);
+    S[q][r] = S[r][q] = fmaf(-s, spr, c * sqr);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         float vp = V[3 * k + p], vq = V[3 * k + q];
@@ -235,12 +234,12 @@ __device__ __forceinline__ void qrRotate(float* B, float* U, int p, int q) {
 }
 
 __device__ __forceinline__ void svd3(const float* A, float* U, float* s, float* V) {
-    float S[3][3];
+    float S[3][3];  // A^T A (symmetric: upper triangle formed, mirrored)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
-            S[i][j] = fmaf(A[6 + i], A[6 + j], fmaf(A[3 + i], A[3 + j], A[i] * A[j]));
+        for (int j = i; j < 3; ++j)
+            S[i][j] = S[j][i] = fmaf(A[6 + i], A[6 + j], fmaf(A[3 + i], A[3 + j], A[i] * A[j]));
 #pragma unroll
     for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
 #pragma unroll 1

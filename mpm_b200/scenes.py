@@ -48,10 +48,12 @@ class Scene:
                           self.dt, transfer=self.transfer, gravity=self.gravity, boundary=self.boundary,
                           sticky_cells=self.sticky_cells, volume_mode=self.volume_mode)
 
-    def solver(self):
+    def solver(self, device=None):
         from .solver import APICMPMSolver3D, MPMSolver3D
         opts = dict(gravity=self.gravity, boundary=self.boundary, sticky_cells=self.sticky_cells,
                     volume_mode=self.volume_mode)
+        if device is not None:
+            opts["device"] = device
         if self.transfer == _abi.TRANSFER_APIC:
             return APICMPMSolver3D(self.particles, self.origin, self.resolution, self.stride, self.friction,
                                    self.interpolation, self.dt, **opts)

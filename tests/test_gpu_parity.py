@@ -119,10 +119,12 @@ def test_grid_update_matches_oracle(gpu, transfer, interp):
     o.update_grid_velocities(dt)
     o.grid_collision(dt)
     # v = p/m carries no stress but divides the 1e-6 momentum error by light
-    # node masses; v* = v + dt f/m inherits the FP32 stress error of f (1e-4,
-    # the force tolerance above)
+    # node masses; v* = v + dt f/m inherits the FP32 stress error of f: the
+    # stress is 2 mu U diag(s (s - 1)) U^T with s from an FP32 SVD (absolute
+    # error ~1e-6), i.e. ~1e-4 relative at the ~1% strains of this scene, and
+    # dt f/m at light nodes carries it into v* at up to ~2x that
     assert relerr(g.download_grid(_abi.GRID_VELOCITY), o.grid(_abi.GRID_VELOCITY)) < 1e-5
-    assert relerr(g.download_grid(_abi.GRID_VELOCITY_STAR), o.grid(_abi.GRID_VELOCITY_STAR)) < 1e-4
+    assert relerr(g.download_grid(_abi.GRID_VELOCITY_STAR), o.grid(_abi.GRID_VELOCITY_STAR)) < 2e-4
 
 
 def _particle_fields(transfer):

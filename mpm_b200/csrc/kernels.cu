@@ -392,6 +392,23 @@ __global__ void __launch_bounds__(kThreads) stressKernel(const SceneDev* __restr
 //     MASS         : m, -, -, -
 //   weights: (N(d), N'(d)/h) pairs per axis and stencil offset (float2)
 // ---------------------------------------------------------------------------
+// Staging-record stride (floats): a multiple of 4 (float4 loads) whose
+// multiples q * P, q < groups, start at least 4 banks apart, so that the
+// broadcast loads of a warp's particle groups never share a bank.
+__host__ __device__ constexpr bool stageStrideOk(int P, int groups) {
+    for (int a = 0; a < groups; ++a)
+        for (int b = a + 1; b < groups; ++b) {
+            const int d = ((b - a) * P) % 32;
+            if (d < 4 || d > 28) return false;
+        }
+    return true;
+}
+__host__ __device__ constexpr int stageStride(int base, int groups) {
+    int P = (base + 3) / 4 * 4;
+    while (!stageStrideOk(P, groups)) P += 4;
+    return P;
+}
+
 template <int S, int MODE, int STAGE = 16>
 struct P2GLayout {
     static constexpr int F = modeFields(MODE);
@@ -402,13 +419,19 @@ struct P2GLayout {
     static constexpr int TJ = (TN + kThreads - 1) / kThreads;
     static constexpr int SH = (MODE == MODE_MASS) ? 4 : (MODE == MODE_FLIP ? 12 : 20);  // shared floats
     static constexpr int WB = SH;                     // weight pairs start
-    static constexpr int P = ((SH + 6 * S) + 3) / 4 * 4;
+    static constexpr int P = stageStride(SH + 6 * S, G);
     static constexpr int kStage = STAGE;              // particles staged per warp round
     static constexpr int kSlots = 32;                 // segment partials per round
     static constexpr int kSeg = 96;                   // particles per segment (at most)
     static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg
-    static constexpr size_t smemFloats = (size_t)kWarps * kStage * P + (size_t)kSlots * F * 64;
-    static constexpr size_t smemBytes = smemFloats * 4 + (2 * 64 + 3 * kMaxSeg + 4) * 4;
+    // dynamic shared memory: stage [kWarps][kStage][P] floats, partials
+    // [kSlots][F][NS] floats, then the control ints (cellBeg[64], cellEnd[64],
+    // segCell/segBeg/segEnd[kMaxSeg], ctl[4]); the kernel takes its pointers
+    // from these offsets
+    static constexpr size_t kPartialOff = (size_t)kWarps * kStage * P;
+    static constexpr size_t kCtlOff = kPartialOff + (size_t)kSlots * F * NS;
+    static constexpr int kCtlInts = 2 * 64 + 3 * kMaxSeg + 4;
+    static constexpr size_t smemBytes = kCtlOff * 4 + (size_t)kCtlInts * 4;
     static_assert(kMaxSeg >= 64 + (int)(kBlockChunk / kSeg) + 1, "segment list too small");
 };
 
@@ -418,9 +441,9 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
     constexpr int F = L::F;
     extern __shared__ float4 smem4[];
     float* smem = reinterpret_cast<float*>(smem4);
-    float* stage = smem;                                        // [warp][kStage][P]
-    float* partial = smem + (size_t)kWarps * L::kStage * L::P;  // [slot][F][64]
-    int* cellBeg = (int*)(partial + (size_t)L::kSlots * F * 64);
+    float* stage = smem;                     // [warp][kStage][P]
+    float* partial = smem + L::kPartialOff;  // [slot][F][NS]
+    int* cellBeg = (int*)(smem + L::kCtlOff);
     int* cellEnd = cellBeg + 64;
     int* segCell = cellEnd + 64;                                // segment list, in cell order
     int* segBeg = segCell + L::kMaxSeg;
@@ -673,11 +696,11 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                         acc[c][f] = sum;
                     }
                 if (grp == 0) {
-                    float* pc = partial + (size_t)cl * F * 64 + na + S * nb;
+                    float* pc = partial + (size_t)cl * F * L::NS + na + S * nb;
 #pragma unroll
                     for (int c = 0; c < S; ++c)
 #pragma unroll
-                        for (int f = 0; f < F; ++f) pc[f * 64 + L::PAIRS * c] = acc[c][f];
+                        for (int f = 0; f < F; ++f) pc[f * L::NS + L::PAIRS * c] = acc[c][f];
                 }
             }
             __syncthreads();
@@ -694,9 +717,9 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                         if ((unsigned)dx >= (unsigned)S || (unsigned)dy >= (unsigned)S || (unsigned)dz >= (unsigned)S)
                             continue;
                         // stencil node index of the lane layout: a + S (b + S c)
-                        const float* pc = partial + (size_t)(sg - r0) * F * 64 + dx + S * (dy + S * dz);
+                        const float* pc = partial + (size_t)(sg - r0) * F * L::NS + dx + S * (dy + S * dz);
 #pragma unroll
-                        for (int f = 0; f < F; ++f) tacc[j][f] += pc[f * 64];
+                        for (int f = 0; f < F; ++f) tacc[j][f] += pc[f * L::NS];
                     }
                 }
             }
@@ -1344,19 +1367,24 @@ static void setP2GAttr() {
 static int p2gStage() {
     static int v = [] {
         const char* e = getenv("MPM_P2G_STAGE");
-        return (e && atoi(e) == 16) ? 16 : 32;
+        const int k = e ? atoi(e) : 32;
+        return (k == 16 || k == 24) ? k : 32;
     }();
     return v;
 }
 
+template <int S, int MODE, int STAGE>
+static void p2gLaunch(const LaunchCtx& c, const StepArgs& a, int want) {
+    setP2GAttr<S, MODE, STAGE>();
+    p2gKernel<S, MODE, STAGE><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, STAGE>::smemBytes, c.stream>>>(a, want);
+}
+
 template <int S, int MODE>
 static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
-    if (p2gStage() == 32) {
-        setP2GAttr<S, MODE, 32>();
-        p2gKernel<S, MODE, 32><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, 32>::smemBytes, c.stream>>>(a, want);
-    } else {
-        setP2GAttr<S, MODE, 16>();
-        p2gKernel<S, MODE, 16><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, 16>::smemBytes, c.stream>>>(a, want);
+    switch (p2gStage()) {
+        case 16: p2gLaunch<S, MODE, 16>(c, a, want); break;
+        case 24: p2gLaunch<S, MODE, 24>(c, a, want); break;
+        default: p2gLaunch<S, MODE, 32>(c, a, want); break;
     }
 }
 

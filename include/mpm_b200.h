@@ -167,6 +167,13 @@ MPM_API mpm_status mpm_device_count(int32_t* count);
 /* Select the CUDA device that later solver/batch creations on this thread
  * use (the library's CUDA runtime keeps its own current device). */
 MPM_API mpm_status mpm_set_device(int32_t device);
+/* Scene state (particle buffers, grids, download staging) comes from a
+ * per-device stream-ordered memory pool that keeps freed memory for the next
+ * scene, so adding and removing scenes needs no cudaMalloc/cudaFree.  This
+ * returns the pool's unused memory on `device` to the driver.  No
+ * counterpart in the reference (thrust::device_vector allocates per
+ * solver). */
+MPM_API mpm_status mpm_release_cached_memory(int32_t device);
 
 /* Counters of the last step (read back from the device; synchronizes). */
 typedef struct mpm_step_stats {

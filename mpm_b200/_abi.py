@@ -108,6 +108,7 @@ SIGNATURES = {
     "mpm_sort_keys_device_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),
     "mpm_set_device": (C.c_int, [C.c_int32]),
+    "mpm_release_cached_memory": (C.c_int, [C.c_int32]),
     "mpm_config_parse_yaml": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Config))]),
     "mpm_config_parse_yaml_string": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.POINTER(Config))]),
     "mpm_config_free": (C.c_int, [C.POINTER(Config)]),

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -59,17 +60,64 @@ static float stencilRange(int interp) {
     return interp == MPM_INTERP_LINEAR ? 1.0f : (interp == MPM_INTERP_QUADRATIC_BSPLINE ? 1.5f : 2.0f);
 }
 
+// Per-device stream-ordered memory pool for scene state.  Freed blocks stay
+// in the pool (release threshold: unlimited), so scenes that come and go in
+// a batch or a server reuse device memory without cudaMalloc/cudaFree and
+// their device-wide synchronisation.  mpm_release_cached_memory() returns
+// the unused part to the driver.
+static cudaMemPool_t scenePool(int device, mpm_status* st) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64) {
+        *st = fail(MPM_ERR_INVALID_ARG, "device index out of range");
+        return nullptr;
+    }
+    if (!pools[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *st = fail(MPM_ERR_CUDA, std::string("memory pool: ") + cudaGetErrorString(e));
+            return nullptr;
+        }
+        pools[device] = pool;
+    }
+    *st = MPM_OK;
+    return pools[device];
+}
+
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
-    ~DevMem() {
-        if (p) cudaFree(p);
+    cudaStream_t pool_stream = nullptr;  // set: memory of the scene pool, freed in this stream's order
+    ~DevMem() { release(); }
+    void release() {
+        if (p) {
+            if (pool_stream) cudaFreeAsync(p, pool_stream);
+            else cudaFree(p);
+        }
+        p = nullptr;
+        bytes = 0;
+        pool_stream = nullptr;
+    }
+    // Grow to at least b bytes, by at least half the current size, so that a
+    // batch whose scenes come and go rarely reallocates.
+    mpm_status grow(size_t b, const char* what) {
+        if (p && bytes >= b) return MPM_OK;
+        return alloc(std::max(b, bytes + bytes / 2), what);
     }
     mpm_status alloc(size_t b, const char* what) {
         if (p && bytes >= b) return MPM_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
+        release();
         if (b == 0) b = 16;
         cudaError_t e = cudaMalloc(&p, b);
         if (e != cudaSuccess) {
@@ -78,6 +126,23 @@ struct DevMem {
             return fail(MPM_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" + std::to_string(b) + " bytes)");
         }
         bytes = b;
+        return MPM_OK;
+    }
+    // From the scene pool, in the order of `stream` (the engine's stream; the
+    // memory is usable there at once and elsewhere after an event on it).
+    mpm_status allocPooled(size_t b, const char* what, cudaMemPool_t pool, cudaStream_t stream) {
+        if (p && bytes >= b) return MPM_OK;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, b, pool, stream);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return fail(MPM_ERR_OOM, std::string("pool allocation failed for ") + what + " (" + std::to_string(b) +
+                                         " bytes)");
+        }
+        bytes = b;
+        pool_stream = stream;
         return MPM_OK;
     }
     template <class T>
@@ -201,16 +266,19 @@ public:
         for (int a = 0; a < 3; ++a) sc->nb[a] = ((d.resolution[a] + 3) >> 2) + 1;
         sc->nblocks = (uint32_t)sc->nb[0] * sc->nb[1] * sc->nb[2];
         const size_t cap = std::max<size_t>(p.n, 1);
+        mpm_status pst;
+        cudaMemPool_t pool = scenePool(device_, &pst);
+        if (!pool) return pst;
         for (int b = 0; b < 2; ++b) {
-            MPM_TRY(sc->buf_f[b].alloc(sizeof(float) * NFIELDS * cap, "particle state"));
-            MPM_TRY(sc->buf_pid[b].alloc(sizeof(uint32_t) * cap, "particle ids"));
-            MPM_TRY(sc->buf_mat[b].alloc(sizeof(uint16_t) * cap, "particle materials"));
+            MPM_TRY(sc->buf_f[b].allocPooled(sizeof(float) * NFIELDS * cap, "particle state", pool, stream_));
+            MPM_TRY(sc->buf_pid[b].allocPooled(sizeof(uint32_t) * cap, "particle ids", pool, stream_));
+            MPM_TRY(sc->buf_mat[b].allocPooled(sizeof(uint16_t) * cap, "particle materials", pool, stream_));
         }
         const size_t nodes = sc->nodes();
-        MPM_TRY(sc->vstar.alloc(sizeof(float4) * nodes, "grid v*"));
+        MPM_TRY(sc->vstar.allocPooled(sizeof(float4) * nodes, "grid v*", pool, stream_));
         CUDA_TRY(cudaMemsetAsync(sc->vstar.p, 0, sizeof(float4) * nodes, stream_));
         if (d.transfer == MPM_TRANSFER_PIC_FLIP) {
-            MPM_TRY(sc->vold.alloc(sizeof(float4) * nodes, "grid v"));
+            MPM_TRY(sc->vold.allocPooled(sizeof(float4) * nodes, "grid v", pool, stream_));
             CUDA_TRY(cudaMemsetAsync(sc->vold.p, 0, sizeof(float4) * nodes, stream_));
         }
         // Materials: Lame parameters as in src/material_point3d.cu:25-26.
@@ -226,7 +294,7 @@ public:
             mats[i].model = m.model;
         }
         sc->nmat = p.nmaterials;
-        MPM_TRY(sc->mats.alloc(sizeof(MaterialDev) * mats.size(), "materials"));
+        MPM_TRY(sc->mats.allocPooled(sizeof(MaterialDev) * mats.size(), "materials", pool, stream_));
         CUDA_TRY(cudaMemcpyAsync(sc->mats.p, mats.data(), sizeof(MaterialDev) * mats.size(), cudaMemcpyHostToDevice,
                                  stream_));
         // Particle state in the caller's order: the caller's arrays are copied
@@ -235,7 +303,7 @@ public:
         if (p.n > 0) {
             const bool has_vol = d.volume_mode == MPM_VOLUME_PRESCRIBED;
             const size_t n = p.n;
-            MPM_TRY(tmp_.alloc(sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
+            MPM_TRY(tmp_.grow(sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
             float* staged = tmp_.as<float>();
             CUDA_TRY(cudaMemcpyAsync(staged, p.position, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
             CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
@@ -362,36 +430,29 @@ public:
         // batch scratch
         const size_t nk = std::max<size_t>(ntot, 1);
         for (int k = 0; k < 2; ++k) {
-            MPM_TRY(keys_[k].alloc(sizeof(uint32_t) * nk, "keys"));
-            MPM_TRY(vals_[k].alloc(sizeof(uint32_t) * nk, "values"));
+            MPM_TRY(keys_[k].grow(sizeof(uint32_t) * nk, "keys"));
+            MPM_TRY(vals_[k].grow(sizeof(uint32_t) * nk, "values"));
         }
-        const size_t tiles = radixTiles(nk);
-        MPM_TRY(hist_.alloc(sizeof(uint32_t) * 256 * tiles, "radix histogram"));
-        MPM_TRY(scan32_.alloc(sizeof(uint32_t) * (scanScratchElems(256 * tiles) + 1), "scan scratch"));
-        MPM_TRY(sort_scratch_.alloc(sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
-        MPM_TRY(compact_scratch_.alloc(sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
+        MPM_TRY(sort_scratch_.grow(sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
+        MPM_TRY(compact_scratch_.grow(sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
                                        "compaction scratch"));
-        MPM_TRY(block_count_.alloc(sizeof(uint32_t) * tb, "block counts"));
+        MPM_TRY(block_count_.grow(sizeof(uint32_t) * tb, "block counts"));
         CUDA_TRY(cudaMemsetAsync(block_count_.p, 0, sizeof(uint32_t) * tb, stream_));
-        MPM_TRY(packed_.alloc(sizeof(unsigned long long) * tb, "block scan"));
-        MPM_TRY(scanned_.alloc(sizeof(unsigned long long) * tb, "block scan"));
-        MPM_TRY(scan64_.alloc(sizeof(unsigned long long) * (scanScratchElems(tb) + 1), "block scan scratch"));
-        MPM_TRY(total64_.alloc(sizeof(unsigned long long), "block scan total"));
-        MPM_TRY(sbb_.alloc(sizeof(uint32_t) * (ns + 1), "scene block bases"));
+        MPM_TRY(sbb_.grow(sizeof(uint32_t) * (ns + 1), "scene block bases"));
         CUDA_TRY(cudaMemcpyAsync(sbb_.p, sbb.data(), sizeof(uint32_t) * (ns + 1), cudaMemcpyHostToDevice, stream_));
         // work items: one per non-empty block plus one per further kBlockChunk particles
         max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
-        MPM_TRY(active_.alloc(sizeof(BlockItem) * max_active_, "active blocks"));
-        MPM_TRY(outside_.alloc(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
+        MPM_TRY(active_.grow(sizeof(BlockItem) * max_active_, "active blocks"));
+        MPM_TRY(outside_.grow(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
         // [0] work items, [1] outside items, [2] active nodes, [8..13] item schedulers
         MPM_TRY(counters_.alloc(sizeof(uint32_t) * 16, "counters"));
         CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 16, stream_));
-        MPM_TRY(block_slot_.alloc(sizeof(int32_t) * tb, "block slots"));
+        MPM_TRY(block_slot_.grow(sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
         for (auto& s : scenes_) maxS = std::max(maxS, s->S);
         tile_stride_ = (size_t)7 * tileNodes(maxS);
-        MPM_TRY(tiles_.alloc(sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
-        MPM_TRY(scenes_dev_.alloc(sizeof(SceneDev) * std::max(ns, 1), "scene table"));
+        MPM_TRY(tiles_.grow(sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
+        MPM_TRY(scenes_dev_.grow(sizeof(SceneDev) * std::max(ns, 1), "scene table"));
         CUDA_TRY(cudaMemcpyAsync(scenes_dev_.p, host_scenes_.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice,
                                  stream_));
         CUDA_TRY(cudaStreamSynchronize(stream_));
@@ -446,10 +507,6 @@ public:
     BlockBuffers blockBuffers() const {
         BlockBuffers bb;
         bb.block_count = block_count_.as<uint32_t>();
-        bb.packed = packed_.as<unsigned long long>();
-        bb.scanned = scanned_.as<unsigned long long>();
-        bb.scan_partials64 = scan64_.as<unsigned long long>();
-        bb.total64 = total64_.as<unsigned long long>();
         bb.scene_block_base = sbb_.as<uint32_t>();
         bb.active = active_.as<BlockItem>();
         bb.outside = outside_.as<BlockItem>();
@@ -554,6 +611,10 @@ public:
         for (auto& s : scenes_)
             if ((all || s->need_init) && s->desc.volume_mode == MPM_VOLUME_GRID_ESTIMATE) any_estimate = true;
         if (any_estimate) {
+            // the mass pass covers only the scenes being initialized
+            for (size_t i = 0; i < scenes_.size(); ++i)
+                host_scenes_[i].init_pass = (all || scenes_[i]->need_init) ? 1 : 0;
+            MPM_TRY(uploadSceneTable());
             MPM_TRY(sortLive());
             StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
             LaunchCtx c = ctx();
@@ -572,7 +633,10 @@ public:
                 launchVolume(one, parity_, s.S);
             }
             CUDA_TRY(cudaGetLastError());
-            keys_valid_ = false;  // block counts were consumed by the compaction
+            // The sort and the work items stay valid for the first step (the
+            // positions have not moved); the block counts were consumed by the
+            // compaction, so the keys must be recounted after that step.
+            keys_valid_ = false;
         }
         for (auto& s : scenes_) {
             if (all || s->need_init) s->stress_stale = true;  // V0 changed
@@ -616,6 +680,7 @@ public:
         const int p0 = parity_, k0 = kcur_;
         if (!g.exec) {
             const uint64_t l0 = kernelLaunches();
+            sorted_valid_ = false;  // the graph must contain the sort
             CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             mpm_status st = stepBody();
             cudaGraph_t graph = nullptr;
@@ -653,7 +718,12 @@ public:
     }
 
     mpm_status stepBody() {
-        MPM_TRY(sortLive());
+        if (!sorted_valid_) {
+            MPM_TRY(sortLive());
+        } else {
+            // reusing the sort of initialize(): its mass pass counted nodes
+            CUDA_TRY(cudaMemsetAsync(counters_.as<uint32_t>() + 2, 0, sizeof(uint32_t), stream_));
+        }
         MPM_TRY(refreshStress());
         graph_sorted_[parity_][kcur_] = sorted_;
         const int next = 1 - sorted_;
@@ -905,7 +975,10 @@ public:
         const size_t bytes = sizeof(float) * per * s.n;
         if (s.stage[k].bytes < bytes) {
             if (s.stage_pending[k]) CUDA_TRY(cudaEventSynchronize(s.stage_done[k]));
-            MPM_TRY(s.stage[k].alloc(bytes, "download staging buffer"));
+            mpm_status pst;
+            cudaMemPool_t pool = scenePool(device_, &pst);
+            if (!pool) return pst;
+            MPM_TRY(s.stage[k].allocPooled(bytes, "download staging buffer", pool, stream_));
         }
         if (s.stage_pending[k]) CUDA_TRY(cudaStreamWaitEvent(stream_, s.stage_done[k], 0));
         launchGatherField(ctx(), idx, parity_, base, comps, mode, s.stage[k].as<float>());
@@ -1026,7 +1099,7 @@ private:
     size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
-    DevMem keys_[2], vals_[2], hist_, scan32_, sort_scratch_, compact_scratch_, block_count_, packed_, scanned_, scan64_, total64_, sbb_, active_,
+    DevMem keys_[2], vals_[2], sort_scratch_, compact_scratch_, block_count_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
     cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)
@@ -1237,6 +1310,17 @@ mpm_status mpm_set_device(int32_t device) {
     if (e != cudaSuccess) {
         cudaGetLastError();
         return mpm::fail(MPM_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    return MPM_OK;
+}
+mpm_status mpm_release_cached_memory(int32_t device) {
+    mpm_status st;
+    cudaMemPool_t pool = mpm::scenePool(device, &st);
+    if (!pool) return st;
+    cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return mpm::fail(MPM_ERR_CUDA, std::string("cudaMemPoolTrimTo: ") + cudaGetErrorString(e));
     }
     return MPM_OK;
 }

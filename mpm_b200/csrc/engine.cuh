@@ -69,6 +69,7 @@ struct SceneDev {
     uint32_t cap;          // plane stride of the particle buffers
     float dt, gravity, friction, blend, dinv;
     int transfer, interp, S, boundary, sticky, pcoll, nmat;
+    int init_pass;         // 1: the mass pass of initialize() covers this scene
     ParticleBuf buf[2];
     float4* vstar;         // dense res^3
     float4* vold;          // dense res^3 (PIC-FLIP)

@@ -24,10 +24,6 @@ struct LaunchCtx {
 
 struct BlockBuffers {
     uint32_t* block_count;            // total_blocks
-    unsigned long long* packed;       // total_blocks
-    unsigned long long* scanned;      // total_blocks
-    unsigned long long* scan_partials64;
-    unsigned long long* total64;      // 1
     uint32_t* scene_block_base;       // nscenes + 1
     BlockItem* active;                // max_active
     BlockItem* outside;               // nscenes
@@ -44,8 +40,6 @@ size_t scanScratchElems(size_t n);
 template <class T>
 cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, cudaStream_t st);
 size_t radixTiles(size_t n);
-cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n, int bits,
-                           uint32_t* hist, uint32_t* scan_partials, bool* result_in_b, cudaStream_t st);
 size_t onesweepScratchWords(size_t n, int bits);
 cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
                               int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st);
@@ -55,7 +49,6 @@ cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint
 
 // kernels.cu
 void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err);
-void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks);
 size_t compactScratchWords64(uint32_t total_blocks);
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
                            unsigned long long* scratch, uint32_t* err);

@@ -166,62 +166,6 @@ __global__ void __launch_bounds__(kThreads) keyKernel(const SceneDev* __restrict
     }
 }
 
-// Packs (active flag << 32 | count) per global block.  Scene outside blocks
-// never become active.
-__global__ void __launch_bounds__(kThreads) packBlocksKernel(const uint32_t* __restrict__ block_count,
-                                                              unsigned long long* __restrict__ packed,
-                                                              uint32_t total_blocks,
-                                                              const uint32_t* __restrict__ scene_block_base,
-                                                              int nscenes, uint32_t* __restrict__ counters) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        counters[1] = 0;
-        counters[2] = 0;
-    }
-    for (uint32_t b = blockIdx.x * kThreads + threadIdx.x; b < total_blocks; b += gridDim.x * kThreads) {
-        uint32_t c = block_count[b];
-        int s = sceneOfBlock(scene_block_base, nscenes, b);
-        bool outside = (b == scene_block_base[s + 1] - 1);
-        // work items of at most kBlockChunk particles each
-        unsigned long long items = (c > 0 && !outside) ? (unsigned long long)((c + kBlockChunk - 1) / kBlockChunk) : 0ull;
-        packed[b] = (items << 32) | (unsigned long long)c;
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) compactBlocksKernel(
-    const unsigned long long* __restrict__ packed, const unsigned long long* __restrict__ scanned,
-    const unsigned long long* __restrict__ total, uint32_t total_blocks, const uint32_t* __restrict__ scene_block_base,
-    int nscenes, BlockItem* __restrict__ active, BlockItem* __restrict__ outside, uint32_t* __restrict__ counters,
-    int32_t* __restrict__ block_slot, uint32_t* __restrict__ block_count) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = (uint32_t)(*total >> 32);
-    for (uint32_t b = blockIdx.x * kThreads + threadIdx.x; b < total_blocks; b += gridDim.x * kThreads) {
-        unsigned long long v = packed[b], s = scanned[b];
-        uint32_t count = (uint32_t)(v & 0xffffffffull);
-        uint32_t start = (uint32_t)(s & 0xffffffffull);
-        int scene = sceneOfBlock(scene_block_base, nscenes, b);
-        const uint32_t items = (uint32_t)(v >> 32);
-        if (items) {
-            // consecutive work items (and tile slots) of one block, in particle order
-            const uint32_t slot = (uint32_t)(s >> 32);
-            for (uint32_t j = 0; j < items; ++j) {
-                const uint32_t off = j * kBlockChunk;
-                active[slot + j] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
-            }
-            block_slot[b] = (int32_t)slot;
-        } else {
-            block_slot[b] = -1;
-            if (count > 0) {
-                const uint32_t nitems = (count + kBlockChunk - 1) / kBlockChunk;
-                const uint32_t o = atomicAdd(&counters[1], nitems);
-                for (uint32_t j = 0; j < nitems; ++j) {
-                    const uint32_t off = j * kBlockChunk;
-                    outside[o + j] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
-                }
-            }
-        }
-        block_count[b] = 0;
-    }
-}
-
 // Block compaction in one kernel: each CTA scans a tile of 1024 block counts,
 // publishes the tile's (work items, particles) sums and looks back over the
 // earlier tiles' published words (single-pass scan, dynamic tile ids, every
@@ -464,6 +408,7 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
+        if (MODE == MODE_MASS && !sc.init_pass) continue;
         const float* pf = sc.buf[args.parity].f;
         const size_t cap = sc.cap;
 
@@ -758,6 +703,7 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
+        if (MODE == MODE_MASS && !sc.init_pass) continue;
         if (args.block_slot[it.block] != (int32_t)w) continue;  // a block's first work item does its nodes
         const uint32_t lb = it.block - sc.block_base;
         const int B[3] = {(int)(lb % (uint32_t)sc.nb[0]), (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]),
@@ -1331,18 +1277,6 @@ void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t 
     compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
         bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,
         bb.block_slot, scratch + 1, reinterpret_cast<uint32_t*>(scratch), ntiles, err);
-}
-
-void launchCompact(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks) {
-    noteLaunches(2);
-    unsigned grid = (unsigned)std::min<size_t>((total_blocks + kThreads - 1) / kThreads, (size_t)c.num_sms * 8);
-    if (grid == 0) grid = 1;
-    packBlocksKernel<<<grid, kThreads, 0, c.stream>>>(bb.block_count, bb.packed, total_blocks, bb.scene_block_base,
-                                                      c.nscenes, bb.counters);
-    exclusiveScan<unsigned long long>(bb.packed, bb.scanned, total_blocks, bb.scan_partials64, bb.total64, c.stream);
-    compactBlocksKernel<<<grid, kThreads, 0, c.stream>>>(bb.packed, bb.scanned, bb.total64, total_blocks,
-                                                         bb.scene_block_base, c.nscenes, bb.active, bb.outside,
-                                                         bb.counters, bb.block_slot, bb.block_count);
 }
 
 void launchStress(const LaunchCtx& c, int parity) {

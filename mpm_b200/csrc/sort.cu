@@ -385,41 +385,6 @@ template cudaError_t exclusiveScan<unsigned long long>(const unsigned long long*
 
 size_t radixTiles(size_t n) { return (n + kSortTile - 1) / kSortTile; }
 
-// Sorts (keys_a, identity values) by the low `bits` bits of the keys.
-// Returns in *result_in_b whether the sorted arrays ended in (keys_b, vals_b).
-cudaError_t radixSortPairs(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
-                           int bits, uint32_t* hist, uint32_t* scan_partials, bool* result_in_b, cudaStream_t st) {
-    *result_in_b = false;
-    if (n == 0) return cudaSuccess;
-    int ntiles = (int)radixTiles(n);
-    uint32_t *kin = keys_a, *vin = vals_a, *kout = keys_b, *vout = vals_b;
-    bool first = true;
-    for (int shift = 0; shift < bits || first; shift += 8) {
-        int pass_bits = bits - shift < 8 ? bits - shift : 8;
-        if (pass_bits <= 0) pass_bits = 1;
-        uint32_t mask = (1u << pass_bits) - 1u;
-        noteLaunches(2);
-        radixUpsweepKernel<<<ntiles, kThreads, 0, st>>>(kin, (uint32_t)n, shift, mask, hist, ntiles);
-        cudaError_t e = exclusiveScan<uint32_t>(hist, hist, (size_t)256 * ntiles, scan_partials, nullptr, st);
-        if (e != cudaSuccess) return e;
-        if (first)
-            radixDownsweepKernel<true><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, hist, (uint32_t)n, shift, mask,
-                                                                    ntiles);
-        else
-            radixDownsweepKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, hist, (uint32_t)n, shift,
-                                                                     mask, ntiles);
-        first = false;
-        uint32_t* t = kin;
-        kin = kout;
-        kout = t;
-        t = vin;
-        vin = vout;
-        vout = t;
-        *result_in_b = !*result_in_b;
-    }
-    return cudaGetLastError();
-}
-
 // Same sort with every buffer supplied by the caller: `in_keys` is only read,
 // the result always lands in (out_keys, out_vals), and (tmp_keys, tmp_vals)
 // is the other ping-pong pair.  The pass count decides which pair the first

@@ -44,3 +44,20 @@ def test_budget_admission_defers_and_rejects(gpu):
     rep = srv.run(reqs)
     srv.close()
     assert len(rep.rejected) == len(reqs) and not rep.results
+
+
+def test_release_cached_memory_between_solvers(gpu):
+    """Scene memory comes from a pool that keeps freed blocks; releasing the
+    cache between solvers leaves later solvers working and bitwise equal."""
+    lib = _abi.load()
+    sc = scenes.tiny_scene(n=2048, res=16)
+    g = sc.solver()
+    g.step(3)
+    x0 = g.download(_abi.FIELD_POSITION)
+    g.close()
+    _abi.check(lib.mpm_release_cached_memory(0), "mpm_release_cached_memory")
+    g = sc.solver()
+    g.step(3)
+    assert np.array_equal(g.download(_abi.FIELD_POSITION), x0)
+    g.close()
+    assert _abi.STATUS_NAMES[lib.mpm_release_cached_memory(-1)] == "INVALID_ARG"

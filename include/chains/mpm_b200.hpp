@@ -104,6 +104,9 @@ public:
         return out;
     }
     mpm_solver* handle() { return h_; }
+    // Checkpoint of the full state (mpm_solver_save); resume with the
+    // solver class's fromCheckpoint().
+    void save(const std::string& path) { check(mpm_solver_save(h_, path.c_str()), "save"); }
 
     SolverBase(const SolverBase&) = delete;
     SolverBase& operator=(const SolverBase&) = delete;
@@ -191,6 +194,11 @@ public:
                interpolationType, deltaTime, MPM_TRANSFER_PIC_FLIP);
     }
     explicit MPMSolver3D(mpm_solver* h) : SolverBase(h) {}
+    static MPMSolver3D fromCheckpoint(const std::string& path) {
+        mpm_solver* h = nullptr;
+        check(mpm_solver_load(path.c_str(), &h), "fromCheckpoint");
+        return MPMSolver3D(h);
+    }
     void gridToParticles(float dt, float blendCoefficient) {
         check(mpm_solver_grid_to_particles(h_, dt, blendCoefficient), "gridToParticles");
     }
@@ -206,6 +214,11 @@ public:
                interpolationType, deltaTime, MPM_TRANSFER_APIC);
     }
     explicit APICMPMSolver3D(mpm_solver* h) : SolverBase(h) {}
+    static APICMPMSolver3D fromCheckpoint(const std::string& path) {
+        mpm_solver* h = nullptr;
+        check(mpm_solver_load(path.c_str(), &h), "fromCheckpoint");
+        return APICMPMSolver3D(h);
+    }
     void gridToParticles(float dt) { check(mpm_solver_grid_to_particles(h_, dt, 0.f), "gridToParticles"); }
 };
 

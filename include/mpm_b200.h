@@ -193,6 +193,16 @@ MPM_API mpm_status mpm_solver_create(const mpm_scene_desc* desc,
 /* Replaces ~MPMSolver3D (src/mpm_solver3d.cu:93-98). */
 MPM_API mpm_status mpm_solver_destroy(mpm_solver* s);
 
+/* Checkpoint and resume (no counterpart in the reference, which has no
+ * checkpoint).  mpm_solver_save writes the scene description, the material
+ * table and the full particle state -- every field, in the solver's internal
+ * particle order, with the cached stress -- to `path`; mpm_solver_load creates
+ * a solver from such a file (checked on the host before any device work:
+ * MPM_ERR_IO if unreadable, MPM_ERR_PARSE if not a valid checkpoint).  The
+ * loaded solver's steps are bitwise those the saved solver would have taken. */
+MPM_API mpm_status mpm_solver_save(mpm_solver* s, const char* path);
+MPM_API mpm_status mpm_solver_load(const char* path, mpm_solver** out);
+
 /* simulateOneStep() repeated nsteps times (src/mpm_solver3d.cu:100-125,
  * src/apic_mpm_solver3d.cu:99-124).  Asynchronous on the solver's stream;
  * returns errors of earlier steps. */

@@ -27,6 +27,11 @@ MPM_API mpm_status mpm_batch_add_scene(mpm_batch* b, const mpm_scene_desc* desc,
                                const mpm_particles_in* particles, int32_t* scene_id);
 /* Release a scene's device state.  Waits for the batch's stream. */
 MPM_API mpm_status mpm_batch_remove_scene(mpm_batch* b, int32_t scene_id);
+/* Checkpoint one scene of a batch / add a scene from a checkpoint (the
+ * format of mpm_solver_save; a scene saved from a solver or a batch loads into
+ * either).  For preempting and resuming served requests. */
+MPM_API mpm_status mpm_batch_save_scene(mpm_batch* b, int32_t scene_id, const char* path);
+MPM_API mpm_status mpm_batch_load_scene(mpm_batch* b, const char* path, int32_t* scene_id);
 /* Advance every scene nsteps steps (asynchronous). */
 MPM_API mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps);
 MPM_API mpm_status mpm_batch_synchronize(mpm_batch* b);
@@ -36,6 +41,7 @@ MPM_API mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t fi
 MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
+MPM_API mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_t* n);
 MPM_API mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out);
 /* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */
 MPM_API mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms);

@@ -79,6 +79,8 @@ SIGNATURES = {
     "mpm_device_count": (C.c_int, [C.POINTER(C.c_int32)]),
     "mpm_solver_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(ParticlesIn), C.POINTER(_P)]),
     "mpm_solver_destroy": (C.c_int, [_P]),
+    "mpm_solver_save": (C.c_int, [_P, C.c_char_p]),
+    "mpm_solver_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "mpm_solver_step": (C.c_int, [_P, C.c_int32]),
     "mpm_solver_synchronize": (C.c_int, [_P]),
     "mpm_solver_initialize": (C.c_int, [_P]),
@@ -125,12 +127,15 @@ SIGNATURES = {
     "mpm_batch_destroy": (C.c_int, [_P]),
     "mpm_batch_add_scene": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesIn), C.POINTER(C.c_int32)]),
     "mpm_batch_remove_scene": (C.c_int, [_P, C.c_int32]),
+    "mpm_batch_save_scene": (C.c_int, [_P, C.c_int32, C.c_char_p]),
+    "mpm_batch_load_scene": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int32)]),
     "mpm_batch_step": (C.c_int, [_P, C.c_int32]),
     "mpm_batch_synchronize": (C.c_int, [_P]),
     "mpm_batch_download": (C.c_int, [_P, C.c_int32, C.c_int32, _F]),
     "mpm_batch_download_async": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_void_p]),
     "mpm_batch_download_wait": (C.c_int, [_P]),
     "mpm_batch_num_scenes": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "mpm_batch_scene_particles": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_size_t)]),
     "mpm_batch_profile": (C.c_int, [_P, C.c_int32]),
     "mpm_batch_profile_read": (C.c_int, [_P, _F, C.POINTER(C.c_int32), C.c_int32]),
 }

@@ -10,6 +10,7 @@ batching; each scene's result is bitwise the result of solving it alone.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Dict
 
 import numpy as np
@@ -61,6 +62,19 @@ class Batch:
     def remove(self, sid: int):
         check(self._lib.mpm_batch_remove_scene(self._h, int(sid)), "mpm_batch_remove_scene")
         self._n.pop(int(sid), None)
+
+    def save_scene(self, sid: int, path: str):
+        """Checkpoint one scene (the format of MPMSolver3D.save)."""
+        check(self._lib.mpm_batch_save_scene(self._h, int(sid), os.fsencode(path)), "mpm_batch_save_scene")
+
+    def load_scene(self, path: str) -> int:
+        """Add a scene from a checkpoint; returns its id."""
+        sid = C.c_int32()
+        check(self._lib.mpm_batch_load_scene(self._h, os.fsencode(path), C.byref(sid)), "mpm_batch_load_scene")
+        n = C.c_size_t()
+        check(self._lib.mpm_batch_scene_particles(self._h, sid, C.byref(n)), "mpm_batch_scene_particles")
+        self._n[int(sid.value)] = int(n.value)
+        return int(sid.value)
 
     @property
     def num_scenes(self) -> int:

@@ -169,6 +169,7 @@ struct SceneHost {
     cudaEvent_t stage_ready[2] = {}, stage_done[2] = {};
     bool stage_pending[2] = {};
     int stage_next = 0;
+    std::vector<mpm_material> mats_in;  // as given (kept for checkpoints)
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
     ~SceneHost() {
         for (int k = 0; k < 2; ++k) {
@@ -257,15 +258,17 @@ public:
         return MPM_OK;
     }
 
-    mpm_status addScene(const mpm_scene_desc& d, const mpm_particles_in& p, int* out_id) {
-        MPM_TRY(validate(d, p));
+    // A new scene's device buffers and material table (state not yet set).
+    mpm_status newScene(const mpm_scene_desc& d, const mpm_material* materials, int nmaterials, size_t n,
+                        std::unique_ptr<SceneHost>* out) {
         auto sc = std::make_unique<SceneHost>();
         sc->desc = d;
-        sc->n = p.n;
+        sc->n = n;
         sc->S = stencilSize(d.interpolation);
         for (int a = 0; a < 3; ++a) sc->nb[a] = ((d.resolution[a] + 3) >> 2) + 1;
         sc->nblocks = (uint32_t)sc->nb[0] * sc->nb[1] * sc->nb[2];
-        const size_t cap = std::max<size_t>(p.n, 1);
+        sc->mats_in.assign(materials, materials + nmaterials);
+        const size_t cap = std::max<size_t>(n, 1);
         mpm_status pst;
         cudaMemPool_t pool = scenePool(device_, &pst);
         if (!pool) return pst;
@@ -282,9 +285,9 @@ public:
             CUDA_TRY(cudaMemsetAsync(sc->vold.p, 0, sizeof(float4) * nodes, stream_));
         }
         // Materials: Lame parameters as in src/material_point3d.cu:25-26.
-        std::vector<MaterialDev> mats(p.nmaterials);
-        for (int i = 0; i < p.nmaterials; ++i) {
-            const mpm_material& m = p.materials[i];
+        std::vector<MaterialDev> mats(nmaterials);
+        for (int i = 0; i < nmaterials; ++i) {
+            const mpm_material& m = materials[i];
             double E = m.youngs_modulus, nu = m.poisson_ratio;
             mats[i].mu0 = (float)(E / (2.0 * (1.0 + nu)));
             mats[i].lambda0 = (float)((double)(m.youngs_modulus * m.poisson_ratio) / ((1.0 + nu) * (1.0 - 2.0 * nu)));
@@ -293,10 +296,30 @@ public:
             mats[i].theta_s = m.critical_stretch;
             mats[i].model = m.model;
         }
-        sc->nmat = p.nmaterials;
+        sc->nmat = nmaterials;
         MPM_TRY(sc->mats.allocPooled(sizeof(MaterialDev) * mats.size(), "materials", pool, stream_));
         CUDA_TRY(cudaMemcpyAsync(sc->mats.p, mats.data(), sizeof(MaterialDev) * mats.size(), cudaMemcpyHostToDevice,
                                  stream_));
+        CUDA_TRY(cudaStreamSynchronize(stream_));  // the host material table is freed on return
+        *out = std::move(sc);
+        return MPM_OK;
+    }
+
+    int registerScene(std::unique_ptr<SceneHost> sc) {
+        sc->id = next_id_++;
+        const int id = sc->id;
+        scenes_.push_back(std::move(sc));
+        dirty_ = true;
+        keys_valid_ = false;
+        sorted_valid_ = false;
+        return id;
+    }
+
+    mpm_status addScene(const mpm_scene_desc& d, const mpm_particles_in& p, int* out_id) {
+        MPM_TRY(validate(d, p));
+        std::unique_ptr<SceneHost> sc;
+        MPM_TRY(newScene(d, p.materials, p.nmaterials, p.n, &sc));
+        const size_t cap = std::max<size_t>(p.n, 1);
         // Particle state in the caller's order: the caller's arrays are copied
         // as they are (x, v interleaved; m; V0 if prescribed) into a staging
         // buffer and a kernel writes the SoA planes (Fe = Fp = I, B = 0).
@@ -324,13 +347,134 @@ public:
             CUDA_TRY(cudaStreamSynchronize(stream_));
         }
         sc->need_init = true;
-        sc->id = next_id_++;
-        *out_id = sc->id;
         sc->stress_stale = true;
-        scenes_.push_back(std::move(sc));
-        dirty_ = true;
-        keys_valid_ = false;
-        sorted_valid_ = false;
+        *out_id = registerScene(std::move(sc));
+        return MPM_OK;
+    }
+
+    // ---- checkpoints ----------------------------------------------------------
+    // File layout (little endian): "MPMB200\0", u32 version, u32 sizeof(desc),
+    // mpm_scene_desc, i32 nmaterials, mpm_material[nmaterials], u64 n,
+    // u32 flags (bit 0: cached stress stale), then in the engine's internal
+    // particle order the 41 float planes (n floats each), the original
+    // particle ids (u32 x n) and the material ids (u16 x n).  Restoring that
+    // order and the cached stress makes the continuation bitwise identical.
+    static constexpr uint32_t kCkptVersion = 1;
+
+    mpm_status saveScene(int id, const char* path) {
+        if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        SceneHost& s = *scenes_[idx];
+        const size_t n = s.n;
+        std::vector<float> planes((size_t)NFIELDS * n);
+        std::vector<uint32_t> pid(n);
+        std::vector<uint16_t> mat(n);
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        const size_t cap = std::max<size_t>(n, 1);
+        for (int f = 0; f < NFIELDS && n; ++f)
+            CUDA_TRY(cudaMemcpy(planes.data() + (size_t)f * n, s.buf_f[parity_].as<float>() + (size_t)f * cap,
+                                sizeof(float) * n, cudaMemcpyDeviceToHost));
+        if (n) {
+            CUDA_TRY(cudaMemcpy(pid.data(), s.buf_pid[parity_].p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+            CUDA_TRY(cudaMemcpy(mat.data(), s.buf_mat[parity_].p, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost));
+        }
+        std::FILE* fp = std::fopen(path, "wb");
+        if (!fp) return fail(MPM_ERR_IO, std::string("cannot open ") + path + " for writing");
+        const char magic[8] = {'M', 'P', 'M', 'B', '2', '0', '0', 0};
+        const uint32_t ver = kCkptVersion, dsz = (uint32_t)sizeof(mpm_scene_desc);
+        const int32_t nm = (int32_t)s.mats_in.size();
+        const uint64_t n64 = n;
+        const uint32_t flags = s.stress_stale ? 1u : 0u;
+        bool ok = std::fwrite(magic, 1, 8, fp) == 8 && std::fwrite(&ver, 4, 1, fp) == 1 &&
+                  std::fwrite(&dsz, 4, 1, fp) == 1 && std::fwrite(&s.desc, sizeof(mpm_scene_desc), 1, fp) == 1 &&
+                  std::fwrite(&nm, 4, 1, fp) == 1 &&
+                  std::fwrite(s.mats_in.data(), sizeof(mpm_material), s.mats_in.size(), fp) == s.mats_in.size() &&
+                  std::fwrite(&n64, 8, 1, fp) == 1 && std::fwrite(&flags, 4, 1, fp) == 1 &&
+                  std::fwrite(planes.data(), sizeof(float), planes.size(), fp) == planes.size() &&
+                  std::fwrite(pid.data(), sizeof(uint32_t), n, fp) == n &&
+                  std::fwrite(mat.data(), sizeof(uint16_t), n, fp) == n;
+        ok = (std::fclose(fp) == 0) && ok;
+        if (!ok) return fail(MPM_ERR_IO, std::string("write failed: ") + path);
+        return MPM_OK;
+    }
+
+    // Reads and checks a checkpoint on the host (no device work).
+    struct Checkpoint {
+        mpm_scene_desc desc{};
+        std::vector<mpm_material> mats;
+        size_t n = 0;
+        uint32_t flags = 0;
+        std::vector<float> planes;
+        std::vector<uint32_t> pid;
+        std::vector<uint16_t> mat;
+    };
+    static mpm_status readCheckpoint(const char* path, Checkpoint* ck) {
+        if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
+        std::FILE* fp = std::fopen(path, "rb");
+        if (!fp) return fail(MPM_ERR_IO, std::string("cannot open ") + path);
+        std::unique_ptr<std::FILE, int (*)(std::FILE*)> guard(fp, std::fclose);
+        char magic[8];
+        uint32_t ver = 0, dsz = 0;
+        int32_t nm = 0;
+        uint64_t n64 = 0;
+        if (std::fread(magic, 1, 8, fp) != 8 || memcmp(magic, "MPMB200", 8) != 0)
+            return fail(MPM_ERR_PARSE, std::string(path) + ": not a checkpoint");
+        if (std::fread(&ver, 4, 1, fp) != 1 || ver != kCkptVersion || std::fread(&dsz, 4, 1, fp) != 1 ||
+            dsz != sizeof(mpm_scene_desc))
+            return fail(MPM_ERR_PARSE, std::string(path) + ": unsupported checkpoint version");
+        if (std::fread(&ck->desc, sizeof(mpm_scene_desc), 1, fp) != 1 || std::fread(&nm, 4, 1, fp) != 1 || nm < 1 ||
+            nm > 65535)
+            return fail(MPM_ERR_PARSE, std::string(path) + ": truncated or corrupt header");
+        ck->mats.resize(nm);
+        if (std::fread(ck->mats.data(), sizeof(mpm_material), nm, fp) != (size_t)nm ||
+            std::fread(&n64, 8, 1, fp) != 1 || n64 > 0x7fffffffull || std::fread(&ck->flags, 4, 1, fp) != 1)
+            return fail(MPM_ERR_PARSE, std::string(path) + ": truncated or corrupt header");
+        mpm_particles_in none{};
+        none.materials = ck->mats.data();
+        none.nmaterials = nm;
+        MPM_TRY(validate(ck->desc, none));
+        const size_t n = (size_t)n64;
+        ck->n = n;
+        try {
+            ck->planes.resize((size_t)NFIELDS * n);
+            ck->pid.resize(n);
+            ck->mat.resize(n);
+        } catch (const std::bad_alloc&) {
+            return fail(MPM_ERR_OOM, "host allocation failed");
+        }
+        if (std::fread(ck->planes.data(), sizeof(float), ck->planes.size(), fp) != ck->planes.size() ||
+            std::fread(ck->pid.data(), sizeof(uint32_t), n, fp) != n ||
+            std::fread(ck->mat.data(), sizeof(uint16_t), n, fp) != n)
+            return fail(MPM_ERR_PARSE, std::string(path) + ": truncated particle data");
+        std::vector<uint8_t> seen(n, 0);
+        for (size_t i = 0; i < n; ++i) {
+            if (ck->pid[i] >= n || seen[ck->pid[i]]) return fail(MPM_ERR_PARSE, std::string(path) + ": bad particle ids");
+            seen[ck->pid[i]] = 1;
+            if (ck->mat[i] >= (uint32_t)nm) return fail(MPM_ERR_PARSE, std::string(path) + ": bad material ids");
+        }
+        return MPM_OK;
+    }
+
+    mpm_status loadScene(const Checkpoint& ck, int* out_id) {
+        std::unique_ptr<SceneHost> sc;
+        MPM_TRY(newScene(ck.desc, ck.mats.data(), (int)ck.mats.size(), ck.n, &sc));
+        const size_t n = ck.n, cap = std::max<size_t>(n, 1);
+        const int b = parity_;
+        for (int f = 0; f < NFIELDS && n; ++f)
+            CUDA_TRY(cudaMemcpyAsync(sc->buf_f[b].as<float>() + (size_t)f * cap, ck.planes.data() + (size_t)f * n,
+                                     sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+        if (n) {
+            CUDA_TRY(cudaMemcpyAsync(sc->buf_pid[b].p, ck.pid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
+                                     stream_));
+            CUDA_TRY(cudaMemcpyAsync(sc->buf_mat[b].p, ck.mat.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice,
+                                     stream_));
+        }
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        sc->need_init = false;  // V0 is part of the state
+        sc->stress_stale = (ck.flags & 1u) != 0;
+        *out_id = registerScene(std::move(sc));
         return MPM_OK;
     }
 
@@ -1205,6 +1349,34 @@ mpm_status mpm_solver_destroy(mpm_solver* s) {
     return MPM_OK;
 }
 
+mpm_status mpm_solver_save(mpm_solver* s, const char* path) {
+    MPM_TRY(check(s));
+    return s->eng.saveScene(s->scene, path);
+}
+
+mpm_status mpm_solver_load(const char* path, mpm_solver** out) {
+    if (!out) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    try {
+        Engine::Checkpoint ck;
+        mpm_status st = Engine::readCheckpoint(path, &ck);  // host only: checked before any device work
+        if (st != MPM_OK) return st;
+        std::unique_ptr<mpm_solver> s(new mpm_solver);
+        st = s->eng.init();
+        if (st != MPM_OK) return st;
+        st = s->eng.loadScene(ck, &s->scene);
+        if (st != MPM_OK) return st;
+        st = s->eng.ensureReady();
+        if (st != MPM_OK) return st;
+        st = s->eng.synchronize();
+        if (st != MPM_OK) return st;
+        *out = s.release();
+        return MPM_OK;
+    } catch (const std::bad_alloc&) {
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+}
+
 mpm_status mpm_solver_step(mpm_solver* s, int32_t nsteps) {
     MPM_TRY(check(s));
     GUARD(s->eng.step(nsteps));
@@ -1417,6 +1589,23 @@ mpm_status mpm_batch_remove_scene(mpm_batch* b, int32_t scene_id) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.removeScene(scene_id);
 }
+mpm_status mpm_batch_save_scene(mpm_batch* b, int32_t scene_id, const char* path) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.saveScene(scene_id, path);
+}
+mpm_status mpm_batch_load_scene(mpm_batch* b, const char* path, int32_t* scene_id) {
+    if (!b || !scene_id) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    try {
+        Engine::Checkpoint ck;
+        MPM_TRY(Engine::readCheckpoint(path, &ck));
+        int id = -1;
+        MPM_TRY(b->eng.loadScene(ck, &id));
+        *scene_id = id;
+        return MPM_OK;
+    } catch (const std::bad_alloc&) {
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+}
 mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     GUARD(b->eng.step(nsteps));
@@ -1440,6 +1629,13 @@ mpm_status mpm_batch_download_wait(mpm_batch* b) {
 mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
     if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
     *n = (int32_t)b->eng.numScenes();
+    return MPM_OK;
+}
+mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_t* n) {
+    if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    const mpm::SceneHost* s = const_cast<mpm_batch*>(b)->eng.scene(scene_id);
+    if (!s) return mpm::fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+    *n = s->n;
     return MPM_OK;
 }
 mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms) {

@@ -10,6 +10,7 @@ rendering methods (GL buffers, OpenVDB) are replaced by ``download``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -141,6 +142,36 @@ class _SolverBase:
         check(self._lib.mpm_solver_create(C.byref(self._desc), C.byref(pin), C.byref(h)), "mpm_solver_create")
         del keep
         self._h = h
+
+    # -- checkpoints -------------------------------------------------------
+    def save(self, path: str):
+        """Write the full state to `path` (mpm_solver_save); resume with
+        ``from_checkpoint``: the resumed steps are bitwise the ones this solver
+        would take."""
+        check(self._lib.mpm_solver_save(self._h, os.fsencode(path)), "save")
+
+    @classmethod
+    def from_checkpoint(cls, path: str, device: Optional[int] = None):
+        lib = _abi.load()
+        if _abi.device_count() < 1:
+            raise RuntimeError("mpm_b200 needs a CUDA device; there is no CPU fallback")
+        if device is not None:
+            check(lib.mpm_set_device(int(device)), "mpm_set_device")
+        h = C.c_void_p()
+        check(lib.mpm_solver_load(os.fsencode(path), C.byref(h)), "mpm_solver_load")
+        self = cls.__new__(cls)
+        self._lib = lib
+        self._h = h
+        desc = _abi.SceneDesc()
+        check(lib.mpm_solver_get_desc(h, C.byref(desc)), "get_desc")
+        self._desc = desc
+        n = C.c_size_t()
+        check(lib.mpm_solver_num_particles(h, C.byref(n)), "num_particles")
+        self._n = int(n.value)
+        self._res = tuple(int(r) for r in desc.resolution)
+        self._delta_time = float(desc.dt)
+        self._blend_coefficient = float(desc.blend)
+        return self
 
     # -- lifetime ----------------------------------------------------------
     def close(self):

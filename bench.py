@@ -232,12 +232,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) per step of a kernel family from one ncu capture
+# (profiles/g2p_two_balls_128.md, p2g_two_balls_128.md, grid_two_balls_128.md,
+# p2g_g2p_batch16.md; batch64 scaled from its 16-scene subset by particles).
+NCU_TRAFFIC = {
+    "two_balls": {"g2p": 245.9e6, "p2g": 104.7e6, "grid": 4.43e6},
+    "batch64": {"g2p": 1.996e9},
+}
+
+
 def traffic_of(family, workload):
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(p):
-        return None
-    d = json.load(open(p))
-    return d.get(workload, {}).get(family)
+    return NCU_TRAFFIC.get(workload, {}).get(family)
 
 
 # --- CPU and naive-GPU baselines --------------------------------------------------

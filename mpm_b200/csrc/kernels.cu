@@ -365,7 +365,7 @@ struct P2GLayout {
     static constexpr int WB = SH;                     // weight pairs start
     static constexpr int P = stageStride(SH + 6 * S, G);
     static constexpr int kStage = STAGE;              // particles staged per warp round
-    static constexpr int kSlots = 32;                 // segment partials per round
+    static constexpr int kSlots = 32;                 // segment partials per round (<= 32: one per lane)
     static constexpr int kSeg = 96;                   // particles per segment (at most)
     static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg
     // dynamic shared memory: stage [kWarps][kStage][P] floats, partials
@@ -465,20 +465,31 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
             const int rend = min(nseg, r0 + L::kSlots);
             // ---- particle phase: warps take segments of this round dynamically ----
             float* st = stage + (size_t)warp * L::kStage * L::P;
+            // The round's particles [rb, re) are cut into windows of kStage; a
+            // warp takes a window and handles the segments that start in it:
+            // several sparse cells share one staging pass, a long segment
+            // takes several.  Each segment is summed by one warp, in order.
+            const int rb = segBeg[r0], re = segEnd[rend - 1];
+            const int nwin = (re - rb + L::kStage - 1) / L::kStage;
             while (true) {
-                int sg = 0;
-                if (lane == 0) sg = r0 + atomicAdd(&ctl[1], 1);
-                sg = __shfl_sync(0xffffffffu, sg, 0);
-                if (sg >= rend) break;
-                const int cl = sg - r0;  // partial slot
-                const int beg = segBeg[sg], end = segEnd[sg];
+                int wi = 0;
+                if (lane == 0) wi = atomicAdd(&ctl[1], 1);
+                wi = __shfl_sync(0xffffffffu, wi, 0);
+                if (wi >= nwin) break;
+                const int sl = r0 + lane;  // a round has at most 32 segments: one per lane
+                const bool starts = sl < rend && (segBeg[sl] - rb) / L::kStage == wi;
+                const unsigned own = __ballot_sync(0xffffffffu, starts);
+                if (!own) continue;
+                const int s_first = r0 + __ffs(own) - 1, s_last = r0 + 31 - __clz(own);
+                const int cb = segBeg[s_first], ce = segEnd[s_last];
+                int cur = s_first;  // segment being summed
                 float acc[S][F];
 #pragma unroll
                 for (int c = 0; c < S; ++c)
 #pragma unroll
                     for (int f = 0; f < F; ++f) acc[c][f] = 0.f;
-                for (int g0 = beg; g0 < end; g0 += L::kStage) {
-                    const int np = min(L::kStage, end - g0);
+                for (int g0 = cb; g0 < ce; g0 += L::kStage) {
+                    const int np = min(L::kStage, ce - g0);
                     if (lane < np) {
                         float* my = st + lane * L::P;
                         const uint32_t gs = it.start + (uint32_t)(g0 + lane);
@@ -561,9 +572,13 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                         }
                     }
                     __syncwarp();
+                    // the segments overlapping this pass, in order
+                    while (cur <= s_last) {
+                    const int se = segEnd[cur];
+                    const int qlo = max(segBeg[cur], g0) - g0, qhi = min(se, g0 + np) - g0;
                     if (lane_on) {
                         const float fa = (float)na, fb = (float)nb;
-                        for (int q = grp; q < np; q += L::G) {
+                        for (int q = qlo + grp; q < qhi; q += L::G) {
                             const float* pq = st + q * L::P;
                             const float4 s0 = *reinterpret_cast<const float4*>(pq);
                             const float m = s0.x;
@@ -625,27 +640,26 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                             }
                         }
                     }
-                    __syncwarp();
-                }
-                // Sum the groups' columns in group order into group 0 (fixed
-                // order, so the partial does not depend on timing).
-#pragma unroll
-                for (int c = 0; c < S; ++c)
-#pragma unroll
-                    for (int f = 0; f < F; ++f) {
-                        const float mine = acc[c][f];
-                        float sum = mine;
-#pragma unroll
-                        for (int g = 1; g < L::G; ++g)
-                            sum += __shfl_sync(0xffffffffu, mine, min(lane + g * L::PAIRS, 31));
-                        acc[c][f] = sum;
-                    }
-                if (grp == 0) {
-                    float* pc = partial + (size_t)cl * F * L::NS + na + S * nb;
+                    if (se > g0 + np) break;  // the segment continues in the next pass
+                    // Segment done: sum the groups' columns in group order into
+                    // group 0 (fixed order, so the partial does not depend on
+                    // timing), write its slot, start the next segment.
 #pragma unroll
                     for (int c = 0; c < S; ++c)
 #pragma unroll
-                        for (int f = 0; f < F; ++f) pc[f * L::NS + L::PAIRS * c] = acc[c][f];
+                        for (int f = 0; f < F; ++f) {
+                            const float mine = acc[c][f];
+                            float sum = mine;
+#pragma unroll
+                            for (int g = 1; g < L::G; ++g)
+                                sum += __shfl_sync(0xffffffffu, mine, min(lane + g * L::PAIRS, 31));
+                            acc[c][f] = 0.f;
+                            if (grp == 0)
+                                partial[(size_t)(cur - r0) * F * L::NS + f * L::NS + na + S * nb + L::PAIRS * c] = sum;
+                        }
+                    ++cur;
+                    }
+                    __syncwarp();
                 }
             }
             __syncthreads();

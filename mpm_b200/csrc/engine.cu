@@ -201,6 +201,14 @@ public:
             cudaEventDestroy(r.e1);
         }
         for (auto e : event_pool_) cudaEventDestroy(e);
+        for (int k = 0; k < kMaxSide; ++k) {
+            if (side_[k]) {
+                cudaStreamSynchronize(side_[k]);
+                cudaStreamDestroy(side_[k]);
+            }
+            if (join_[k]) cudaEventDestroy(join_[k]);
+        }
+        if (fork_) cudaEventDestroy(fork_);
         if (stream_) cudaStreamDestroy(stream_);
     }
 
@@ -588,9 +596,10 @@ public:
         max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
         MPM_TRY(active_.grow(sizeof(BlockItem) * max_active_, "active blocks"));
         MPM_TRY(outside_.grow(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
-        // [0] work items, [1] outside items, [2] active nodes, [8..13] item schedulers
-        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 16, "counters"));
-        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 16, stream_));
+        // [0] work items, [1] outside items, [2] active nodes, [8 + 8k .. 13 + 8k] item
+        // schedulers of the k-th stencil/transfer combination
+        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 64, "counters"));
+        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 64, stream_));
         MPM_TRY(block_slot_.grow(sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
         for (auto& s : scenes_) maxS = std::max(maxS, s->S);
@@ -874,20 +883,46 @@ public:
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
         LaunchCtx c = ctx();
         auto cs = combos();
-        mark(KF_P2G, 0);
-        for (auto& k : cs)
-            launchP2G(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
-        mark(KF_P2G, 1);
-        collect(KF_P2G);
-        mark(KF_GRID, 0);
-        for (auto& k : cs)
-            launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
-        mark(KF_GRID, 1);
-        collect(KF_GRID);
-        mark(KF_G2P, 0);
-        for (auto& k : cs) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, true);
-        mark(KF_G2P, 1);
-        collect(KF_G2P);
+        if (cs.size() > 1 && !profiling_) {
+            // Scenes of different (stencil, transfer) combinations share no
+            // items, tiles or nodes: their P2G -> grid -> G2P chains run
+            // concurrently, combination k on side stream k - 1, each with its
+            // own work-item schedulers; the step joins them on the main stream.
+            MPM_TRY(ensureSideStreams((int)cs.size() - 1));
+            CUDA_TRY(cudaEventRecord(fork_, stream_));
+            for (size_t k = 0; k < cs.size(); ++k) {
+                LaunchCtx ck = c;
+                StepArgs ak = a;
+                ak.sched = counters_.as<uint32_t>() + 8 + 8 * k;
+                if (k > 0) {
+                    ck.stream = side_[k - 1];
+                    CUDA_TRY(cudaStreamWaitEvent(ck.stream, fork_, 0));
+                }
+                const int mode = cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP;
+                launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
+                launchGrid(ck, ak, cs[k].S, mode, cs[k].transfer);
+                launchG2P(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true);
+                if (k > 0) {
+                    CUDA_TRY(cudaEventRecord(join_[k - 1], ck.stream));
+                    CUDA_TRY(cudaStreamWaitEvent(stream_, join_[k - 1], 0));
+                }
+            }
+        } else {
+            mark(KF_P2G, 0);
+            for (auto& k : cs)
+                launchP2G(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+            mark(KF_P2G, 1);
+            collect(KF_P2G);
+            mark(KF_GRID, 0);
+            for (auto& k : cs)
+                launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+            mark(KF_GRID, 1);
+            collect(KF_GRID);
+            mark(KF_G2P, 0);
+            for (auto& k : cs) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, true);
+            mark(KF_G2P, 1);
+            collect(KF_G2P);
+        }
         CUDA_TRY(cudaGetLastError());
         parity_ ^= 1;
         kcur_ = next;
@@ -1247,6 +1282,20 @@ private:
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
     cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)
+    // side streams of the concurrent per-combination chains (stepBody)
+    static constexpr int kMaxSide = 5;
+    cudaStream_t side_[kMaxSide] = {};
+    cudaEvent_t fork_ = nullptr, join_[kMaxSide] = {};
+    mpm_status ensureSideStreams(int n) {
+        if (n > kMaxSide) return fail(MPM_ERR_UNSUPPORTED, "too many stencil/transfer combinations");
+        if (!fork_) CUDA_TRY(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+        for (int k = 0; k < n; ++k)
+            if (!side_[k]) {
+                CUDA_TRY(cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking));
+                CUDA_TRY(cudaEventCreateWithFlags(&join_[k], cudaEventDisableTiming));
+            }
+        return MPM_OK;
+    }
     struct GraphSlot {
         cudaGraphExec_t exec = nullptr;
         uint64_t launches = 0;

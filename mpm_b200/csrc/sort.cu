@@ -252,12 +252,19 @@ __global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* _
     const uint32_t lt = (1u << lane) - 1u;
     const size_t tbase = (size_t)tile * kSortTile + (size_t)warp * 32 * kSortItems;
     uint32_t k[kSortItems], v[kSortItems], r[kSortItems];
+    // all loads first, so that they are in flight together (the ranking
+    // below synchronises the warp after every item)
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const size_t i = tbase + (size_t)j * 32 + lane;
         const bool valid = i < n;
         k[j] = valid ? keys_in[i] : 0u;
         v[j] = valid ? (kIdentVals ? (uint32_t)i : vals_in[i]) : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const size_t i = tbase + (size_t)j * 32 + lane;
+        const bool valid = i < n;
         const uint32_t d = valid ? (k[j] >> shift) & mask : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const int leader = __ffs(peers) - 1;
@@ -283,22 +290,36 @@ __global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* _
             atomicExch(mine, kFlagPrefix | run);
         } else {
             atomicExch(mine, kFlagAgg | run);
+            // Walk back over the earlier tiles' words, four per round trip
+            // (independent loads), until an inclusive prefix is found.
             int t = (int)tile - 1;
             int polls = 0;
-            while (t >= 0) {
-                const uint32_t w = *(volatile const uint32_t*)(status + (size_t)t * 256 + d);
-                const uint32_t f = w & ~kCountMask;
-                if (f == 0) {
+            bool done = false;
+            while (!done && t >= 0) {
+                uint32_t w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    w[q] = (t - q >= 0) ? *(volatile const uint32_t*)(status + (size_t)(t - q) * 256 + d) : kFlagPrefix;
+                bool waiting = false;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (done || waiting) continue;
+                    const uint32_t f = w[q] & ~kCountMask;
+                    if (f == 0) {  // not published yet: poll again from this tile
+                        waiting = true;
+                        continue;
+                    }
+                    excl += w[q] & kCountMask;
+                    --t;
+                    if (f == kFlagPrefix) done = true;
+                }
+                if (waiting) {
                     if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
                         atomicOr(err, 8u);
                         break;
                     }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += w & kCountMask;
-                if (f == kFlagPrefix) break;
-                --t;
             }
             atomicExch(mine, kFlagPrefix | (excl + run));
         }

@@ -877,48 +877,90 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
                 dw[a][k] *= sc.inv_h;
             }
         }
+        // Separable gather in packed FP32 pairs: the x and y components of
+        // every sum go through one __ffma2_rn (two exactly rounded FMAs, the
+        // same results as fmaf), z through fmaf.  Column j of grad v and of
+        // the APIC moment K is held as (row 0, row 1) pair + row 2.
+        float2 wp[S], dwp[S], wap[S];
+#pragma unroll
+        for (int a = 0; a < S; ++a) {
+            wp[a] = make_float2(w[0][a], w[0][a]);
+            dwp[a] = make_float2(dw[0][a], dw[0][a]);
+            const float wa = w[0][a] * (float)a;
+            wap[a] = make_float2(wa, wa);
+        }
+        float2 vp_xy = make_float2(0.f, 0.f), df_xy = make_float2(0.f, 0.f), gv_xy[3], K_xy[3];
+        float vp_z = 0.f, df_z = 0.f, gv_z[3], K_z[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            gv_xy[j] = K_xy[j] = make_float2(0.f, 0.f);
+            gv_z[j] = K_z[j] = 0.f;
+        }
 #pragma unroll
         for (int c = 0; c < S; ++c) {
 #pragma unroll
             for (int b = 0; b < S; ++b) {
-                float r0[3] = {0.f, 0.f, 0.f}, r1[3] = {0.f, 0.f, 0.f}, rd[3] = {0.f, 0.f, 0.f},
-                      rv[3] = {0.f, 0.f, 0.f};
+                float2 r0 = make_float2(0.f, 0.f), r1 = r0, rd = r0, rv = r0;
+                float r0z = 0.f, r1z = 0.f, rdz = 0.f, rvz = 0.f;
                 const int rowbase = lo[0] + T * ((lo[1] + b) + T * (lo[2] + c));
 #pragma unroll
                 for (int a = 0; a < S; ++a) {
                     const float4 g = tvs[rowbase + a];
-                    const float gs3[3] = {g.x, g.y, g.z};
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        r0[i] = fmaf(w[0][a], gs3[i], r0[i]);
-                        rd[i] = fmaf(dw[0][a], gs3[i], rd[i]);
-                        if (APIC) r1[i] = fmaf(w[0][a] * (float)a, gs3[i], r1[i]);
-                    }
-                    if (!APIC) {
+                    const float2 gxy = make_float2(g.x, g.y);
+                    r0 = __ffma2_rn(wp[a], gxy, r0);
+                    r0z = fmaf(w[0][a], g.z, r0z);
+                    rd = __ffma2_rn(dwp[a], gxy, rd);
+                    rdz = fmaf(dw[0][a], g.z, rdz);
+                    if (APIC) {
+                        r1 = __ffma2_rn(wap[a], gxy, r1);
+                        r1z = fmaf(wap[a].x, g.z, r1z);
+                    } else {
                         const float4 o = tvo[rowbase + a];
-                        rv[0] = fmaf(w[0][a], g.x - o.x, rv[0]);
-                        rv[1] = fmaf(w[0][a], g.y - o.y, rv[1]);
-                        rv[2] = fmaf(w[0][a], g.z - o.z, rv[2]);
+                        const float2 d = __fadd2_rn(gxy, make_float2(-o.x, -o.y));  // g - o, exactly
+                        rv = __ffma2_rn(wp[a], d, rv);
+                        rvz = fmaf(w[0][a], g.z - o.z, rvz);
                     }
                 }
                 const float wyz = w[1][b] * w[2][c];
                 const float dy = dw[1][b] * w[2][c];
                 const float dz = w[1][b] * dw[2][c];
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    vpic[i] = fmaf(wyz, r0[i], vpic[i]);
-                    gv[3 * i + 0] = fmaf(wyz, rd[i], gv[3 * i + 0]);
-                    gv[3 * i + 1] = fmaf(dy, r0[i], gv[3 * i + 1]);
-                    gv[3 * i + 2] = fmaf(dz, r0[i], gv[3 * i + 2]);
-                    if (APIC) {
-                        K[3 * i + 0] = fmaf(wyz, r1[i], K[3 * i + 0]);
-                        K[3 * i + 1] = fmaf(wyz * (float)b, r0[i], K[3 * i + 1]);
-                        K[3 * i + 2] = fmaf(wyz * (float)c, r0[i], K[3 * i + 2]);
-                    } else {
-                        dflip[i] = fmaf(wyz, rv[i], dflip[i]);
-                    }
+                const float2 wyz2 = make_float2(wyz, wyz), dy2 = make_float2(dy, dy), dz2 = make_float2(dz, dz);
+                vp_xy = __ffma2_rn(wyz2, r0, vp_xy);
+                vp_z = fmaf(wyz, r0z, vp_z);
+                gv_xy[0] = __ffma2_rn(wyz2, rd, gv_xy[0]);
+                gv_z[0] = fmaf(wyz, rdz, gv_z[0]);
+                gv_xy[1] = __ffma2_rn(dy2, r0, gv_xy[1]);
+                gv_z[1] = fmaf(dy, r0z, gv_z[1]);
+                gv_xy[2] = __ffma2_rn(dz2, r0, gv_xy[2]);
+                gv_z[2] = fmaf(dz, r0z, gv_z[2]);
+                if (APIC) {
+                    const float wb = wyz * (float)b, wc = wyz * (float)c;
+                    K_xy[0] = __ffma2_rn(wyz2, r1, K_xy[0]);
+                    K_z[0] = fmaf(wyz, r1z, K_z[0]);
+                    K_xy[1] = __ffma2_rn(make_float2(wb, wb), r0, K_xy[1]);
+                    K_z[1] = fmaf(wb, r0z, K_z[1]);
+                    K_xy[2] = __ffma2_rn(make_float2(wc, wc), r0, K_xy[2]);
+                    K_z[2] = fmaf(wc, r0z, K_z[2]);
+                } else {
+                    df_xy = __ffma2_rn(wyz2, rv, df_xy);
+                    df_z = fmaf(wyz, rvz, df_z);
                 }
             }
+        }
+        vpic[0] = vp_xy.x;
+        vpic[1] = vp_xy.y;
+        vpic[2] = vp_z;
+        dflip[0] = df_xy.x;
+        dflip[1] = df_xy.y;
+        dflip[2] = df_z;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            gv[0 * 3 + j] = gv_xy[j].x;
+            gv[1 * 3 + j] = gv_xy[j].y;
+            gv[2 * 3 + j] = gv_z[j];
+            K[0 * 3 + j] = K_xy[j].x;
+            K[1 * 3 + j] = K_xy[j].y;
+            K[2 * 3 + j] = K_z[j];
         }
     }
     // New velocity (src/mpm_solver3d.cu:362-363; apic :366-374).

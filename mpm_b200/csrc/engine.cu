@@ -613,6 +613,7 @@ public:
         dirty_ = false;
         keys_valid_ = false;
         sorted_valid_ = false;
+        stage_check_ = true;
         return MPM_OK;
     }
 
@@ -628,6 +629,7 @@ public:
         c.nscenes = (int)scenes_.size();
         c.stream = stream_;
         c.num_sms = num_sms_;
+        c.p2g_stage = p2g_stage_;
         c.particle_blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((max_n_ + kThreads - 1) / kThreads,
                                                                            (size_t)num_sms_ * 16));
         c.node_blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((max_nodes_ + kThreads - 1) / kThreads,
@@ -931,10 +933,32 @@ public:
         return MPM_OK;
     }
 
+    // P2G stages 32 particles per warp pass in dense scenes and 16 in sparse
+    // ones (fewer than 8 particles per cell on average: the smaller staging
+    // buffer fits 3 CTAs per SM and the passes are rarely full).  Decided
+    // once after the first step that follows a change of the scene set,
+    // from the number of work items of that step.
+    mpm_status checkP2GStage() {
+        if (!stage_check_) return MPM_OK;
+        stage_check_ = false;
+        uint32_t items = 0;
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        CUDA_TRY(cudaMemcpy(&items, counters_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        const int stage = (items > 0 && ntot_ / items < 512) ? 16 : 32;
+        if (stage != p2g_stage_) {
+            p2g_stage_ = stage;
+            dropGraphs();
+        }
+        return MPM_OK;
+    }
+
     mpm_status step(int n) {
         if (n < 0) return fail(MPM_ERR_INVALID_ARG, "nsteps must be >= 0");
         MPM_TRY(ensureReady());
-        for (int i = 0; i < n; ++i) MPM_TRY(stepOnce());
+        for (int i = 0; i < n; ++i) {
+            MPM_TRY(stepOnce());
+            MPM_TRY(checkP2GStage());
+        }
         return MPM_OK;
     }
 
@@ -942,7 +966,10 @@ public:
         if (!ms) return fail(MPM_ERR_INVALID_ARG, "null output");
         MPM_TRY(ensureReady());
         CUDA_TRY(cudaEventRecord(ev_[0][0], stream_));
-        for (int i = 0; i < n; ++i) MPM_TRY(stepOnce());
+        for (int i = 0; i < n; ++i) {
+            MPM_TRY(stepOnce());
+            MPM_TRY(checkP2GStage());
+        }
         CUDA_TRY(cudaEventRecord(ev_[0][1], stream_));
         CUDA_TRY(cudaEventSynchronize(ev_[0][1]));
         CUDA_TRY(cudaEventElapsedTime(ms, ev_[0][0], ev_[0][1]));
@@ -1274,6 +1301,8 @@ private:
     std::vector<SceneDev> host_scenes_;
     int next_id_ = 0;
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
+    int p2g_stage_ = 32;       // see checkP2GStage()
+    bool stage_check_ = true;
     int parity_ = 0, kcur_ = 0, sorted_ = 0;
     size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
     uint32_t total_blocks_ = 0;

@@ -20,6 +20,7 @@ struct LaunchCtx {
     unsigned node_blocks;       // grid.x of dense per-node kernels
     unsigned persistent_blocks; // grid of the persistent block kernels
     int num_sms;
+    int p2g_stage;              // particles staged per warp pass in P2G (16 or 32)
 };
 
 struct BlockBuffers {

@@ -576,9 +576,12 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                     while (cur <= s_last) {
                     const int se = segEnd[cur];
                     const int qlo = max(segBeg[cur], g0) - g0, qhi = min(se, g0 + np) - g0;
+                    // group grp sums the segment's particles j = grp (mod G), in
+                    // order, however the segment is cut into staging passes
+                    const int jlo = g0 + qlo - segBeg[cur];
                     if (lane_on) {
                         const float fa = (float)na, fb = (float)nb;
-                        for (int q = qlo + grp; q < qhi; q += L::G) {
+                        for (int q = qlo + (grp - jlo % L::G + L::G) % L::G; q < qhi; q += L::G) {
                             const float* pq = st + q * L::P;
                             const float4 s0 = *reinterpret_cast<const float4*>(pq);
                             const float m = s0.x;
@@ -1354,11 +1357,12 @@ static void setP2GAttr() {
 // the per-particle staging cost; measured 0.212 vs 0.221 ms on the 1M-particle
 // cubic APIC scene) or 16 (smaller shared-memory footprint).  MPM_P2G_STAGE=16
 // selects the latter.
-static int p2gStage() {
+// MPM_P2G_STAGE=16|24|32 overrides the engine's choice (for measurements).
+static int p2gStageOverride() {
     static int v = [] {
         const char* e = getenv("MPM_P2G_STAGE");
-        const int k = e ? atoi(e) : 32;
-        return (k == 16 || k == 24) ? k : 32;
+        const int k = e ? atoi(e) : 0;
+        return (k == 16 || k == 24 || k == 32) ? k : 0;
     }();
     return v;
 }
@@ -1371,7 +1375,7 @@ static void p2gLaunch(const LaunchCtx& c, const StepArgs& a, int want) {
 
 template <int S, int MODE>
 static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
-    switch (p2gStage()) {
+    switch (p2gStageOverride() ? p2gStageOverride() : c.p2g_stage) {
         case 16: p2gLaunch<S, MODE, 16>(c, a, want); break;
         case 24: p2gLaunch<S, MODE, 24>(c, a, want); break;
         default: p2gLaunch<S, MODE, 32>(c, a, want); break;

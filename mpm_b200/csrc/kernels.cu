@@ -715,6 +715,9 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
     constexpr int F = modeFields(MODE);
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
+    // first work item and number of work items of the 3^3 blocks around the
+    // current one, index (ox + 1) + 3 (oy + 1) + 9 (oz + 1)
+    __shared__ int nbSlot[27], nbItems[27];
     const uint32_t nact = args.counters[0];
     for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
         const BlockItem it = args.active[w];
@@ -725,6 +728,18 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
         const uint32_t lb = it.block - sc.block_base;
         const int B[3] = {(int)(lb % (uint32_t)sc.nb[0]), (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]),
                           (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]))};
+        if (threadIdx.x < 27) {
+            const int o[3] = {(int)threadIdx.x % 3 - 1, ((int)threadIdx.x / 3) % 3 - 1, (int)threadIdx.x / 9 - 1};
+            const int slot = blockSlotAt(args, sc, B[0] + o[0], B[1] + o[1], B[2] + o[2]);
+            int cnt = 0;
+            if (slot >= 0) {
+                const uint32_t blk = args.active[slot].block;
+                for (uint32_t s2 = (uint32_t)slot; s2 < nact && args.active[s2].block == blk; ++s2) ++cnt;
+            }
+            nbSlot[threadIdx.x] = slot;
+            nbItems[threadIdx.x] = cnt;
+        }
+        __syncthreads();
         for (int round = 0; round < 2; ++round) {
             const int d = round * 4 + (threadIdx.x >> 6);
             const int dd[3] = {d & 1, (d >> 1) & 1, (d >> 2) & 1};
@@ -732,7 +747,7 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
             if (N[0] >= sc.nb[0] || N[1] >= sc.nb[1] || N[2] >= sc.nb[2]) continue;
             bool owner = true;
             for (int e = 0; e < d && owner; ++e)
-                if (blockSlotAt(args, sc, N[0] - (e & 1), N[1] - ((e >> 1) & 1), N[2] - ((e >> 2) & 1)) >= 0)
+                if (nbSlot[(dd[0] - (e & 1) + 1) + 3 * (dd[1] - ((e >> 1) & 1) + 1) + 9 * (dd[2] - ((e >> 2) & 1) + 1)] >= 0)
                     owner = false;
             if (!owner) continue;
             const int l = threadIdx.x & 63;
@@ -748,11 +763,11 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
                 const int de[3] = {e & 1, (e >> 1) & 1, (e >> 2) & 1};
                 const int ix = L[0] + 4 * de[0], iy = L[1] + 4 * de[1], iz = L[2] + 4 * de[2];
                 if (ix >= T || iy >= T || iz >= T) continue;
-                const int slot = blockSlotAt(args, sc, N[0] - de[0], N[1] - de[1], N[2] - de[2]);
+                const int nbi = (dd[0] - de[0] + 1) + 3 * (dd[1] - de[1] + 1) + 9 * (dd[2] - de[2] + 1);
+                const int slot = nbSlot[nbi];
                 if (slot < 0) continue;
                 // every work item (tile) of that block, in item order
-                const uint32_t blk = args.active[slot].block;
-                for (uint32_t s2 = (uint32_t)slot; s2 < nact && args.active[s2].block == blk; ++s2) {
+                for (uint32_t s2 = (uint32_t)slot; s2 < (uint32_t)(slot + nbItems[nbi]); ++s2) {
                     const float* tile = args.tiles + (size_t)s2 * args.tile_stride + ix + T * (iy + T * iz);
 #pragma unroll
                     for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
@@ -811,6 +826,7 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
             sc.vstar[node] = make_float4(vs[0], vs[1], vs[2], m);
             if (MODE == MODE_FLIP) sc.vold[node] = make_float4(vo[0], vo[1], vo[2], 0.f);
         }
+        __syncthreads();  // the neighbour table is rewritten for the next item
     }
 }
 

@@ -200,6 +200,7 @@ __global__ void __launch_bounds__(kThreads) radixDownsweepKernel(const uint32_t*
 
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagPrefix = 2u << 30, kCountMask = (1u << 30) - 1u;
 constexpr int kLookbackLimit = 1 << 22;
+constexpr int kLookWidth = 8;  // predecessor words read per look-back round trip
 
 __global__ void __launch_bounds__(kThreads) onesweepHistKernel(const uint32_t* __restrict__ keys, uint32_t n,
                                                                 int passes, int bits, uint32_t* __restrict__ ghist) {
@@ -290,19 +291,19 @@ __global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* _
             atomicExch(mine, kFlagPrefix | run);
         } else {
             atomicExch(mine, kFlagAgg | run);
-            // Walk back over the earlier tiles' words, four per round trip
-            // (independent loads), until an inclusive prefix is found.
+            // Walk back over the earlier tiles' words, kLookWidth per round
+            // trip (independent loads), until an inclusive prefix is found.
             int t = (int)tile - 1;
             int polls = 0;
             bool done = false;
             while (!done && t >= 0) {
-                uint32_t w[4];
+                uint32_t w[kLookWidth];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < kLookWidth; ++q)
                     w[q] = (t - q >= 0) ? *(volatile const uint32_t*)(status + (size_t)(t - q) * 256 + d) : kFlagPrefix;
                 bool waiting = false;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < kLookWidth; ++q) {
                     if (done || waiting) continue;
                     const uint32_t f = w[q] & ~kCountMask;
                     if (f == 0) {  // not published yet: poll again from this tile

@@ -21,6 +21,7 @@ namespace mpm {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kSortTileKeys = kThreads * 8;  // keys per radix-sort tile (8 per thread)
 // Largest particle count of one P2G/G2P work item: denser blocks are split
 // into several items (each with its own P2G tile, merged in item order), so
 // one crowded block cannot serialize a whole step.

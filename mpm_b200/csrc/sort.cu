@@ -18,8 +18,8 @@ namespace {
 
 constexpr int kScanItems = 16;                      // per thread
 constexpr int kScanChunk = kThreads * kScanItems;   // 4096 per CTA
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kThreads * kSortItems;    // 4096 keys per tile
+constexpr int kSortItems = kSortTileKeys / kThreads;
+constexpr int kSortTile = kSortTileKeys;
 
 template <class T>
 __device__ __forceinline__ T warpInclusiveScan(T x) {

@@ -10,7 +10,7 @@
 // scan partials) lives in one fixed, file-scope device array instead.
 //
 // That array is part of the library image: every GPU that loads the library
-// holds it (MPM_SORT_NOALLOC_MAX_KEYS keys, about 8.7 MB) until the process
+// holds it (MPM_SORT_NOALLOC_MAX_KEYS keys, about 8.9 MB) until the process
 // exits.  All calls share it, so calls whose work overlaps on the GPU race
 // with each other; serialize them (one stream, or events).  Every word a call
 // reads from the array is first written by that same call (the histogram by
@@ -32,9 +32,10 @@ mpm_status recordError(mpm_status st, const char* msg);
 namespace {
 
 constexpr size_t kMaxKeys = MPM_SORT_NOALLOC_MAX_KEYS;
-constexpr size_t kTilesMax = (kMaxKeys + 4095) / 4096;  // radix tiles of 4096 keys
+constexpr size_t kTilesMax = (kMaxKeys + kSortTileKeys - 1) / kSortTileKeys;  // radix tiles
 constexpr size_t kHistWords = 256 * kTilesMax;
 constexpr size_t kPartialWords = 64;                    // >= scan chunks of the histogram + 1
+static_assert(kPartialWords >= (kHistWords + 4095) / 4096 + 1, "scan partials too small");
 constexpr size_t kScratchWords = 2 * kMaxKeys + kHistWords + kPartialWords;
 
 // The scratch: [tmp keys | tmp values | histogram | scan partials].

@@ -236,7 +236,7 @@ def peaks():
 # (profiles/g2p_two_balls_128.md, p2g_two_balls_128.md, grid_two_balls_128.md,
 # p2g_g2p_batch16.md; batch64 scaled from its 16-scene subset by particles).
 NCU_TRAFFIC = {
-    "two_balls": {"g2p": 245.9e6, "p2g": 104.7e6, "grid": 4.43e6},
+    "two_balls": {"g2p": 247.3e6, "p2g": 105.0e6, "grid": 4.4e6},
     "batch64": {"g2p": 1.996e9},
 }
 
@@ -346,7 +346,9 @@ def run_ours(args, ws, rank, local):
     total = allsum(ws, float(work.n * args.steps))
     value = total / t_max
 
-    fams = {k: v for k, v in prof.items() if k in ("p2g", "g2p", "grid", "sort")}
+    # the roofline kernel: the longest family among those that move the
+    # state (the sort and compaction are overhead without algorithmic bytes)
+    fams = {k: v for k, v in prof.items() if k in ("p2g", "g2p", "grid")}
     dom = max(fams, key=lambda k: fams[k][0] * fams[k][1])
     dur = fams[dom][0] * 1e-3
     byt = algorithmic_bytes(work.scenes, dom, stats)

@@ -586,6 +586,8 @@ public:
             MPM_TRY(vals_[k].grow(sizeof(uint32_t) * nk, "values"));
         }
         MPM_TRY(sort_scratch_.grow(sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
+        MPM_TRY(inc_scratch_.grow(sizeof(uint32_t) * incrementalSortScratchWords(nk, key_bits_),
+                                  "incremental sort scratch"));
         MPM_TRY(compact_scratch_.grow(sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
                                        "compaction scratch"));
         MPM_TRY(block_count_.grow(sizeof(uint32_t) * tb, "block counts"));
@@ -613,6 +615,7 @@ public:
         dirty_ = false;
         keys_valid_ = false;
         sorted_valid_ = false;
+        incremental_ok_ = false;
         stage_check_ = true;
         return MPM_OK;
     }
@@ -711,14 +714,25 @@ public:
             collect(KF_KEYS);
             keys_valid_ = true;
         }
-        bool inB = false;
         mark(KF_SORT, 0);
-        CUDA_TRY(radixSortOnesweep(keys_[kcur_].as<uint32_t>(), vals_[kcur_].as<uint32_t>(),
-                                   keys_[1 - kcur_].as<uint32_t>(), vals_[1 - kcur_].as<uint32_t>(), ntot_, key_bits_,
-                                   sort_scratch_.as<uint32_t>(), err_.as<uint32_t>(), &inB, stream_));
+        if (incremental_ok_ && !full_sort_only_ && (ntot_ >= kIncrementalMinKeys || incremental_always_)) {
+            // keys_[1 - kcur_] still holds the previous step's sorted keys,
+            // aligned with the live particle order: sort incrementally into it
+            const int out = 1 - kcur_;
+            CUDA_TRY(incrementalSort(keys_[kcur_].as<uint32_t>(), keys_[out].as<uint32_t>(), ntot_, key_bits_,
+                                     keys_[out].as<uint32_t>(), vals_[out].as<uint32_t>(), inc_scratch_.as<uint32_t>(),
+                                     err_.as<uint32_t>(), stream_));
+            sorted_ = out;
+        } else {
+            bool inB = false;
+            CUDA_TRY(radixSortOnesweep(keys_[kcur_].as<uint32_t>(), vals_[kcur_].as<uint32_t>(),
+                                       keys_[1 - kcur_].as<uint32_t>(), vals_[1 - kcur_].as<uint32_t>(), ntot_,
+                                       key_bits_, sort_scratch_.as<uint32_t>(), err_.as<uint32_t>(), &inB, stream_));
+            sorted_ = inB ? 1 - kcur_ : kcur_;
+        }
+        incremental_ok_ = false;  // set again once G2P has reordered the particles by this sort
         mark(KF_SORT, 1);
         collect(KF_SORT);
-        sorted_ = inB ? 1 - kcur_ : kcur_;
         mark(KF_COMPACT, 0);
         launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(),
                               err_.as<uint32_t>());
@@ -829,7 +843,7 @@ public:
     mpm_status stepOnce() {
         bool stale = false;
         for (auto& s : scenes_) stale |= s->stress_stale;
-        const bool steady = use_graphs_ && keys_valid_ && !stale && !profiling_ && !dirty_;
+        const bool steady = use_graphs_ && keys_valid_ && incremental_ok_ && !stale && !profiling_ && !dirty_;
         if (!steady) return stepBody();
         GraphSlot& g = graphs_[parity_][kcur_];
         const int p0 = parity_, k0 = kcur_;
@@ -869,6 +883,7 @@ public:
         kcur_ = 1 - sorted_;
         keys_valid_ = true;
         sorted_valid_ = false;
+        incremental_ok_ = true;
         return MPM_OK;
     }
 
@@ -930,6 +945,7 @@ public:
         kcur_ = next;
         keys_valid_ = true;   // G2P wrote next step's keys and block counts (and stress)
         sorted_valid_ = false;
+        incremental_ok_ = true;  // the live order is now this step's sorted order
         return MPM_OK;
     }
 
@@ -1303,11 +1319,22 @@ private:
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
+    // the previous step's sorted keys are aligned with the live particle order
+    // (sortLive may sort incrementally); MPM_FULL_SORT=1 always sorts all keys,
+    // MPM_INCREMENTAL_SORT=1 sorts incrementally whatever the size (both for
+    // tests and measurements)
+    bool incremental_ok_ = false;
+    const bool full_sort_only_ = getenv("MPM_FULL_SORT") != nullptr;
+    const bool incremental_always_ = getenv("MPM_INCREMENTAL_SORT") != nullptr;
+    // Below this many keys the full radix sort is faster (the movers' sort
+    // costs a few fixed-latency passes): 1M keys 0.072 ms full vs 0.100 ms
+    // incremental, 8.5M keys 0.43 ms vs 0.30 ms on the B200.
+    static constexpr size_t kIncrementalMinKeys = (size_t)3 << 20;
     int parity_ = 0, kcur_ = 0, sorted_ = 0;
     size_t ntot_ = 0, max_nodes_ = 0, max_n_ = 0, max_active_ = 1, tile_stride_ = 0;
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
-    DevMem keys_[2], vals_[2], sort_scratch_, compact_scratch_, block_count_, sbb_, active_,
+    DevMem keys_[2], vals_[2], sort_scratch_, inc_scratch_, compact_scratch_, block_count_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
     bool profiling_ = false;
     cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)

@@ -43,7 +43,14 @@ cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, 
 size_t radixTiles(size_t n);
 size_t onesweepScratchWords(size_t n, int bits);
 cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
-                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st);
+                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st,
+                              const uint32_t* n_dev = nullptr);
+// Incremental sort (sort.cu): the stable sort of `keys` (n, live order) given
+// that `prev` (the previous step's sorted keys, aligned with the same live
+// order) is ascending.  Output equals radixSortOnesweep's (keys, perm).
+size_t incrementalSortScratchWords(size_t n, int bits);
+cudaError_t incrementalSort(const uint32_t* keys, const uint32_t* prev, size_t n, int bits, uint32_t* out_keys,
+                            uint32_t* out_perm, uint32_t* scratch, uint32_t* err, cudaStream_t st);
 cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint32_t* out_vals, uint32_t* tmp_keys,
                                uint32_t* tmp_vals, size_t n, int bits, uint32_t* hist, uint32_t* scan_partials,
                                cudaStream_t st);

@@ -203,7 +203,9 @@ constexpr int kLookbackLimit = 1 << 22;
 constexpr int kLookWidth = 8;  // predecessor words read per look-back round trip
 
 __global__ void __launch_bounds__(kThreads) onesweepHistKernel(const uint32_t* __restrict__ keys, uint32_t n,
-                                                                int passes, int bits, uint32_t* __restrict__ ghist) {
+                                                                const uint32_t* __restrict__ n_dev, int passes,
+                                                                int bits, uint32_t* __restrict__ ghist) {
+    if (n_dev) n = *n_dev;  // the key count is only known on the device
     __shared__ uint32_t h[4][256];
     for (int i = threadIdx.x; i < 4 * 256; i += kThreads) (&h[0][0])[i] = 0;
     __syncthreads();
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* _
                                                                 const uint32_t* __restrict__ vals_in,
                                                                 uint32_t* __restrict__ keys_out,
                                                                 uint32_t* __restrict__ vals_out, uint32_t n,
+                                                                const uint32_t* __restrict__ n_dev,
                                                                 int shift, uint32_t mask,
                                                                 const uint32_t* __restrict__ ghist,
                                                                 uint32_t* __restrict__ tile_counter,
@@ -249,6 +252,10 @@ __global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* _
     }
     __syncthreads();
     const uint32_t tile = tile_s;
+    // With a device-side count the grid covers the largest possible count;
+    // tiles past the actual keys leave at once (later tiles never wait on them).
+    if (n_dev) n = *n_dev;
+    if ((size_t)tile * kSortTile >= n) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     const size_t tbase = (size_t)tile * kSortTile + (size_t)warp * 32 * kSortItems;
@@ -351,9 +358,12 @@ size_t onesweepScratchWords(size_t n, int bits) {
 
 // Stable sort of (keys_a, identity values) by the low `bits` bits, one kernel
 // per 8-bit pass.  `scratch` holds onesweepScratchWords(n, bits) words and is
-// cleared here.  `err` receives bit 8 if a look-back wait gave up.
+// cleared here.  `err` receives bit 8 if a look-back wait gave up.  With
+// `n_dev` the sort covers the first *n_dev keys (known on the device only, at
+// most n) and sorts (keys_a, vals_a) pairs instead of identity values.
 cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, size_t n,
-                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st) {
+                              int bits, uint32_t* scratch, uint32_t* err, bool* result_in_b, cudaStream_t st,
+                              const uint32_t* n_dev) {
     *result_in_b = false;
     if (n == 0) return cudaSuccess;
     if (n > kCountMask) return cudaErrorInvalidValue;
@@ -366,7 +376,7 @@ cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys
     if (e != cudaSuccess) return e;
     const int hblocks = (int)std::min<size_t>((n + kThreads * 16 - 1) / (kThreads * 16), 148 * 4);
     noteLaunches(1 + passes);
-    onesweepHistKernel<<<hblocks, kThreads, 0, st>>>(keys_a, (uint32_t)n, passes, bits, ghist);
+    onesweepHistKernel<<<hblocks, kThreads, 0, st>>>(keys_a, (uint32_t)n, n_dev, passes, bits, ghist);
     uint32_t *kin = keys_a, *vin = vals_a, *kout = keys_b, *vout = vals_b;
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
@@ -374,12 +384,12 @@ cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys
         if (pass_bits <= 0) pass_bits = 1;
         const uint32_t mask = (1u << pass_bits) - 1u;
         uint32_t* stat = status + (size_t)p * ntiles * 256;
-        if (p == 0)
-            onesweepPassKernel<true><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, shift, mask,
-                                                                  ghist + 256 * p, counters + p, stat, err);
+        if (p == 0 && !n_dev)
+            onesweepPassKernel<true><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, n_dev, shift,
+                                                                  mask, ghist + 256 * p, counters + p, stat, err);
         else
-            onesweepPassKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, shift, mask,
-                                                                   ghist + 256 * p, counters + p, stat, err);
+            onesweepPassKernel<false><<<ntiles, kThreads, 0, st>>>(kin, vin, kout, vout, (uint32_t)n, n_dev, shift,
+                                                                   mask, ghist + 256 * p, counters + p, stat, err);
         std::swap(kin, kout);
         std::swap(vin, vout);
         *result_in_b = !*result_in_b;
@@ -441,6 +451,212 @@ cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint
         vin = dv[dst];
         dst ^= 1;
     }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Incremental sort.  Between two steps most particles keep their cell key.
+// The live particle order is the previous step's sorted order, so the keys
+// that did not change ("stayers") already appear in ascending order; only the
+// particles whose key changed ("movers") need sorting.  Steps:
+//   1. partition (one pass, look-back over tiles): stayers (key, index) and
+//      movers (key, index), both in live order;
+//   2. radix-sort the movers by key (stable: ties stay in index order);
+//   3. merge the two sequences by (key, index).
+// Every sequence is ordered by (key, live index), so the result is exactly
+// the stable sort of all keys: the same keys and permutation as
+// radixSortOnesweep.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kPartItems = 8;                        // consecutive keys per thread
+constexpr int kPartTile = kThreads * kPartItems;     // 2048
+constexpr int kMergeItems = 8;
+constexpr int kMergeTile = kThreads * kMergeItems;   // outputs per CTA
+
+__global__ void __launch_bounds__(kThreads) moverPartitionKernel(
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ prev, uint32_t n, uint32_t* __restrict__ a_keys,
+    uint32_t* __restrict__ a_idx, uint32_t* __restrict__ b_keys, uint32_t* __restrict__ b_idx,
+    uint32_t* __restrict__ m_out, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t ntiles,
+    uint32_t* __restrict__ err) {
+    __shared__ uint32_t tile_s, excl_s, tot_s;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = tile_s;
+    const size_t i0 = (size_t)tile * kPartTile + (size_t)threadIdx.x * kPartItems;
+    uint32_t k[kPartItems];
+    uint32_t movers = 0, mvmask = 0;
+#pragma unroll
+    for (int j = 0; j < kPartItems; ++j) {
+        const size_t i = i0 + j;
+        const bool valid = i < n;
+        k[j] = valid ? keys[i] : 0u;
+        const uint32_t pk = valid ? prev[i] : 0u;
+        const bool mv = valid && k[j] != pk;
+        mvmask |= (mv ? 1u : 0u) << j;
+        movers += mv ? 1u : 0u;
+    }
+    const uint32_t before = blockExclusiveScan(movers, &tot_s);  // movers of earlier threads of the tile
+    if (threadIdx.x == 0) {
+        uint32_t excl = 0;
+        if (tile == 0) {
+            atomicExch(&status[0], kFlagPrefix | tot_s);
+        } else {
+            atomicExch(&status[tile], kFlagAgg | tot_s);
+            int t = (int)tile - 1;
+            int polls = 0;
+            while (t >= 0) {
+                const uint32_t w = *(volatile const uint32_t*)(status + t);
+                const uint32_t f = w & ~kCountMask;
+                if (f == 0) {
+                    if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
+                        atomicOr(err, 8u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += w & kCountMask;
+                if (f == kFlagPrefix) break;
+                --t;
+            }
+            atomicExch(&status[tile], kFlagPrefix | (excl + tot_s));
+        }
+        excl_s = excl;
+        if (tile == ntiles - 1) *m_out = excl + tot_s;
+    }
+    __syncthreads();
+    uint32_t mb = excl_s + before;  // movers before the current key
+#pragma unroll
+    for (int j = 0; j < kPartItems; ++j) {
+        const size_t i = i0 + j;
+        if (i >= n) break;
+        if (mvmask >> j & 1u) {
+            b_keys[mb] = k[j];
+            b_idx[mb] = (uint32_t)i;
+            ++mb;
+        } else {
+            const uint32_t pa = (uint32_t)i - mb;  // stayers before it
+            a_keys[pa] = k[j];
+            a_idx[pa] = (uint32_t)i;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long composite(uint32_t key, uint32_t idx) {
+    return ((unsigned long long)key << 32) | idx;
+}
+
+// Number of stayers among the first d outputs of the merge (merge path).
+__device__ __forceinline__ uint32_t mergePath(const uint32_t* a_keys, const uint32_t* a_idx, uint32_t na,
+                                              const uint32_t* b_keys, const uint32_t* b_idx, uint32_t nb, uint32_t d) {
+    uint32_t lo = d > nb ? d - nb : 0u, hi = d < na ? d : na;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t bj = d - 1 - mid;
+        if (composite(a_keys[mid], a_idx[mid]) < composite(b_keys[bj], b_idx[bj])) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Split points of the merge: split[c] = stayers among the first c * kMergeTile outputs.
+__global__ void __launch_bounds__(kThreads) mergeSplitKernel(const uint32_t* __restrict__ a_keys,
+                                                              const uint32_t* __restrict__ a_idx,
+                                                              const uint32_t* __restrict__ b_keys,
+                                                              const uint32_t* __restrict__ b_idx, uint32_t n,
+                                                              const uint32_t* __restrict__ m_dev,
+                                                              uint32_t* __restrict__ split, uint32_t nsplit) {
+    const uint32_t c = blockIdx.x * kThreads + threadIdx.x;
+    if (c >= nsplit) return;
+    const uint32_t m = *m_dev, na = n - m;
+    const uint32_t d = (uint32_t)min((size_t)c * kMergeTile, (size_t)n);
+    split[c] = mergePath(a_keys, a_idx, na, b_keys, b_idx, m, d);
+}
+
+// One CTA merges kMergeTile outputs: its stayer and mover ranges are staged in
+// shared memory, each thread finds its own split there and merges 8 outputs.
+__global__ void __launch_bounds__(kThreads) mergeKernel(const uint32_t* __restrict__ a_keys,
+                                                         const uint32_t* __restrict__ a_idx,
+                                                         const uint32_t* __restrict__ b_keys,
+                                                         const uint32_t* __restrict__ b_idx, uint32_t n,
+                                                         const uint32_t* __restrict__ m_dev,
+                                                         const uint32_t* __restrict__ split,
+                                                         uint32_t* __restrict__ out_keys,
+                                                         uint32_t* __restrict__ out_perm) {
+    __shared__ unsigned long long sa[kMergeTile], sb[kMergeTile];
+    const uint32_t m = *m_dev, na = n - m;
+    const uint32_t d0 = blockIdx.x * kMergeTile;
+    if (d0 >= n) return;
+    const uint32_t d1 = min(n, d0 + (uint32_t)kMergeTile);
+    const uint32_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
+    const uint32_t b0 = d0 - a0, b1 = d1 - a1;
+    const uint32_t la = a1 - a0, lb = b1 - b0;  // la + lb = d1 - d0 <= kMergeTile
+    for (uint32_t i = threadIdx.x; i < la; i += kThreads) sa[i] = composite(a_keys[a0 + i], a_idx[a0 + i]);
+    for (uint32_t i = threadIdx.x; i < lb; i += kThreads) sb[i] = composite(b_keys[b0 + i], b_idx[b0 + i]);
+    __syncthreads();
+    const uint32_t dl = threadIdx.x * kMergeItems;
+    if (dl >= la + lb) return;
+    uint32_t lo = dl > lb ? dl - lb : 0u, hi = dl < la ? dl : la;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sa[mid] < sb[dl - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+    }
+    uint32_t ia = lo, ib = dl - lo;
+    const uint32_t dend = min(dl + (uint32_t)kMergeItems, la + lb);
+    for (uint32_t dd = dl; dd < dend; ++dd) {
+        const bool takeA = ib >= lb || (ia < la && sa[ia] < sb[ib]);
+        const unsigned long long v = takeA ? sa[ia++] : sb[ib++];
+        out_keys[d0 + dd] = (uint32_t)(v >> 32);
+        out_perm[d0 + dd] = (uint32_t)v;
+    }
+    (void)na;
+}
+
+}  // namespace
+
+// Scratch layout (u32 words): a_keys, a_idx, b_keys, b_idx, b_keys2, b_idx2
+// (n each), mover count, partition tile counter and status words, merge
+// split points, then the movers' radix-sort scratch.
+static size_t partitionTiles(size_t n) { return (n + kPartTile - 1) / kPartTile; }
+static size_t mergeSplits(size_t n) { return (n + kMergeTile - 1) / kMergeTile + 1; }
+
+size_t incrementalSortScratchWords(size_t n, int bits) {
+    return 6 * n + 2 + partitionTiles(n) + mergeSplits(n) + onesweepScratchWords(n, bits) + 64;
+}
+
+cudaError_t incrementalSort(const uint32_t* keys, const uint32_t* prev, size_t n, int bits, uint32_t* out_keys,
+                            uint32_t* out_perm, uint32_t* scratch, uint32_t* err, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    if (n > kCountMask) return cudaErrorInvalidValue;
+    uint32_t* a_keys = scratch;
+    uint32_t* a_idx = a_keys + n;
+    uint32_t* b_keys = a_idx + n;
+    uint32_t* b_idx = b_keys + n;
+    uint32_t* b_keys2 = b_idx + n;
+    uint32_t* b_idx2 = b_keys2 + n;
+    uint32_t* m_dev = b_idx2 + n;
+    uint32_t* tile_counter = m_dev + 1;
+    uint32_t* status = tile_counter + 1;
+    const size_t ptiles = partitionTiles(n);
+    uint32_t* split = status + ptiles;
+    const size_t nsplit = mergeSplits(n);
+    uint32_t* sort_scratch = split + nsplit;
+    cudaError_t e = cudaMemsetAsync(m_dev, 0, sizeof(uint32_t) * (2 + ptiles), st);
+    if (e != cudaSuccess) return e;
+    noteLaunches(3);
+    moverPartitionKernel<<<(unsigned)ptiles, kThreads, 0, st>>>(keys, prev, (uint32_t)n, a_keys, a_idx, b_keys, b_idx,
+                                                                m_dev, tile_counter, status, (uint32_t)ptiles, err);
+    bool inB = false;
+    e = radixSortOnesweep(b_keys, b_idx, b_keys2, b_idx2, n, bits, sort_scratch, err, &inB, st, m_dev);
+    if (e != cudaSuccess) return e;
+    const uint32_t* mk = inB ? b_keys2 : b_keys;
+    const uint32_t* mi = inB ? b_idx2 : b_idx;
+    mergeSplitKernel<<<(unsigned)((nsplit + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        a_keys, a_idx, mk, mi, (uint32_t)n, m_dev, split, (uint32_t)nsplit);
+    mergeKernel<<<(unsigned)(nsplit - 1), kThreads, 0, st>>>(a_keys, a_idx, mk, mi, (uint32_t)n, m_dev, split, out_keys,
+                                                             out_perm);
     return cudaGetLastError();
 }
 

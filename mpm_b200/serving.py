@@ -40,7 +40,7 @@ def scene_device_bytes(scene) -> int:
     flip = scene.transfer == _abi.TRANSFER_PIC_FLIP
     particles = 2 * n * (41 * 4 + 4 + 2)
     grid = nodes * 16 * (2 if flip else 1)
-    sort = n * 16 + (n + 4095) // 4096 * 256 * 4
+    sort = n * (16 + 24) + (n + 2047) // 2048 * 256 * 4 * 2  # radix + incremental sort scratch
     tables = blocks * (4 + 8 + 8 + 4)
     S = {0: 2, 1: 3, 2: 4}[scene.interpolation]
     tiles = min(blocks, max(n, 1)) * 7 * (S + 3) ** 3 * 4

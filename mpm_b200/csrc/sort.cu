@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kThreads) onesweepHistKernel(const uint32_t* _
 }
 
 template <bool kIdentVals>
-__global__ void __launch_bounds__(kThreads) onesweepPassKernel(const uint32_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kThreads, 4) onesweepPassKernel(const uint32_t* __restrict__ keys_in,
                                                                 const uint32_t* __restrict__ vals_in,
                                                                 uint32_t* __restrict__ keys_out,
                                                                 uint32_t* __restrict__ vals_out, uint32_t n,

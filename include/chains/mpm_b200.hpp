@@ -98,6 +98,15 @@ public:
         check(mpm_solver_download(h_, MPM_FIELD_POSITION4, out.data()), "positions4");
         return out;
     }
+    // Density grid sum_p m_p w_ip / h^3 (what writeToOpenVDB rasterises),
+    // res.x * res.y * res.z floats, index x + X (y + Y z).
+    std::vector<float> density() {
+        mpm_scene_desc d{};
+        check(mpm_solver_get_desc(h_, &d), "density");
+        std::vector<float> out((size_t)d.resolution[0] * d.resolution[1] * d.resolution[2]);
+        check(mpm_solver_download_density(h_, out.data()), "density");
+        return out;
+    }
     std::vector<float> download(int field, int comps) {
         std::vector<float> out((size_t)comps * numParticles());
         check(mpm_solver_download(h_, field, out.data()), "download");

@@ -250,6 +250,12 @@ MPM_API mpm_status mpm_solver_download(mpm_solver* s, int32_t field, float* host
 MPM_API mpm_status mpm_solver_download_async(mpm_solver* s, int32_t field, float* host_out);
 /* Wait for every asynchronous download issued so far. */
 MPM_API mpm_status mpm_solver_download_wait(mpm_solver* s);
+/* Density of the current state on the dense grid: res[0]*res[1]*res[2]
+ * floats, node index x + X (y + Y z), value sum_p m_p w_ip / h^3 -- the grid
+ * that writeToOpenVDB (src/mpm_solver3d.cu:509-572) rasterises and writes as
+ * an OpenVDB "density" grid; here it is returned headless (no OpenVDB file).
+ * Does not change the particle state. */
+MPM_API mpm_status mpm_solver_download_density(mpm_solver* s, float* host_out);
 /* Download a dense grid field (res^3 * components floats).  Valid after
  * particles_to_grid() and the grid sub-steps of the split API, or after
  * mpm_solver_step when the solver keeps the dense debug grid. */

@@ -40,8 +40,11 @@ MPM_API mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t fi
 /* Asynchronous form (see mpm_solver_download_async) and its wait. */
 MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
+/* Density grid of one scene (see mpm_solver_download_density). */
+MPM_API mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out);
 MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
 MPM_API mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_t* n);
+MPM_API mpm_status mpm_batch_scene_desc(const mpm_batch* b, int32_t scene_id, mpm_scene_desc* desc);
 MPM_API mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out);
 /* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */
 MPM_API mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms);

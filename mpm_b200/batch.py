@@ -30,6 +30,7 @@ class Batch:
         check(self._lib.mpm_batch_create(C.byref(h)), "mpm_batch_create")
         self._h = h
         self._n: Dict[int, int] = {}
+        self._res: Dict[int, tuple] = {}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -57,6 +58,7 @@ class Batch:
               "mpm_batch_add_scene")
         del keep
         self._n[int(sid.value)] = scene.n
+        self._res[int(sid.value)] = tuple(int(r) for r in scene.resolution)
         return int(sid.value)
 
     def remove(self, sid: int):
@@ -73,7 +75,10 @@ class Batch:
         check(self._lib.mpm_batch_load_scene(self._h, os.fsencode(path), C.byref(sid)), "mpm_batch_load_scene")
         n = C.c_size_t()
         check(self._lib.mpm_batch_scene_particles(self._h, sid, C.byref(n)), "mpm_batch_scene_particles")
+        desc = _abi.SceneDesc()
+        check(self._lib.mpm_batch_scene_desc(self._h, sid, C.byref(desc)), "mpm_batch_scene_desc")
         self._n[int(sid.value)] = int(n.value)
+        self._res[int(sid.value)] = tuple(int(r) for r in desc.resolution)
         return int(sid.value)
 
     @property
@@ -102,6 +107,14 @@ class Batch:
         check(self._lib.mpm_batch_download(self._h, int(sid), int(field), out.ctypes.data_as(C.POINTER(C.c_float))),
               "mpm_batch_download")
         return out.reshape(n, 3, 3) if comps == 9 else (out[:, 0] if comps == 1 else out)
+
+    def density(self, sid: int) -> np.ndarray:
+        """Density grid of one scene (see MPMSolver3D.density), shape (res_z, res_y, res_x)."""
+        res = self._res[int(sid)]
+        out = np.empty(res[0] * res[1] * res[2], np.float32)
+        check(self._lib.mpm_batch_download_density(self._h, int(sid), out.ctypes.data_as(C.POINTER(C.c_float))),
+              "mpm_batch_download_density")
+        return out.reshape(res[2], res[1], res[0])
 
     def download_async(self, sid: int, field: int, ptr: int):
         """Queue a download of one scene's current state into caller memory at

@@ -1221,6 +1221,38 @@ public:
         return MPM_OK;
     }
 
+    // Density of one scene on its dense grid (res^3 floats, node index
+    // x + X (y + Y z)): a mass pass of that scene alone on a cleared grid, then
+    // m / h^3 per node.  The particle state is not changed: the next step
+    // continues exactly as without this call.
+    mpm_status downloadDensity(int id, float* host) {
+        MPM_TRY(ensureReady());
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!host) return fail(MPM_ERR_INVALID_ARG, "null output pointer");
+        SceneHost& s = *scenes_[idx];
+        const size_t nodes = s.nodes();
+        CUDA_TRY(cudaMemsetAsync(s.vstar.p, 0, sizeof(float4) * nodes, stream_));
+        if (s.n > 0) {
+            for (size_t i = 0; i < scenes_.size(); ++i) host_scenes_[i].init_pass = (int)(i == (size_t)idx);
+            MPM_TRY(uploadSceneTable());
+            if (!sorted_valid_) MPM_TRY(sortLive());
+            StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
+            LaunchCtx c = ctx();
+            launchP2G(c, a, s.S, MODE_MASS, -1);
+            launchGrid(c, a, s.S, MODE_MASS, -1);
+            keys_valid_ = false;  // block counts were consumed by the compaction
+        }
+        // cell_vol_inv as the reference forms it: 1.0 / (h*h*h) in double, stored as float
+        const float h = s.desc.stride;
+        const float inv = (float)(1.0 / (double)(h * h * h));
+        MPM_TRY(tmp_.grow(sizeof(float) * nodes, "density buffer"));
+        launchDensity(ctx(), s.vstar.as<float4>(), nodes, inv, tmp_.as<float>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(host, tmp_.p, sizeof(float) * nodes, cudaMemcpyDeviceToHost, stream_));
+        return synchronize();
+    }
+
     mpm_status upload(int id, int field, const float* host) {
         MPM_TRY(ensureReady());
         int idx = sceneIndex(id);
@@ -1569,6 +1601,10 @@ mpm_status mpm_solver_download_wait(mpm_solver* s) {
     MPM_TRY(check(s));
     return s->eng.downloadWait();
 }
+mpm_status mpm_solver_download_density(mpm_solver* s, float* host_out) {
+    MPM_TRY(check(s));
+    return s->eng.downloadDensity(s->scene, host_out);
+}
 mpm_status mpm_solver_download_grid(mpm_solver* s, int32_t field, float* host_out) {
     MPM_TRY(check(s));
     if (!host_out) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -1731,6 +1767,10 @@ mpm_status mpm_batch_download_wait(mpm_batch* b) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.downloadWait();
 }
+mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.downloadDensity(scene_id, host_out);
+}
 mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
     if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
     *n = (int32_t)b->eng.numScenes();
@@ -1741,6 +1781,13 @@ mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_
     const mpm::SceneHost* s = const_cast<mpm_batch*>(b)->eng.scene(scene_id);
     if (!s) return mpm::fail(MPM_ERR_INVALID_ARG, "unknown scene id");
     *n = s->n;
+    return MPM_OK;
+}
+mpm_status mpm_batch_scene_desc(const mpm_batch* b, int32_t scene_id, mpm_scene_desc* desc) {
+    if (!b || !desc) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");
+    const mpm::SceneHost* s = const_cast<mpm_batch*>(b)->eng.scene(scene_id);
+    if (!s) return mpm::fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+    *desc = s->desc;
     return MPM_OK;
 }
 mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms) {

@@ -1477,6 +1477,19 @@ void launchVolume(const LaunchCtx& c, int parity, int S) {
     else if (S == 3) volumeKernel<3><<<g, kThreads, 0, c.stream>>>(c.scenes, parity);
     else volumeKernel<4><<<g, kThreads, 0, c.stream>>>(c.scenes, parity);
 }
+// Density rasterisation (writeToOpenVDB, src/mpm_solver3d.cu:509-572): node
+// density = sum_p m_p w_ip / h^3, from the node masses of a mass pass.
+__global__ void densityKernel(const float4* __restrict__ vstar, size_t nodes, float inv_cell_vol,
+                              float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads)
+        out[i] = vstar[i].w * inv_cell_vol;
+}
+void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out) {
+    noteLaunches(1);
+    const unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((nodes + kThreads - 1) / kThreads,
+                                                                          (size_t)c.num_sms * 16));
+    densityKernel<<<blocks, kThreads, 0, c.stream>>>(vstar, nodes, inv_cell_vol, out);
+}
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out) {
     noteLaunches(1);
     gatherFieldKernel<<<c.particle_blocks, kThreads, 0, c.stream>>>(c.scenes, scene, parity, field, comps, mode, out);

@@ -296,6 +296,13 @@ class _SolverBase:
         after download_wait() or synchronize()."""
         check(self._lib.mpm_solver_download_async(self._h, int(field), C.c_void_p(ptr)), "download_async")
 
+    def density(self) -> np.ndarray:
+        """Density grid sum_p m_p w_ip / h^3 of the current state (the grid the
+        reference's writeToOpenVDB writes), shape (res_z, res_y, res_x)."""
+        out = np.empty(self._res[0] * self._res[1] * self._res[2], np.float32)
+        check(self._lib.mpm_solver_download_density(self._h, out.ctypes.data_as(C.POINTER(C.c_float))), "density")
+        return out.reshape(self._res[2], self._res[1], self._res[0])
+
     def download_wait(self):
         check(self._lib.mpm_solver_download_wait(self._h), "download_wait")
 

@@ -59,6 +59,15 @@ struct MaterialPoint3D {
 };
 using APICMaterialPoint3D = MaterialPoint3D;
 
+// LevelSetCollisionObject3D (include/collision_object3d.h:9-12): signed
+// distance per grid node (index x + X (y + Y z), negative inside), here in
+// float with the object's friction and surface velocity.
+struct LevelSetCollisionObject3D {
+    std::vector<float> level_set;
+    float friction = 0.f;
+    Vec3f velocity;
+};
+
 namespace detail {
 
 class SolverBase {
@@ -107,6 +116,16 @@ public:
         check(mpm_solver_download_density(h_, out.data()), "density");
         return out;
     }
+    // Applies the object in every grid collision (mpm_solver_set_level_set).
+    void setCollisionObject(const LevelSetCollisionObject3D& obj) {
+        const float v[3] = {obj.velocity.x, obj.velocity.y, obj.velocity.z};
+        mpm_scene_desc d{};
+        check(mpm_solver_get_desc(h_, &d), "setCollisionObject");
+        if (obj.level_set.size() != (size_t)d.resolution[0] * d.resolution[1] * d.resolution[2])
+            throw std::runtime_error("setCollisionObject: level set size does not match the grid");
+        check(mpm_solver_set_level_set(h_, obj.level_set.data(), obj.friction, v), "setCollisionObject");
+    }
+    void clearCollisionObject() { check(mpm_solver_set_level_set(h_, nullptr, 0.f, nullptr), "clearCollisionObject"); }
     std::vector<float> download(int field, int comps) {
         std::vector<float> out((size_t)comps * numParticles());
         check(mpm_solver_download(h_, field, out.data()), "download");

@@ -231,6 +231,19 @@ MPM_API mpm_status mpm_solver_advect_particles(mpm_solver* s, float dt);  /* :38
 MPM_API mpm_status mpm_solver_set_particles_collision(mpm_solver* s, int32_t enable);
 MPM_API mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32_t* enable);
 
+/* Level-set collision object (LevelSetCollisionObject3D, a level set per grid
+ * node, include/collision_object3d.h:9-12; declared but never applied by the
+ * reference).  phi: res_x*res_y*res_z signed distances in world units at the
+ * grid nodes, index x + X*(y + Y*z), negative inside the object; NULL removes
+ * the object.  Each grid collision (and each particle collision when enabled)
+ * applies it after the grid boundary: the distance is interpolated
+ * trilinearly at the moved position (node + dt v*, particle + dt v); where it
+ * is <= 0 the velocity relative to the object's surface velocity gets the
+ * friction law of applyBoundaryCollision (src/collision_object3d.cu:38-51)
+ * with the normalised trilinear gradient as normal.  velocity (3 floats, NULL
+ * = at rest) is the surface velocity; friction >= 0.  The values are copied. */
+MPM_API mpm_status mpm_solver_set_level_set(mpm_solver* s, const float* phi, float friction, const float* velocity);
+
 MPM_API mpm_status mpm_solver_num_particles(const mpm_solver* s, size_t* n);
 MPM_API mpm_status mpm_solver_get_desc(const mpm_solver* s, mpm_scene_desc* desc);
 

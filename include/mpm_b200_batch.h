@@ -42,6 +42,9 @@ MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int3
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 /* Density grid of one scene (see mpm_solver_download_density). */
 MPM_API mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out);
+/* Level-set collision object of one scene (see mpm_solver_set_level_set). */
+MPM_API mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* phi, float friction,
+                                           const float* velocity);
 MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
 MPM_API mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_t* n);
 MPM_API mpm_status mpm_batch_scene_desc(const mpm_batch* b, int32_t scene_id, mpm_scene_desc* desc);

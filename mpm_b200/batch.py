@@ -116,6 +116,16 @@ class Batch:
               "mpm_batch_download_density")
         return out.reshape(res[2], res[1], res[0])
 
+    def set_collision_object(self, sid: int, obj=None):
+        """Level-set collision object of one scene (see MPMSolver3D.set_collision_object)."""
+        F = C.POINTER(C.c_float)
+        if obj is None:
+            check(self._lib.mpm_batch_set_level_set(self._h, int(sid), None, 0.0, None), "mpm_batch_set_level_set")
+            return
+        phi, vel = obj.arrays(self._res[int(sid)])
+        check(self._lib.mpm_batch_set_level_set(self._h, int(sid), phi.ctypes.data_as(F), float(obj.friction),
+                                                vel.ctypes.data_as(F)), "mpm_batch_set_level_set")
+
     def download_async(self, sid: int, field: int, ptr: int):
         """Queue a download of one scene's current state into caller memory at
         address ptr; complete after download_wait() or synchronize()."""

@@ -170,6 +170,9 @@ struct SceneHost {
     bool stage_pending[2] = {};
     int stage_next = 0;
     std::vector<mpm_material> mats_in;  // as given (kept for checkpoints)
+    DevMem phi;                         // level-set collision object (nodes floats), if set
+    bool has_phi = false;
+    float phi_friction = 0.f, phi_vel[3] = {0.f, 0.f, 0.f};
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
     ~SceneHost() {
         for (int k = 0; k < 2; ++k) {
@@ -365,9 +368,12 @@ public:
     // mpm_scene_desc, i32 nmaterials, mpm_material[nmaterials], u64 n,
     // u32 flags (bit 0: cached stress stale), then in the engine's internal
     // particle order the 41 float planes (n floats each), the original
-    // particle ids (u32 x n) and the material ids (u16 x n).  Restoring that
-    // order and the cached stress makes the continuation bitwise identical.
-    static constexpr uint32_t kCkptVersion = 1;
+    // particle ids (u32 x n) and the material ids (u16 x n); version 2 adds
+    // u32 has_level_set and, if set, f32 friction, f32 velocity[3] and the
+    // level set (f32 per grid node).  Restoring that order and the cached
+    // stress makes the continuation bitwise identical.  Version 1 files
+    // (no level-set section) are still read.
+    static constexpr uint32_t kCkptVersion = 2;
 
     mpm_status saveScene(int id, const char* path) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -388,6 +394,12 @@ public:
             CUDA_TRY(cudaMemcpy(pid.data(), s.buf_pid[parity_].p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
             CUDA_TRY(cudaMemcpy(mat.data(), s.buf_mat[parity_].p, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost));
         }
+        std::vector<float> phi;
+        if (s.has_phi) {
+            phi.resize(s.nodes());
+            CUDA_TRY(cudaMemcpy(phi.data(), s.phi.p, sizeof(float) * phi.size(), cudaMemcpyDeviceToHost));
+        }
+        const uint32_t has_phi = s.has_phi ? 1u : 0u;
         std::FILE* fp = std::fopen(path, "wb");
         if (!fp) return fail(MPM_ERR_IO, std::string("cannot open ") + path + " for writing");
         const char magic[8] = {'M', 'P', 'M', 'B', '2', '0', '0', 0};
@@ -402,7 +414,10 @@ public:
                   std::fwrite(&n64, 8, 1, fp) == 1 && std::fwrite(&flags, 4, 1, fp) == 1 &&
                   std::fwrite(planes.data(), sizeof(float), planes.size(), fp) == planes.size() &&
                   std::fwrite(pid.data(), sizeof(uint32_t), n, fp) == n &&
-                  std::fwrite(mat.data(), sizeof(uint16_t), n, fp) == n;
+                  std::fwrite(mat.data(), sizeof(uint16_t), n, fp) == n && std::fwrite(&has_phi, 4, 1, fp) == 1;
+        if (ok && has_phi)
+            ok = std::fwrite(&s.phi_friction, 4, 1, fp) == 1 && std::fwrite(s.phi_vel, 4, 3, fp) == 3 &&
+                 std::fwrite(phi.data(), sizeof(float), phi.size(), fp) == phi.size();
         ok = (std::fclose(fp) == 0) && ok;
         if (!ok) return fail(MPM_ERR_IO, std::string("write failed: ") + path);
         return MPM_OK;
@@ -417,6 +432,9 @@ public:
         std::vector<float> planes;
         std::vector<uint32_t> pid;
         std::vector<uint16_t> mat;
+        bool has_phi = false;
+        float phi_friction = 0.f, phi_vel[3] = {0.f, 0.f, 0.f};
+        std::vector<float> phi;
     };
     static mpm_status readCheckpoint(const char* path, Checkpoint* ck) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -429,7 +447,7 @@ public:
         uint64_t n64 = 0;
         if (std::fread(magic, 1, 8, fp) != 8 || memcmp(magic, "MPMB200", 8) != 0)
             return fail(MPM_ERR_PARSE, std::string(path) + ": not a checkpoint");
-        if (std::fread(&ver, 4, 1, fp) != 1 || ver != kCkptVersion || std::fread(&dsz, 4, 1, fp) != 1 ||
+        if (std::fread(&ver, 4, 1, fp) != 1 || ver < 1 || ver > kCkptVersion || std::fread(&dsz, 4, 1, fp) != 1 ||
             dsz != sizeof(mpm_scene_desc))
             return fail(MPM_ERR_PARSE, std::string(path) + ": unsupported checkpoint version");
         if (std::fread(&ck->desc, sizeof(mpm_scene_desc), 1, fp) != 1 || std::fread(&nm, 4, 1, fp) != 1 || nm < 1 ||
@@ -456,6 +474,23 @@ public:
             std::fread(ck->pid.data(), sizeof(uint32_t), n, fp) != n ||
             std::fread(ck->mat.data(), sizeof(uint16_t), n, fp) != n)
             return fail(MPM_ERR_PARSE, std::string(path) + ": truncated particle data");
+        if (ver >= 2) {
+            uint32_t has_phi = 0;
+            if (std::fread(&has_phi, 4, 1, fp) != 1 || has_phi > 1)
+                return fail(MPM_ERR_PARSE, std::string(path) + ": truncated or corrupt level-set section");
+            if (has_phi) {
+                const size_t nodes = (size_t)ck->desc.resolution[0] * ck->desc.resolution[1] * ck->desc.resolution[2];
+                try {
+                    ck->phi.resize(nodes);
+                } catch (const std::bad_alloc&) {
+                    return fail(MPM_ERR_OOM, "host allocation failed");
+                }
+                if (std::fread(&ck->phi_friction, 4, 1, fp) != 1 || std::fread(ck->phi_vel, 4, 3, fp) != 3 ||
+                    std::fread(ck->phi.data(), sizeof(float), nodes, fp) != nodes)
+                    return fail(MPM_ERR_PARSE, std::string(path) + ": truncated level-set section");
+                ck->has_phi = true;
+            }
+        }
         std::vector<uint8_t> seen(n, 0);
         for (size_t i = 0; i < n; ++i) {
             if (ck->pid[i] >= n || seen[ck->pid[i]]) return fail(MPM_ERR_PARSE, std::string(path) + ": bad particle ids");
@@ -483,6 +518,13 @@ public:
         sc->need_init = false;  // V0 is part of the state
         sc->stress_stale = (ck.flags & 1u) != 0;
         *out_id = registerScene(std::move(sc));
+        if (ck.has_phi) {
+            mpm_status st = setLevelSet(*out_id, ck.phi.data(), ck.phi_friction, ck.phi_vel);
+            if (st != MPM_OK) {
+                removeScene(*out_id);
+                return st;
+            }
+        }
         return MPM_OK;
     }
 
@@ -569,6 +611,9 @@ public:
             d.vold = s.vold.as<float4>();
             d.mats = s.mats.as<MaterialDev>();
             d.dbg = s.dbg.as<float>();
+            d.phi = s.has_phi ? s.phi.as<float>() : nullptr;
+            d.phi_friction = s.phi_friction;
+            for (int a = 0; a < 3; ++a) d.phi_vel[a] = s.phi_vel[a];
             max_nodes_ = std::max(max_nodes_, s.nodes());
             max_n_ = std::max(max_n_, s.n);
         }
@@ -1314,6 +1359,43 @@ public:
         return MPM_OK;
     }
 
+    // Level-set collision object of a scene: phi holds the signed distance at
+    // every grid node (index x + X(y + Y z), world units, negative inside),
+    // or is null to remove the object.
+    mpm_status setLevelSet(int id, const float* phi, float friction, const float* velocity) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        SceneHost& s = *scenes_[idx];
+        if (phi) {
+            for (int a = 0; a < 3; ++a)
+                if (s.desc.resolution[a] < 2) return fail(MPM_ERR_INVALID_ARG, "a level set needs >= 2 nodes per axis");
+            if (!(friction >= 0.f) || !std::isfinite(friction))
+                return fail(MPM_ERR_INVALID_ARG, "level-set friction must be finite and >= 0");
+            if (velocity)
+                for (int a = 0; a < 3; ++a)
+                    if (!std::isfinite(velocity[a])) return fail(MPM_ERR_INVALID_ARG, "level-set velocity not finite");
+            const size_t nodes = s.nodes();
+            for (size_t i = 0; i < nodes; ++i)
+                if (!std::isfinite(phi[i])) return fail(MPM_ERR_INVALID_ARG, "level set has a non-finite value");
+            CUDA_TRY(cudaStreamSynchronize(stream_));  // earlier steps may still read the old values
+            MPM_TRY(s.phi.grow(sizeof(float) * nodes, "level set"));
+            CUDA_TRY(cudaMemcpy(s.phi.p, phi, sizeof(float) * nodes, cudaMemcpyHostToDevice));
+            s.has_phi = true;
+            s.phi_friction = friction;
+            for (int a = 0; a < 3; ++a) s.phi_vel[a] = velocity ? velocity[a] : 0.f;
+        } else {
+            s.has_phi = false;
+        }
+        if (!dirty_) {
+            SceneDev& d = host_scenes_[idx];
+            d.phi = s.has_phi ? s.phi.as<float>() : nullptr;
+            d.phi_friction = s.phi_friction;
+            for (int a = 0; a < 3; ++a) d.phi_vel[a] = s.phi_vel[a];
+            MPM_TRY(uploadSceneTable());
+        }
+        return MPM_OK;
+    }
+
     mpm_status profile(int enable) {
         MPM_TRY(accumulateProfile());
         if (enable) {
@@ -1571,6 +1653,10 @@ mpm_status mpm_solver_set_particles_collision(mpm_solver* s, int32_t enable) {
     MPM_TRY(check(s));
     return s->eng.setParticlesCollision(s->scene, enable);
 }
+mpm_status mpm_solver_set_level_set(mpm_solver* s, const float* phi, float friction, const float* velocity) {
+    MPM_TRY(check(s));
+    return s->eng.setLevelSet(s->scene, phi, friction, velocity);
+}
 mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32_t* enable) {
     MPM_TRY(check(s));
     if (!enable) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -1770,6 +1856,11 @@ mpm_status mpm_batch_download_wait(mpm_batch* b) {
 mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.downloadDensity(scene_id, host_out);
+}
+mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* phi, float friction,
+                                   const float* velocity) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.setLevelSet(scene_id, phi, friction, velocity);
 }
 mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
     if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");

@@ -76,6 +76,12 @@ struct SceneDev {
     float4* vold;          // dense res^3 (PIC-FLIP)
     const MaterialDev* mats;
     float* dbg;            // split-mode dense grid: mass, vel[3], force[3], vstar[3] planes
+    // Level-set collision object (the reference's LevelSetCollisionObject3D,
+    // include/collision_object3d.h:9-12): signed distance sampled on the grid
+    // nodes (index x + X(y + Y z), negative inside), or null.
+    const float* phi;
+    float phi_friction;
+    float phi_vel[3];      // velocity of the collider's surface
 };
 
 struct BlockItem {

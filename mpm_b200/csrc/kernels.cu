@@ -28,6 +28,77 @@ uint64_t kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {
 
+// Level-set collision object (LevelSetCollisionObject3D,
+// include/collision_object3d.h:9-12, declared but not applied by the
+// reference).  The signed distance is interpolated trilinearly at pos (clamped
+// to the grid); where it is <= 0 the velocity relative to the collider's
+// surface gets the friction law of applyBoundaryCollision
+// (src/collision_object3d.cu:38-51) with the normalised trilinear gradient as
+// the normal.
+__device__ __forceinline__ float3 levelSetCollisionV(const SceneDev& sc, float px, float py, float pz, float vx, float vy,
+                                                  float vz) {
+    const float pos[3] = {px, py, pz};
+    float vel[3] = {vx, vy, vz};
+    int i0[3];
+    float f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float g = (pos[a] - sc.origin[a]) * sc.inv_h;
+        g = fminf(fmaxf(g, 0.f), (float)(sc.res[a] - 1));
+        i0[a] = min((int)g, sc.res[a] - 2);
+        f[a] = g - (float)i0[a];
+    }
+    const size_t X = (size_t)sc.res[0], XY = X * (size_t)sc.res[1];
+    const float* p0 = sc.phi + (size_t)i0[0] + X * (size_t)i0[1] + XY * (size_t)i0[2];
+    float c[8];  // corner (dx, dy, dz) at index dx + 2 dy + 4 dz
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c[k] = p0[(k & 1) + ((k >> 1) & 1) * X + ((k >> 2) & 1) * XY];
+    float phi = 0.f, gr[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int d[3] = {k & 1, (k >> 1) & 1, (k >> 2) & 1};
+        float w[3], s[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a] = d[a] ? f[a] : 1.f - f[a];
+            s[a] = d[a] ? 1.f : -1.f;
+        }
+        phi += c[k] * (w[0] * w[1] * w[2]);
+        gr[0] += c[k] * (s[0] * w[1] * w[2]);
+        gr[1] += c[k] * (w[0] * s[1] * w[2]);
+        gr[2] += c[k] * (w[0] * w[1] * s[2]);
+    }
+    if (phi > 0.f) return make_float3(vx, vy, vz);
+    const float gn = sqrtf(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    if (!(gn > 0.f)) return make_float3(vx, vy, vz);  // flat level set: no normal
+    float n[3], rel[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        n[a] = gr[a] / gn;
+        rel[a] = vel[a] - sc.phi_vel[a];
+    }
+    const float vn = rel[0] * n[0] + rel[1] * n[1] + rel[2] * n[2];
+    if (vn >= kFltEps) return make_float3(vx, vy, vz);  // separating
+    float vt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vt[a] = rel[a] - vn * n[a];
+    const float vtn = sqrtf(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+    if (vtn <= -sc.phi_friction * vn + kFltEps) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) vel[a] = sc.phi_vel[a];
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) vel[a] = (vt[a] + sc.phi_friction * vn * (vt[a] / vtn)) + sc.phi_vel[a];
+    }
+    return make_float3(vel[0], vel[1], vel[2]);
+}
+__device__ __forceinline__ void levelSetCollision(const SceneDev& sc, const float* pos, float* vel) {
+    const float3 r = levelSetCollisionV(sc, pos[0], pos[1], pos[2], vel[0], vel[1], vel[2]);
+    vel[0] = r.x;
+    vel[1] = r.y;
+    vel[2] = r.z;
+}
+
 __device__ __forceinline__ float ldg(const float* p) { return __ldg(p); }
 
 // Asynchronous 4-byte global -> shared copies (cp.async, L1-allocating).
@@ -711,7 +782,7 @@ __device__ __forceinline__ int blockSlotAt(const StepArgs& args, const SceneDev&
 }
 
 template <int S, int MODE>
-__global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_transfer) {
+__global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int want_transfer) {
     constexpr int F = modeFields(MODE);
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
@@ -822,6 +893,12 @@ __global__ void __launch_bounds__(kThreads) gridKernel(StepArgs args, int want_t
 #pragma unroll
                 for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
                 boundaryCollision(pos, vs, sc.origin, sc.target, sc.friction);
+            }
+            if (sc.phi) {
+                float pos[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
+                levelSetCollision(sc, pos, vs);
             }
             sc.vstar[node] = make_float4(vs[0], vs[1], vs[2], m);
             if (MODE == MODE_FLIP) sc.vold[node] = make_float4(vo[0], vo[1], vo[2], 0.f);
@@ -1066,6 +1143,11 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
 #pragma unroll
             for (int a = 0; a < 3; ++a) pos[a] = x[a] + dt * vn[a];
             boundaryCollision(pos, vn, sc.origin, sc.target, sc.friction);
+            if (sc.phi) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) pos[a] = x[a] + dt * vn[a];
+                levelSetCollision(sc, pos, vn);
+            }
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) x[a] += dt * vn[a];  // advectParticles (:381-391)
@@ -1188,6 +1270,12 @@ __global__ void denseCollisionKernel(const SceneDev* __restrict__ scenes, float 
             for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
             boundaryCollision(pos, vs, sc.origin, sc.target, sc.friction);
         }
+        if (sc.phi) {
+            float pos[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) pos[a] = (sc.origin[a] + sc.h * (float)n[a]) + dt * vs[a];
+            levelSetCollision(sc, pos, vs);
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) sc.dbg[(7 + a) * nodes + i] = vs[a];
     }
@@ -1216,6 +1304,11 @@ __global__ void particlesCollisionKernel(const SceneDev* __restrict__ scenes, in
             x[a] = f[(F_X + a) * cap + i] + dt * v[a];
         }
         boundaryCollision(x, v, sc.origin, sc.target, sc.friction);
+        if (sc.phi) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) x[a] = f[(F_X + a) * cap + i] + dt * v[a];
+            levelSetCollision(sc, x, v);
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) f[(F_V + a) * cap + i] = v[a];
     }

@@ -306,6 +306,17 @@ class _SolverBase:
     def download_wait(self):
         check(self._lib.mpm_solver_download_wait(self._h), "download_wait")
 
+    def set_collision_object(self, obj=None):
+        """Level-set collision object (mpm_b200.level_set.LevelSetCollisionObject3D)
+        applied in every grid collision; None removes it."""
+        if obj is None:
+            check(self._lib.mpm_solver_set_level_set(self._h, None, 0.0, None), "set_level_set")
+            return
+        phi, vel = obj.arrays(self._res)
+        F = C.POINTER(C.c_float)
+        check(self._lib.mpm_solver_set_level_set(self._h, phi.ctypes.data_as(F), float(obj.friction),
+                                                 vel.ctypes.data_as(F)), "set_level_set")
+
     def profile(self, enable: bool = True):
         check(self._lib.mpm_solver_profile(self._h, 1 if enable else 0), "profile")
 

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -249,6 +250,58 @@ Vec3<R> applyBoundaryCollision(const Vec3<R>& position, const Vec3<R>& velocity,
         updated = rel;
     }
     return updated;
+}
+
+// Level-set collision object: trilinear signed distance and gradient at
+// pos (clamped to the grid); where the distance is <= 0 the friction law of
+// applyBoundaryCollision (src/collision_object3d.cu:38-51) acts on the
+// velocity relative to the object's surface velocity, normal = normalised
+// gradient.  The reference declares LevelSetCollisionObject3D
+// (include/collision_object3d.h:9-12) but never applies it.
+template <class R>
+Vec3<R> applyLevelSetCollision(const Vec3<R>& pos, const Vec3<R>& vel, const R* phi, const int res[3],
+                               const Vec3<R>& origin, R h, R friction, const Vec3<R>& vco) {
+    const R eps = (R)kFltEps;
+    int i0[3];
+    R f[3];
+    const R inv_h = (R)1 / h;
+    for (int a = 0; a < 3; ++a) {
+        R g = (pos[a] - origin[a]) * inv_h;
+        g = std::min(std::max(g, (R)0), (R)(res[a] - 1));
+        i0[a] = std::min((int)g, res[a] - 2);
+        f[a] = g - (R)i0[a];
+    }
+    const size_t X = (size_t)res[0], XY = X * (size_t)res[1];
+    R val = 0, gr[3] = {0, 0, 0};
+    for (int k = 0; k < 8; ++k) {
+        const int d[3] = {k & 1, (k >> 1) & 1, (k >> 2) & 1};
+        const R c = phi[(size_t)(i0[0] + d[0]) + X * (size_t)(i0[1] + d[1]) + XY * (size_t)(i0[2] + d[2])];
+        R w[3], sg[3];
+        for (int a = 0; a < 3; ++a) {
+            w[a] = d[a] ? f[a] : (R)1 - f[a];
+            sg[a] = d[a] ? (R)1 : (R)-1;
+        }
+        val += c * (w[0] * w[1] * w[2]);
+        gr[0] += c * (sg[0] * w[1] * w[2]);
+        gr[1] += c * (w[0] * sg[1] * w[2]);
+        gr[2] += c * (w[0] * w[1] * sg[2]);
+    }
+    if (val > 0) return vel;
+    const R gn = std::sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    if (!(gn > 0)) return vel;
+    Vec3<R> n, rel, out;
+    for (int a = 0; a < 3; ++a) {
+        n[a] = gr[a] / gn;
+        rel[a] = vel[a] - vco[a];
+    }
+    const R vn = rel[0] * n[0] + rel[1] * n[1] + rel[2] * n[2];
+    if (vn >= eps) return vel;
+    Vec3<R> vt;
+    for (int a = 0; a < 3; ++a) vt[a] = rel[a] - vn * n[a];
+    const R vtn = std::sqrt(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+    if (vtn <= -friction * vn + eps) return vco;
+    for (int a = 0; a < 3; ++a) out[a] = (vt[a] + friction * vn * (vt[a] / vtn)) + vco[a];
+    return out;
 }
 
 template Vec3<float> applyBoundaryCollision(const Vec3<float>&, const Vec3<float>&, const Vec3<float>&,
@@ -553,11 +606,17 @@ void Solver<R>::gridCollision(R dt) {
                     bool wall = false;
                     for (int a = 0; a < 3; ++a) wall |= (idx[a] < t) || (idx[a] >= res[a] - t);
                     if (wall) n.velocity_star = Vec3<R>{};
-                    continue;
+                } else {
+                    Vec3<R> pos;
+                    for (int a = 0; a < 3; ++a) pos[a] = (origin[a] + h * (R)idx[a]) + dt * n.velocity_star[a];
+                    n.velocity_star = applyBoundaryCollision(pos, n.velocity_star, origin, target, fr);
                 }
-                Vec3<R> pos;
-                for (int a = 0; a < 3; ++a) pos[a] = (origin[a] + h * (R)idx[a]) + dt * n.velocity_star[a];
-                n.velocity_star = applyBoundaryCollision(pos, n.velocity_star, origin, target, fr);
+                if (has_phi) {
+                    Vec3<R> pos;
+                    for (int a = 0; a < 3; ++a) pos[a] = (origin[a] + h * (R)idx[a]) + dt * n.velocity_star[a];
+                    n.velocity_star = applyLevelSetCollision(pos, n.velocity_star, phi.data(), res, origin, h,
+                                                             phi_friction, phi_vel);
+                }
             }
 }
 
@@ -610,6 +669,10 @@ void Solver<R>::particlesCollision(R dt) {
         Vec3<R> pos;
         for (int a = 0; a < 3; ++a) pos[a] = p.x[a] + dt * p.v[a];
         p.v = applyBoundaryCollision(pos, p.v, origin, target, fr);
+        if (has_phi) {
+            for (int a = 0; a < 3; ++a) pos[a] = p.x[a] + dt * p.v[a];
+            p.v = applyLevelSetCollision(pos, p.v, phi.data(), res, origin, h, phi_friction, phi_vel);
+        }
     }
 }
 
@@ -859,6 +922,51 @@ void orc_collision(int bits, const double* pos, const double* vel, const double*
         Vec3<double> r = applyBoundaryCollision<double>(p, v, a, b, friction);
         for (int i = 0; i < 3; ++i) out[i] = r[i];
     }
+}
+
+int orc_set_level_set(void* p, const double* phi, double friction, const double* vel) {
+    Handle* h = (Handle*)p;
+    auto set = [&](auto* s) {
+        using RR = typename std::remove_pointer<decltype(s)>::type::Real;
+        s->has_phi = phi != nullptr;
+        s->phi.clear();
+        if (!phi) return;
+        const size_t nodes = (size_t)s->res[0] * s->res[1] * s->res[2];
+        s->phi.resize(nodes);
+        for (size_t i = 0; i < nodes; ++i) s->phi[i] = (RR)phi[i];
+        s->phi_friction = (RR)friction;
+        for (int a = 0; a < 3; ++a) s->phi_vel[a] = vel ? (RR)vel[a] : (RR)0;
+    };
+    for (int a = 0; a < 3; ++a)
+        if (phi && (h->f ? h->f->res[a] : h->d->res[a]) < 2) {
+            g_err = "a level set needs >= 2 nodes per axis";
+            return 1;
+        }
+    if (h->f) set(h->f);
+    else set(h->d);
+    return 0;
+}
+
+// One level-set collision (known-answer tests).
+void orc_level_set_collision(int bits, const int* res, const double* origin, double h, const double* phi,
+                             double friction, const double* vco, const double* pos, const double* vel, double* out) {
+    auto run = [&](auto tag) {
+        using RR = decltype(tag);
+        const size_t nodes = (size_t)res[0] * res[1] * res[2];
+        std::vector<RR> ph(nodes);
+        for (size_t i = 0; i < nodes; ++i) ph[i] = (RR)phi[i];
+        Vec3<RR> o, vc, p, v;
+        for (int a = 0; a < 3; ++a) {
+            o[a] = (RR)origin[a];
+            vc[a] = (RR)vco[a];
+            p[a] = (RR)pos[a];
+            v[a] = (RR)vel[a];
+        }
+        Vec3<RR> r = applyLevelSetCollision<RR>(p, v, ph.data(), res, o, (RR)h, (RR)friction, vc);
+        for (int a = 0; a < 3; ++a) out[a] = (double)r[a];
+    };
+    if (bits == 32) run(0.0f);
+    else run(0.0);
 }
 
 // Stress of one particle state (V0 * P F^T as volumeTimesCauchyStress returns).

@@ -234,6 +234,7 @@ struct Node {
 template <class R>
 class Solver {
 public:
+    using Real = R;
     Solver(const mpm_scene_desc& d, const mpm_particles_in& in);
 
     void initialize();                 // src/mpm_solver3d.cu:131-223
@@ -256,6 +257,12 @@ public:
     R h;
     int res[3];
     R Dinv = 0;  // APIC: (k h^2)^-1, src/apic_mpm_solver3d.cu:151-157
+    // Level-set collision object (include/collision_object3d.h:9-12): signed
+    // distance per node, negative inside; applied after the grid boundary.
+    bool has_phi = false;
+    std::vector<R> phi;
+    R phi_friction = 0;
+    Vec3<R> phi_vel{};
 
 private:
     void stencilRange(const Vec3<R>& x, int lo[3], int hi[3]) const;

@@ -53,6 +53,8 @@ def load():
         "orc_spline": (None, [C.c_int, C.c_int, D, C.c_int, D, D]),
         "orc_svd3": (None, [C.c_int, D, D, D, D]),
         "orc_collision": (None, [C.c_int, D, D, D, D, C.c_double, D]),
+        "orc_set_level_set": (C.c_int, [P, D, C.c_double, D]),
+        "orc_level_set_collision": (None, [C.c_int, C.POINTER(C.c_int), D, C.c_double, D, C.c_double, D, D, D, D]),
         "orc_stress": (None, [C.c_int, C.c_int, D, D, C.c_double, C.c_double, C.c_double, C.c_double, D, D]),
         "orc_update_deformation": (None, [C.c_int, D, D, D, C.c_double, C.c_double, C.c_double]),
         "orc_last_error": (C.c_char_p, []),
@@ -107,6 +109,17 @@ class OracleSolver:
 
     def set_particles_collision(self, on: bool):
         self.lib.orc_set_particles_collision(self.h, 1 if on else 0)
+
+    def set_level_set(self, phi=None, friction: float = 0.0, velocity=(0.0, 0.0, 0.0)):
+        """Level-set collision object (signed distance per grid node), None removes it."""
+        if phi is None:
+            self.lib.orc_set_level_set(self.h, None, 0.0, None)
+            return
+        phi = np.ascontiguousarray(phi, np.float64).reshape(-1)
+        assert phi.size == self.res[0] * self.res[1] * self.res[2]
+        vel = np.ascontiguousarray(velocity, np.float64).reshape(3)
+        if self.lib.orc_set_level_set(self.h, _dp(phi), float(friction), _dp(vel)):
+            raise ValueError(self.lib.orc_last_error().decode())
 
     def step(self, n=1):
         self.lib.orc_step(self.h, int(n))
@@ -182,6 +195,16 @@ def collision(bits, pos, vel, lo, hi, friction):
     a = [np.ascontiguousarray(v, np.float64) for v in (pos, vel, lo, hi)]
     out = np.empty(3)
     lib.orc_collision(bits, *[_dp(v) for v in a], float(friction), _dp(out))
+    return out
+
+
+def level_set_collision(bits, res, origin, h, phi, friction, vco, pos, vel):
+    lib = load()
+    r = (C.c_int * 3)(*[int(v) for v in res])
+    a = [np.ascontiguousarray(v, np.float64).reshape(-1) for v in (origin, phi, vco, pos, vel)]
+    out = np.empty(3)
+    lib.orc_level_set_collision(bits, r, _dp(a[0]), float(h), _dp(a[1]), float(friction), _dp(a[2]), _dp(a[3]),
+                                _dp(a[4]), _dp(out))
     return out
 
 

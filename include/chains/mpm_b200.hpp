@@ -125,6 +125,13 @@ public:
             throw std::runtime_error("setCollisionObject: level set size does not match the grid");
         check(mpm_solver_set_level_set(h_, obj.level_set.data(), obj.friction, v), "setCollisionObject");
     }
+    // CFL time step (mpm_solver_set_cfl) and the simulated time.
+    void setCfl(float cfl) { check(mpm_solver_set_cfl(h_, cfl), "setCfl"); }
+    double simulatedTime() {
+        double t = 0.0;
+        check(mpm_solver_time(h_, &t, nullptr), "simulatedTime");
+        return t;
+    }
     void clearCollisionObject() { check(mpm_solver_set_level_set(h_, nullptr, 0.f, nullptr), "clearCollisionObject"); }
     std::vector<float> download(int field, int comps) {
         std::vector<float> out((size_t)comps * numParticles());

@@ -244,6 +244,17 @@ MPM_API mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32
  * = at rest) is the surface velocity; friction >= 0.  The values are copied. */
 MPM_API mpm_status mpm_solver_set_level_set(mpm_solver* s, const float* phi, float friction, const float* velocity);
 
+/* CFL time step (listed as unimplemented in the reference, README.md:60-67).
+ * cfl > 0: every mpm_solver_step step takes dt = min(desc.dt, cfl * stride /
+ * max_p |v_p|), from the particle velocities the step starts with, computed
+ * on the device (no host round trip); cfl = 0 returns to the fixed desc.dt.
+ * The sub-step functions keep the dt they are given. */
+MPM_API mpm_status mpm_solver_set_cfl(mpm_solver* s, float cfl);
+/* Simulated time advanced by mpm_solver_step since creation (carried by
+ * checkpoints) and the dt of the last step; either pointer may be NULL.
+ * Waits for the queued steps. */
+MPM_API mpm_status mpm_solver_time(mpm_solver* s, double* time, float* last_dt);
+
 MPM_API mpm_status mpm_solver_num_particles(const mpm_solver* s, size_t* n);
 MPM_API mpm_status mpm_solver_get_desc(const mpm_solver* s, mpm_scene_desc* desc);
 

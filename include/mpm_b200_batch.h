@@ -42,6 +42,10 @@ MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int3
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 /* Density grid of one scene (see mpm_solver_download_density). */
 MPM_API mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out);
+/* CFL time step and simulated time of one scene (see mpm_solver_set_cfl,
+ * mpm_solver_time). */
+MPM_API mpm_status mpm_batch_set_cfl(mpm_batch* b, int32_t scene_id, float cfl);
+MPM_API mpm_status mpm_batch_time(mpm_batch* b, int32_t scene_id, double* time, float* last_dt);
 /* Level-set collision object of one scene (see mpm_solver_set_level_set). */
 MPM_API mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* phi, float friction,
                                            const float* velocity);

@@ -116,6 +116,16 @@ class Batch:
               "mpm_batch_download_density")
         return out.reshape(res[2], res[1], res[0])
 
+    def set_cfl(self, sid: int, cfl: float):
+        """CFL time step of one scene (see MPMSolver3D.set_cfl)."""
+        check(self._lib.mpm_batch_set_cfl(self._h, int(sid), float(cfl)), "mpm_batch_set_cfl")
+
+    def time(self, sid: int) -> tuple:
+        """(simulated time, dt of the last step) of one scene."""
+        t, dt = C.c_double(), C.c_float()
+        check(self._lib.mpm_batch_time(self._h, int(sid), C.byref(t), C.byref(dt)), "mpm_batch_time")
+        return t.value, dt.value
+
     def set_collision_object(self, sid: int, obj=None):
         """Level-set collision object of one scene (see MPMSolver3D.set_collision_object)."""
         F = C.POINTER(C.c_float)

@@ -173,6 +173,13 @@ struct SceneHost {
     DevMem phi;                         // level-set collision object (nodes floats), if set
     bool has_phi = false;
     float phi_friction = 0.f, phi_vel[3] = {0.f, 0.f, 0.f};
+    // simulated time: steps at the fixed dt are counted here, CFL steps on the
+    // device (CflState); last_cfl tells which holds the last step's dt
+    float cfl = 0.f;
+    DevMem cfl_state;
+    double time_fixed = 0.0;
+    float last_dt = 0.f;
+    bool last_cfl = false;
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
     ~SceneHost() {
         for (int k = 0; k < 2; ++k) {
@@ -289,6 +296,8 @@ public:
             MPM_TRY(sc->buf_mat[b].allocPooled(sizeof(uint16_t) * cap, "particle materials", pool, stream_));
         }
         const size_t nodes = sc->nodes();
+        MPM_TRY(sc->cfl_state.alloc(sizeof(CflState), "CFL state"));
+        CUDA_TRY(cudaMemsetAsync(sc->cfl_state.p, 0, sizeof(CflState), stream_));
         MPM_TRY(sc->vstar.allocPooled(sizeof(float4) * nodes, "grid v*", pool, stream_));
         CUDA_TRY(cudaMemsetAsync(sc->vstar.p, 0, sizeof(float4) * nodes, stream_));
         if (d.transfer == MPM_TRANSFER_PIC_FLIP) {
@@ -370,10 +379,10 @@ public:
     // particle order the 41 float planes (n floats each), the original
     // particle ids (u32 x n) and the material ids (u16 x n); version 2 adds
     // u32 has_level_set and, if set, f32 friction, f32 velocity[3] and the
-    // level set (f32 per grid node).  Restoring that order and the cached
-    // stress makes the continuation bitwise identical.  Version 1 files
-    // (no level-set section) are still read.
-    static constexpr uint32_t kCkptVersion = 2;
+    // level set (f32 per grid node); version 3 adds f32 cfl, f64 simulated
+    // time and f32 last dt.  Restoring that order and the cached stress makes
+    // the continuation bitwise identical.  Older versions are still read.
+    static constexpr uint32_t kCkptVersion = 3;
 
     mpm_status saveScene(int id, const char* path) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -400,6 +409,9 @@ public:
             CUDA_TRY(cudaMemcpy(phi.data(), s.phi.p, sizeof(float) * phi.size(), cudaMemcpyDeviceToHost));
         }
         const uint32_t has_phi = s.has_phi ? 1u : 0u;
+        double sim_t = 0.0;
+        float last_dt = 0.f;
+        MPM_TRY(simTime(id, &sim_t, &last_dt));
         std::FILE* fp = std::fopen(path, "wb");
         if (!fp) return fail(MPM_ERR_IO, std::string("cannot open ") + path + " for writing");
         const char magic[8] = {'M', 'P', 'M', 'B', '2', '0', '0', 0};
@@ -418,6 +430,8 @@ public:
         if (ok && has_phi)
             ok = std::fwrite(&s.phi_friction, 4, 1, fp) == 1 && std::fwrite(s.phi_vel, 4, 3, fp) == 3 &&
                  std::fwrite(phi.data(), sizeof(float), phi.size(), fp) == phi.size();
+        ok = ok && std::fwrite(&s.cfl, 4, 1, fp) == 1 && std::fwrite(&sim_t, 8, 1, fp) == 1 &&
+             std::fwrite(&last_dt, 4, 1, fp) == 1;
         ok = (std::fclose(fp) == 0) && ok;
         if (!ok) return fail(MPM_ERR_IO, std::string("write failed: ") + path);
         return MPM_OK;
@@ -435,6 +449,8 @@ public:
         bool has_phi = false;
         float phi_friction = 0.f, phi_vel[3] = {0.f, 0.f, 0.f};
         std::vector<float> phi;
+        float cfl = 0.f, last_dt = 0.f;
+        double time = 0.0;
     };
     static mpm_status readCheckpoint(const char* path, Checkpoint* ck) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -491,6 +507,11 @@ public:
                 ck->has_phi = true;
             }
         }
+        if (ver >= 3) {
+            if (std::fread(&ck->cfl, 4, 1, fp) != 1 || std::fread(&ck->time, 8, 1, fp) != 1 ||
+                std::fread(&ck->last_dt, 4, 1, fp) != 1 || !(ck->cfl >= 0.f) || !std::isfinite(ck->cfl))
+                return fail(MPM_ERR_PARSE, std::string(path) + ": truncated or corrupt time section");
+        }
         std::vector<uint8_t> seen(n, 0);
         for (size_t i = 0; i < n; ++i) {
             if (ck->pid[i] >= n || seen[ck->pid[i]]) return fail(MPM_ERR_PARSE, std::string(path) + ": bad particle ids");
@@ -517,6 +538,9 @@ public:
         CUDA_TRY(cudaStreamSynchronize(stream_));
         sc->need_init = false;  // V0 is part of the state
         sc->stress_stale = (ck.flags & 1u) != 0;
+        sc->time_fixed = ck.time;
+        sc->last_dt = ck.last_dt;
+        sc->cfl = ck.cfl;
         *out_id = registerScene(std::move(sc));
         if (ck.has_phi) {
             mpm_status st = setLevelSet(*out_id, ck.phi.data(), ck.phi_friction, ck.phi_vel);
@@ -614,10 +638,15 @@ public:
             d.phi = s.has_phi ? s.phi.as<float>() : nullptr;
             d.phi_friction = s.phi_friction;
             for (int a = 0; a < 3; ++a) d.phi_vel[a] = s.phi_vel[a];
+            d.cfl = s.cfl;
+            d.dt_max = s.desc.dt;
+            d.cfl_state = s.cfl_state.as<CflState>();
             max_nodes_ = std::max(max_nodes_, s.nodes());
             max_n_ = std::max(max_n_, s.n);
         }
         sbb[ns] = (uint32_t)tb;
+        any_cfl_ = false;
+        for (auto& s : scenes_) any_cfl_ |= s->cfl > 0.f;
         if (tb * 64 > 0xffffffffull) return fail(MPM_ERR_UNSUPPORTED, "batch grid too large for 32-bit cell keys");
         if (ntot > 0x7fffffffull) return fail(MPM_ERR_UNSUPPORTED, "batch has too many particles");
         ntot_ = ntot;
@@ -940,6 +969,7 @@ public:
             CUDA_TRY(cudaMemsetAsync(counters_.as<uint32_t>() + 2, 0, sizeof(uint32_t), stream_));
         }
         MPM_TRY(refreshStress());
+        if (any_cfl_) launchCfl(ctx(), parity_, max_n_);
         graph_sorted_[parity_][kcur_] = sorted_;
         const int next = 1 - sorted_;
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
@@ -1019,7 +1049,53 @@ public:
         for (int i = 0; i < n; ++i) {
             MPM_TRY(stepOnce());
             MPM_TRY(checkP2GStage());
+            advanceClock();
         }
+        return MPM_OK;
+    }
+
+    void advanceClock() {
+        for (auto& s : scenes_) {
+            s->last_cfl = s->cfl > 0.f;
+            if (!s->last_cfl) {
+                s->time_fixed += (double)s->desc.dt;
+                s->last_dt = s->desc.dt;
+            }
+        }
+    }
+
+    // CFL time step of a scene: cfl > 0 makes every step's dt
+    // min(desc.dt, cfl h / max_p |v_p|) from the velocities the step starts
+    // with; 0 returns to the fixed desc.dt.
+    mpm_status setCfl(int id, float cfl) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!(cfl >= 0.f) || !std::isfinite(cfl)) return fail(MPM_ERR_INVALID_ARG, "cfl must be finite and >= 0");
+        scenes_[idx]->cfl = cfl;
+        if (!dirty_) {
+            host_scenes_[idx].cfl = cfl;
+            MPM_TRY(uploadSceneTable());
+        }
+        bool any = false;
+        for (auto& s : scenes_) any |= s->cfl > 0.f;
+        if (any != any_cfl_) {  // the step's launch sequence changes
+            CUDA_TRY(cudaStreamSynchronize(stream_));
+            any_cfl_ = any;
+            dropGraphs();
+        }
+        return MPM_OK;
+    }
+
+    // Simulated time advanced by step() and the dt of the last step.
+    mpm_status simTime(int id, double* t, float* last_dt) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        SceneHost& s = *scenes_[idx];
+        CflState st{};
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        CUDA_TRY(cudaMemcpy(&st, s.cfl_state.p, sizeof(CflState), cudaMemcpyDeviceToHost));
+        if (t) *t = s.time_fixed + st.time;
+        if (last_dt) *last_dt = s.last_cfl ? st.last_dt : s.last_dt;
         return MPM_OK;
     }
 
@@ -1030,6 +1106,7 @@ public:
         for (int i = 0; i < n; ++i) {
             MPM_TRY(stepOnce());
             MPM_TRY(checkP2GStage());
+            advanceClock();
         }
         CUDA_TRY(cudaEventRecord(ev_[0][1], stream_));
         CUDA_TRY(cudaEventSynchronize(ev_[0][1]));
@@ -1431,6 +1508,7 @@ private:
     std::vector<SceneDev> host_scenes_;
     int next_id_ = 0;
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
+    bool any_cfl_ = false;     // some scene steps with a CFL dt (two more launches per step)
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order
@@ -1657,6 +1735,14 @@ mpm_status mpm_solver_set_level_set(mpm_solver* s, const float* phi, float frict
     MPM_TRY(check(s));
     return s->eng.setLevelSet(s->scene, phi, friction, velocity);
 }
+mpm_status mpm_solver_set_cfl(mpm_solver* s, float cfl) {
+    MPM_TRY(check(s));
+    return s->eng.setCfl(s->scene, cfl);
+}
+mpm_status mpm_solver_time(mpm_solver* s, double* time, float* last_dt) {
+    MPM_TRY(check(s));
+    return s->eng.simTime(s->scene, time, last_dt);
+}
 mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32_t* enable) {
     MPM_TRY(check(s));
     if (!enable) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -1861,6 +1947,14 @@ mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* 
                                    const float* velocity) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.setLevelSet(scene_id, phi, friction, velocity);
+}
+mpm_status mpm_batch_set_cfl(mpm_batch* b, int32_t scene_id, float cfl) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.setCfl(scene_id, cfl);
+}
+mpm_status mpm_batch_time(mpm_batch* b, int32_t scene_id, double* time, float* last_dt) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.simTime(scene_id, time, last_dt);
 }
 mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n) {
     if (!b || !n) return mpm::fail(MPM_ERR_INVALID_ARG, "null argument");

@@ -57,6 +57,15 @@ struct MaterialDev {
     int model;
 };
 
+// Per-scene CFL state in device memory: the running max of |v|^2 as float
+// bits (non-negative floats order like their bit patterns), the dt of the
+// last step and the simulated time it advanced.
+struct CflState {
+    uint32_t vmax2_bits;
+    float last_dt;
+    double time;
+};
+
 struct SceneDev {
     float origin[3];
     float h, inv_h, range;
@@ -82,6 +91,10 @@ struct SceneDev {
     const float* phi;
     float phi_friction;
     float phi_vel[3];      // velocity of the collider's surface
+    // CFL time step: cfl > 0 makes each step's dt = min(dt_max, cfl h / max|v_p|),
+    // written into dt by cflFinalizeKernel before the step's kernels run.
+    float cfl, dt_max;
+    CflState* cfl_state;
 };
 
 struct BlockItem {

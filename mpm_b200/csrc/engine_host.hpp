@@ -74,6 +74,9 @@ void launchVolume(const LaunchCtx& c, int parity, int S);
 void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, size_t cap, const float* staged, size_t n,
                      bool has_volume);
 void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out);
+// CFL time step of the scenes with cfl > 0: max |v|^2 over their live
+// particles, then dt = min(dt_max, cfl h / max|v|) into the scene table.
+void launchCfl(const LaunchCtx& c, int parity, size_t max_n);
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out);
 void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in);
 size_t p2gSmemBytes(int S, int mode);

@@ -1577,6 +1577,50 @@ __global__ void densityKernel(const float4* __restrict__ vstar, size_t nodes, fl
     for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < nodes; i += (size_t)gridDim.x * kThreads)
         out[i] = vstar[i].w * inv_cell_vol;
 }
+// CFL time step (listed as unimplemented in the reference, README.md:60-67).
+__global__ void __launch_bounds__(kThreads) cflMaxKernel(const SceneDev* __restrict__ scenes, int parity) {
+    const SceneDev& sc = scenes[blockIdx.y];
+    if (!(sc.cfl > 0.f)) return;
+    const float* f = sc.buf[parity].f;
+    const size_t cap = sc.cap;
+    float m = 0.f;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
+        const float vx = f[(F_V + 0) * cap + i], vy = f[(F_V + 1) * cap + i], vz = f[(F_V + 2) * cap + i];
+        m = fmaxf(m, __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wm[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kThreads / 32; ++w) m = fmaxf(m, wm[w]);
+        if (m > 0.f) atomicMax(&sc.cfl_state->vmax2_bits, __float_as_uint(m));
+    }
+}
+// One thread per scene: dt from the maximum, written into the (device) scene
+// table that the step's kernels read, then the maximum is cleared.
+__global__ void cflFinalizeKernel(SceneDev* __restrict__ scenes, int nscenes) {
+    for (int i = threadIdx.x; i < nscenes; i += blockDim.x) {
+        SceneDev& sc = scenes[i];
+        if (!(sc.cfl > 0.f)) continue;
+        CflState* st = sc.cfl_state;
+        const float vmax = sqrtf(__uint_as_float(st->vmax2_bits));
+        float dt = sc.dt_max;
+        if (vmax > 0.f) dt = fminf(dt, __fdiv_rn(__fmul_rn(sc.cfl, sc.h), vmax));
+        sc.dt = dt;
+        st->vmax2_bits = 0u;
+        st->last_dt = dt;
+        st->time += (double)dt;
+    }
+}
+void launchCfl(const LaunchCtx& c, int parity, size_t max_n) {
+    noteLaunches(2);
+    const unsigned bx = (unsigned)std::max<size_t>(
+        1, std::min<size_t>((max_n + kThreads - 1) / kThreads, (size_t)c.num_sms * 4));
+    cflMaxKernel<<<dim3(bx, (unsigned)c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity);
+    cflFinalizeKernel<<<1, 128, 0, c.stream>>>(const_cast<SceneDev*>(c.scenes), c.nscenes);
+}
 void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out) {
     noteLaunches(1);
     const unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((nodes + kThreads - 1) / kThreads,

@@ -306,6 +306,16 @@ class _SolverBase:
     def download_wait(self):
         check(self._lib.mpm_solver_download_wait(self._h), "download_wait")
 
+    def set_cfl(self, cfl: float):
+        """CFL time step: cfl > 0 makes each step's dt min(dt, cfl h / max|v_p|); 0 restores the fixed dt."""
+        check(self._lib.mpm_solver_set_cfl(self._h, float(cfl)), "set_cfl")
+
+    def time(self) -> tuple:
+        """(simulated time advanced by step(), dt of the last step)."""
+        t, dt = C.c_double(), C.c_float()
+        check(self._lib.mpm_solver_time(self._h, C.byref(t), C.byref(dt)), "time")
+        return t.value, dt.value
+
     def set_collision_object(self, obj=None):
         """Level-set collision object (mpm_b200.level_set.LevelSetCollisionObject3D)
         applied in every grid collision; None removes it."""

@@ -686,6 +686,14 @@ void Solver<R>::advectParticles(R dt) {
 template <class R>
 void Solver<R>::simulateOneStep() {
     R dt = (R)desc.dt;
+    if (cfl > 0) {  // CFL step from the velocities the step starts with
+        R m = 0;
+        for (const Particle<R>& p : particles) m = std::max(m, (p.v[0] * p.v[0] + p.v[1] * p.v[1]) + p.v[2] * p.v[2]);
+        const R vmax = std::sqrt(m);
+        if (vmax > 0) dt = std::min(dt, (cfl * h) / vmax);
+    }
+    last_dt = dt;
+    time += (double)dt;
     resetGrid();
     particlesToGrid();
     computeGravityForces();
@@ -922,6 +930,17 @@ void orc_collision(int bits, const double* pos, const double* vel, const double*
         Vec3<double> r = applyBoundaryCollision<double>(p, v, a, b, friction);
         for (int i = 0; i < 3; ++i) out[i] = r[i];
     }
+}
+
+void orc_set_cfl(void* p, double cfl) {
+    Handle* h = (Handle*)p;
+    if (h->f) h->f->cfl = (float)cfl;
+    else h->d->cfl = cfl;
+}
+void orc_time(void* p, double* t, double* last_dt) {
+    Handle* h = (Handle*)p;
+    *t = h->f ? h->f->time : h->d->time;
+    *last_dt = h->f ? (double)h->f->last_dt : h->d->last_dt;
 }
 
 int orc_set_level_set(void* p, const double* phi, double friction, const double* vel) {

@@ -259,6 +259,10 @@ public:
     R Dinv = 0;  // APIC: (k h^2)^-1, src/apic_mpm_solver3d.cu:151-157
     // Level-set collision object (include/collision_object3d.h:9-12): signed
     // distance per node, negative inside; applied after the grid boundary.
+    // CFL time step: cfl > 0 makes each step's dt min(desc.dt, cfl h / max|v_p|)
+    R cfl = 0;
+    double time = 0;
+    R last_dt = 0;
     bool has_phi = false;
     std::vector<R> phi;
     R phi_friction = 0;

@@ -54,6 +54,8 @@ def load():
         "orc_svd3": (None, [C.c_int, D, D, D, D]),
         "orc_collision": (None, [C.c_int, D, D, D, D, C.c_double, D]),
         "orc_set_level_set": (C.c_int, [P, D, C.c_double, D]),
+        "orc_set_cfl": (None, [P, C.c_double]),
+        "orc_time": (None, [P, D, D]),
         "orc_level_set_collision": (None, [C.c_int, C.POINTER(C.c_int), D, C.c_double, D, C.c_double, D, D, D, D]),
         "orc_stress": (None, [C.c_int, C.c_int, D, D, C.c_double, C.c_double, C.c_double, C.c_double, D, D]),
         "orc_update_deformation": (None, [C.c_int, D, D, D, C.c_double, C.c_double, C.c_double]),
@@ -120,6 +122,14 @@ class OracleSolver:
         vel = np.ascontiguousarray(velocity, np.float64).reshape(3)
         if self.lib.orc_set_level_set(self.h, _dp(phi), float(friction), _dp(vel)):
             raise ValueError(self.lib.orc_last_error().decode())
+
+    def set_cfl(self, cfl: float):
+        self.lib.orc_set_cfl(self.h, float(cfl))
+
+    def time(self) -> tuple:
+        t, dt = np.zeros(1), np.zeros(1)
+        self.lib.orc_time(self.h, _dp(t), _dp(dt))
+        return float(t[0]), float(dt[0])
 
     def step(self, n=1):
         self.lib.orc_step(self.h, int(n))

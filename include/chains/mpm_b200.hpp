@@ -125,6 +125,12 @@ public:
             throw std::runtime_error("setCollisionObject: level set size does not match the grid");
         check(mpm_solver_set_level_set(h_, obj.level_set.data(), obj.friction, v), "setCollisionObject");
     }
+    // IntegrationType (include/enums.h:17-21): EXPLICIT, SEMI_IMPLICIT (beta
+    // 1/2) or FULL_IMPLICIT (backward Euler, beta 1), see mpm_solver_set_implicit.
+    void setIntegrationType(IntegrationType t, int maxIterations = 50, float tolerance = 1e-5f) {
+        const float beta = t == IntegrationType::EXPLICIT ? 0.f : (t == IntegrationType::SEMI_IMPLICIT ? 0.5f : 1.f);
+        check(mpm_solver_set_implicit(h_, beta, maxIterations, tolerance), "setIntegrationType");
+    }
     // CFL time step (mpm_solver_set_cfl) and the simulated time.
     void setCfl(float cfl) { check(mpm_solver_set_cfl(h_, cfl), "setCfl"); }
     double simulatedTime() {

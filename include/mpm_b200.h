@@ -221,7 +221,7 @@ MPM_API mpm_status mpm_solver_compute_external_forces(mpm_solver* s);     /* :29
 MPM_API mpm_status mpm_solver_compute_gravity_forces(mpm_solver* s);      /* :394-403 */
 MPM_API mpm_status mpm_solver_update_grid_velocities(mpm_solver* s, float dt);   /* :300-310 */
 MPM_API mpm_status mpm_solver_grid_collision(mpm_solver* s, float dt);    /* :405-426 */
-MPM_API mpm_status mpm_solver_solve_linear_system(mpm_solver* s, float dt);      /* :312-314, no-op */
+MPM_API mpm_status mpm_solver_solve_linear_system(mpm_solver* s, float dt);      /* :312-314, see below */
 MPM_API mpm_status mpm_solver_grid_to_particles(mpm_solver* s, float dt, float blend); /* :316-379 */
 MPM_API mpm_status mpm_solver_particles_collision(mpm_solver* s, float dt);      /* :428-445 */
 MPM_API mpm_status mpm_solver_advect_particles(mpm_solver* s, float dt);  /* :381-391 */
@@ -243,6 +243,20 @@ MPM_API mpm_status mpm_solver_get_particles_collision(const mpm_solver* s, int32
  * with the normalised trilinear gradient as normal.  velocity (3 floats, NULL
  * = at rest) is the surface velocity; friction >= 0.  The values are copied. */
 MPM_API mpm_status mpm_solver_set_level_set(mpm_solver* s, const float* phi, float friction, const float* velocity);
+
+/* Semi-implicit update (IntegrationType SEMI_IMPLICIT / FULL_IMPLICIT,
+ * include/enums.h:17-21, and solveLinearSystem, src/mpm_solver3d.cu:312-314:
+ * declared, left empty by the reference).  beta > 0 makes every step solve
+ * (M + beta dt^2 H) v = M v* after the grid collision, H the Hessian of the
+ * elastic energy in the node positions (Stomakhin et al. 2013, section 9),
+ * by conjugate residual preconditioned with the node masses, to
+ * |r| <= tol |M v*| or max_iter iterations, then apply the grid collision to
+ * the solved velocities; beta = 1/2 is the semi-implicit, 1 the backward
+ * Euler update, 0 the explicit step.  mpm_solver_solve_linear_system then
+ * runs the same solve on the split-mode grid (no collision after). */
+MPM_API mpm_status mpm_solver_set_implicit(mpm_solver* s, float beta, int32_t max_iter, float tol);
+/* Iterations and final |r| / |M v*| of the last solve (waits for the queued work). */
+MPM_API mpm_status mpm_solver_solve_info(mpm_solver* s, int32_t* iterations, float* residual);
 
 /* CFL time step (listed as unimplemented in the reference, README.md:60-67).
  * cfl > 0: every mpm_solver_step step takes dt = min(desc.dt, cfl * stride /

@@ -42,6 +42,9 @@ MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int3
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 /* Density grid of one scene (see mpm_solver_download_density). */
 MPM_API mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out);
+/* Semi-implicit update of one scene (see mpm_solver_set_implicit). */
+MPM_API mpm_status mpm_batch_set_implicit(mpm_batch* b, int32_t scene_id, float beta, int32_t max_iter, float tol);
+MPM_API mpm_status mpm_batch_solve_info(mpm_batch* b, int32_t scene_id, int32_t* iterations, float* residual);
 /* CFL time step and simulated time of one scene (see mpm_solver_set_cfl,
  * mpm_solver_time). */
 MPM_API mpm_status mpm_batch_set_cfl(mpm_batch* b, int32_t scene_id, float cfl);

@@ -104,6 +104,8 @@ SIGNATURES = {
     "mpm_solver_download_density": (C.c_int, [_P, _F]),
     "mpm_solver_set_level_set": (C.c_int, [_P, _F, C.c_float, _F]),
     "mpm_solver_set_cfl": (C.c_int, [_P, C.c_float]),
+    "mpm_solver_set_implicit": (C.c_int, [_P, C.c_float, C.c_int32, C.c_float]),
+    "mpm_solver_solve_info": (C.c_int, [_P, C.POINTER(C.c_int32), _F]),
     "mpm_solver_time": (C.c_int, [_P, C.POINTER(C.c_double), _F]),
     "mpm_solver_download_grid": (C.c_int, [_P, C.c_int32, _F]),
     "mpm_solver_upload": (C.c_int, [_P, C.c_int32, _F]),
@@ -141,6 +143,8 @@ SIGNATURES = {
     "mpm_batch_download_density": (C.c_int, [_P, C.c_int32, _F]),
     "mpm_batch_set_level_set": (C.c_int, [_P, C.c_int32, _F, C.c_float, _F]),
     "mpm_batch_set_cfl": (C.c_int, [_P, C.c_int32, C.c_float]),
+    "mpm_batch_set_implicit": (C.c_int, [_P, C.c_int32, C.c_float, C.c_int32, C.c_float]),
+    "mpm_batch_solve_info": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), _F]),
     "mpm_batch_time": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_double), _F]),
     "mpm_batch_num_scenes": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "mpm_batch_scene_particles": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_size_t)]),

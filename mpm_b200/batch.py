@@ -116,6 +116,16 @@ class Batch:
               "mpm_batch_download_density")
         return out.reshape(res[2], res[1], res[0])
 
+    def set_implicit(self, sid: int, beta: float, max_iter: int = 50, tol: float = 1e-5):
+        """Semi-implicit update of one scene (see MPMSolver3D.set_implicit)."""
+        check(self._lib.mpm_batch_set_implicit(self._h, int(sid), float(beta), int(max_iter), float(tol)),
+              "mpm_batch_set_implicit")
+
+    def solve_info(self, sid: int) -> tuple:
+        it, res = C.c_int32(), C.c_float()
+        check(self._lib.mpm_batch_solve_info(self._h, int(sid), C.byref(it), C.byref(res)), "mpm_batch_solve_info")
+        return it.value, res.value
+
     def set_cfl(self, sid: int, cfl: float):
         """CFL time step of one scene (see MPMSolver3D.set_cfl)."""
         check(self._lib.mpm_batch_set_cfl(self._h, int(sid), float(cfl)), "mpm_batch_set_cfl")

@@ -180,6 +180,10 @@ struct SceneHost {
     double time_fixed = 0.0;
     float last_dt = 0.f;
     bool last_cfl = false;
+    // semi-implicit update (beta > 0) and its solver buffers (implicit.cu)
+    float beta = 0.f, solve_tol = 1e-5f;
+    int solve_max_iter = 50;
+    DevMem solve_m, solve_vec, solve_part, solve_status;
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
     ~SceneHost() {
         for (int k = 0; k < 2; ++k) {
@@ -380,9 +384,10 @@ public:
     // particle ids (u32 x n) and the material ids (u16 x n); version 2 adds
     // u32 has_level_set and, if set, f32 friction, f32 velocity[3] and the
     // level set (f32 per grid node); version 3 adds f32 cfl, f64 simulated
-    // time and f32 last dt.  Restoring that order and the cached stress makes
-    // the continuation bitwise identical.  Older versions are still read.
-    static constexpr uint32_t kCkptVersion = 3;
+    // time and f32 last dt; version 4 the semi-implicit settings f32 beta,
+    // i32 max_iter, f32 tol.  Restoring that order and the cached stress
+    // makes the continuation bitwise identical.  Older versions are still read.
+    static constexpr uint32_t kCkptVersion = 4;
 
     mpm_status saveScene(int id, const char* path) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -432,6 +437,8 @@ public:
                  std::fwrite(phi.data(), sizeof(float), phi.size(), fp) == phi.size();
         ok = ok && std::fwrite(&s.cfl, 4, 1, fp) == 1 && std::fwrite(&sim_t, 8, 1, fp) == 1 &&
              std::fwrite(&last_dt, 4, 1, fp) == 1;
+        ok = ok && std::fwrite(&s.beta, 4, 1, fp) == 1 && std::fwrite(&s.solve_max_iter, 4, 1, fp) == 1 &&
+             std::fwrite(&s.solve_tol, 4, 1, fp) == 1;
         ok = (std::fclose(fp) == 0) && ok;
         if (!ok) return fail(MPM_ERR_IO, std::string("write failed: ") + path);
         return MPM_OK;
@@ -451,6 +458,8 @@ public:
         std::vector<float> phi;
         float cfl = 0.f, last_dt = 0.f;
         double time = 0.0;
+        float beta = 0.f, tol = 1e-5f;
+        int32_t max_iter = 50;
     };
     static mpm_status readCheckpoint(const char* path, Checkpoint* ck) {
         if (!path) return fail(MPM_ERR_INVALID_ARG, "null path");
@@ -512,6 +521,11 @@ public:
                 std::fread(&ck->last_dt, 4, 1, fp) != 1 || !(ck->cfl >= 0.f) || !std::isfinite(ck->cfl))
                 return fail(MPM_ERR_PARSE, std::string(path) + ": truncated or corrupt time section");
         }
+        if (ver >= 4) {
+            if (std::fread(&ck->beta, 4, 1, fp) != 1 || std::fread(&ck->max_iter, 4, 1, fp) != 1 ||
+                std::fread(&ck->tol, 4, 1, fp) != 1)
+                return fail(MPM_ERR_PARSE, std::string(path) + ": truncated solver section");
+        }
         std::vector<uint8_t> seen(n, 0);
         for (size_t i = 0; i < n; ++i) {
             if (ck->pid[i] >= n || seen[ck->pid[i]]) return fail(MPM_ERR_PARSE, std::string(path) + ": bad particle ids");
@@ -544,6 +558,13 @@ public:
         *out_id = registerScene(std::move(sc));
         if (ck.has_phi) {
             mpm_status st = setLevelSet(*out_id, ck.phi.data(), ck.phi_friction, ck.phi_vel);
+            if (st != MPM_OK) {
+                removeScene(*out_id);
+                return st;
+            }
+        }
+        if (ck.beta > 0.f) {
+            mpm_status st = setImplicit(*out_id, ck.beta, ck.max_iter, ck.tol);
             if (st != MPM_OK) {
                 removeScene(*out_id);
                 return st;
@@ -641,6 +662,7 @@ public:
             d.cfl = s.cfl;
             d.dt_max = s.desc.dt;
             d.cfl_state = s.cfl_state.as<CflState>();
+            solveFields(s, d);
             max_nodes_ = std::max(max_nodes_, s.nodes());
             max_n_ = std::max(max_n_, s.n);
         }
@@ -691,6 +713,100 @@ public:
         sorted_valid_ = false;
         incremental_ok_ = false;
         stage_check_ = true;
+        any_implicit_ = false;
+        for (auto& s : scenes_) any_implicit_ |= s->beta > 0.f;
+        MPM_TRY(ensureSolveBuffers());
+        return MPM_OK;
+    }
+
+    // ---- semi-implicit update ---------------------------------------------
+    static void solveFields(const SceneHost& s, SceneDev& d) {
+        d.beta = s.beta;
+        d.solve_tol = s.solve_tol;
+        d.solve_max_iter = s.solve_max_iter;
+        d.solve = SolveDev{s.solve_m.as<float>(), s.solve_vec.as<float4>(), s.solve_part.as<double>(),
+                           s.solve_status.as<SolveStatus>()};
+    }
+    // Batch-wide buffers over the sorted particles and the cell keys.
+    mpm_status ensureSolveBuffers() {
+        if (!any_implicit_ || dirty_) return MPM_OK;
+        const size_t n = std::max<size_t>(ntot_, 1);
+        MPM_TRY(cell_range_.grow(sizeof(uint2) * (size_t)total_blocks_ * 64, "solver cell ranges"));
+        MPM_TRY(solve_px_.grow(sizeof(float4) * n, "solver particle positions"));
+        MPM_TRY(solve_prep_.grow(sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
+        MPM_TRY(solve_T_.grow(sizeof(float4) * 3 * n, "solver particle stress differentials"));
+        return MPM_OK;
+    }
+    // beta > 0: every step solves (M + beta dt^2 H) v = M v* after the grid
+    // collision (beta 1/2: Crank-Nicolson-like, 1: backward Euler), to
+    // |r| <= tol |M v*| or max_iter iterations; beta = 0: explicit.
+    mpm_status setImplicit(int id, float beta, int max_iter, float tol) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        if (!(beta >= 0.f) || !std::isfinite(beta)) return fail(MPM_ERR_INVALID_ARG, "beta must be finite and >= 0");
+        if (max_iter < 1 || max_iter > 10000) return fail(MPM_ERR_INVALID_ARG, "max_iter must be in [1, 10000]");
+        if (!(tol >= 0.f) || !std::isfinite(tol)) return fail(MPM_ERR_INVALID_ARG, "tol must be finite and >= 0");
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        SceneHost& s = *scenes_[idx];
+        if (beta > 0.f) {
+            const size_t nodes = s.nodes();
+            MPM_TRY(s.solve_m.grow(sizeof(float) * nodes, "solver node masses"));
+            MPM_TRY(s.solve_vec.grow(sizeof(float4) * 6 * nodes, "solver node vectors"));
+            MPM_TRY(s.solve_part.grow(sizeof(double) * solvePartialDoubles(max_iter), "solver partial sums"));
+            MPM_TRY(s.solve_status.grow(sizeof(SolveStatus), "solver status"));
+            CUDA_TRY(cudaMemset(s.solve_status.p, 0, sizeof(SolveStatus)));
+        }
+        s.beta = beta;
+        s.solve_max_iter = max_iter;
+        s.solve_tol = tol;
+        dropGraphs();  // the launch sequence depends on the solver settings
+        any_implicit_ = false;
+        for (auto& sc : scenes_) any_implicit_ |= sc->beta > 0.f;
+        if (!dirty_) {
+            solveFields(s, host_scenes_[idx]);
+            MPM_TRY(ensureSolveBuffers());
+            MPM_TRY(uploadSceneTable());
+        }
+        return MPM_OK;
+    }
+    mpm_status solveInfo(int id, int* iters, float* residual) {
+        int idx = sceneIndex(id);
+        if (idx < 0) return fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        SolveStatus st{};
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        if (scenes_[idx]->solve_status.p)
+            CUDA_TRY(cudaMemcpy(&st, scenes_[idx]->solve_status.p, sizeof(SolveStatus), cudaMemcpyDeviceToHost));
+        if (iters) *iters = st.iters;
+        if (residual) *residual = st.residual;
+        return MPM_OK;
+    }
+    int maxSolveIters() const {
+        int m = 0;
+        for (auto& s : scenes_)
+            if (s->beta > 0.f) m = std::max(m, s->solve_max_iter);
+        return m;
+    }
+    void launchSolveAll(bool split) {
+        SolveBuffers b{keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), cell_range_.as<uint2>(),
+                       (size_t)total_blocks_ * 64, solve_px_.as<float4>(), solve_prep_.as<float>(),
+                       solve_T_.as<float4>(), (uint32_t)ntot_};
+        const std::vector<int> S = stencilSizes();
+        launchSolve(ctx(), b, parity_, S.data(), (int)S.size(), maxSolveIters(), split);
+    }
+    // Split API: solveLinearSystem(dt) on the split-mode grid (v* of
+    // updateGridVelocities / gridCollision), no collision after.
+    mpm_status solveLinearSystem(float dt) {
+        MPM_TRY(ensureReady());
+        if (!any_implicit_) return MPM_OK;  // explicit: the reference's no-op
+        MPM_TRY(ensureDbg());
+        if (!sorted_valid_) MPM_TRY(sortLive());
+        std::vector<SceneDev> saved = host_scenes_;
+        for (auto& d : host_scenes_) d.dt = dt;
+        MPM_TRY(uploadSceneTable());
+        launchSolveAll(true);
+        CUDA_TRY(cudaGetLastError());
+        host_scenes_ = saved;
+        MPM_TRY(uploadSceneTable());
         return MPM_OK;
     }
 
@@ -975,7 +1091,7 @@ public:
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
         LaunchCtx c = ctx();
         auto cs = combos();
-        if (cs.size() > 1 && !profiling_) {
+        if (cs.size() > 1 && !profiling_ && !any_implicit_) {
             // Scenes of different (stencil, transfer) combinations share no
             // items, tiles or nodes: their P2G -> grid -> G2P chains run
             // concurrently, combination k on side stream k - 1, each with its
@@ -1008,6 +1124,7 @@ public:
             mark(KF_GRID, 0);
             for (auto& k : cs)
                 launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+            if (any_implicit_) launchSolveAll(false);
             mark(KF_GRID, 1);
             collect(KF_GRID);
             mark(KF_G2P, 0);
@@ -1509,6 +1626,8 @@ private:
     int next_id_ = 0;
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     bool any_cfl_ = false;     // some scene steps with a CFL dt (two more launches per step)
+    bool any_implicit_ = false;  // some scene solves the semi-implicit update
+    DevMem cell_range_, solve_px_, solve_prep_, solve_T_;
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order
@@ -1711,9 +1830,16 @@ mpm_status mpm_solver_grid_collision(mpm_solver* s, float dt) {
     return s->eng.gridCollision(dt);
 }
 mpm_status mpm_solver_solve_linear_system(mpm_solver* s, float dt) {
-    (void)dt;
     MPM_TRY(check(s));
-    return MPM_OK;  // the reference's explicit solver leaves this a TODO (src/mpm_solver3d.cu:312-314)
+    return s->eng.solveLinearSystem(dt);  // a no-op while the solver is explicit (beta = 0), as in the reference
+}
+mpm_status mpm_solver_set_implicit(mpm_solver* s, float beta, int32_t max_iter, float tol) {
+    MPM_TRY(check(s));
+    return s->eng.setImplicit(s->scene, beta, max_iter, tol);
+}
+mpm_status mpm_solver_solve_info(mpm_solver* s, int32_t* iterations, float* residual) {
+    MPM_TRY(check(s));
+    return s->eng.solveInfo(s->scene, iterations, residual);
 }
 mpm_status mpm_solver_grid_to_particles(mpm_solver* s, float dt, float blend) {
     MPM_TRY(check(s));
@@ -1947,6 +2073,14 @@ mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* 
                                    const float* velocity) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.setLevelSet(scene_id, phi, friction, velocity);
+}
+mpm_status mpm_batch_set_implicit(mpm_batch* b, int32_t scene_id, float beta, int32_t max_iter, float tol) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.setImplicit(scene_id, beta, max_iter, tol);
+}
+mpm_status mpm_batch_solve_info(mpm_batch* b, int32_t scene_id, int32_t* iterations, float* residual) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.solveInfo(scene_id, iterations, residual);
 }
 mpm_status mpm_batch_set_cfl(mpm_batch* b, int32_t scene_id, float cfl) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");

@@ -66,6 +66,22 @@ struct CflState {
     double time;
 };
 
+// Semi-implicit solve of one scene (see implicit.cu).  vec holds six dense
+// node vectors of float4 (x, r, z, p, Ap, Az; .w unused); part holds the
+// per-block FP64 partial sums of the dot products, [quantity][slot][block].
+struct SolveStatus {
+    int done_at;     // first iteration whose test found convergence (INT_MAX while running)
+    int iters;
+    float residual;  // |r| / |M v*| at the end
+    int pad;
+};
+struct SolveDev {
+    float* m;
+    float4* vec;
+    double* part;
+    SolveStatus* status;
+};
+
 struct SceneDev {
     float origin[3];
     float h, inv_h, range;
@@ -95,6 +111,11 @@ struct SceneDev {
     // written into dt by cflFinalizeKernel before the step's kernels run.
     float cfl, dt_max;
     CflState* cfl_state;
+    // semi-implicit update: beta > 0 makes the step solve
+    // (M + beta dt^2 H) v = M v* after the grid collision
+    float beta, solve_tol;
+    int solve_max_iter;
+    SolveDev solve;
 };
 
 struct BlockItem {

@@ -74,6 +74,26 @@ void launchVolume(const LaunchCtx& c, int parity, int S);
 void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, size_t cap, const float* staged, size_t n,
                      bool has_volume);
 void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out);
+// Semi-implicit solve (implicit.cu) of the scenes with beta > 0.  Global
+// buffers over the sorted particles of the batch and its cell keys.
+struct SolveBuffers {
+    const uint32_t* sorted_keys;  // ntot
+    const uint32_t* perm;         // ntot
+    uint2* cell_range;            // nkeys: first and end sorted position of each cell key
+    size_t nkeys;
+    float4* px;                   // ntot: position, mass (sorted order)
+    float* prep;                  // kSolvePrepPlanes x ntot
+    float4* T;                    // 3 x ntot: V0 dP Fe^T rows
+    uint32_t ntot;
+};
+constexpr int kSolvePrepPlanes = 44;
+constexpr int kSolveBlocks = 512;  // node-kernel blocks per scene = partial sums per dot product
+inline size_t solvePartialDoubles(int max_iter) { return (size_t)4 * (size_t)(max_iter + 2) * kSolveBlocks; }
+// split: v* from and to the split-mode dense planes (no collision after);
+// else from and to the fused step's v* grid, with the grid collision after.
+void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
+                 int max_iter, bool split);
+
 // CFL time step of the scenes with cfl > 0: max |v|^2 over their live
 // particles, then dt = min(dt_max, cfl h / max|v|) into the scene table.
 void launchCfl(const LaunchCtx& c, int parity, size_t max_n);

@@ -306,6 +306,17 @@ class _SolverBase:
     def download_wait(self):
         check(self._lib.mpm_solver_download_wait(self._h), "download_wait")
 
+    def set_implicit(self, beta: float, max_iter: int = 50, tol: float = 1e-5):
+        """Semi-implicit update: beta > 0 solves (M + beta dt^2 H) v = M v* every
+        step (1/2 semi-implicit, 1 backward Euler); 0 is the explicit step."""
+        check(self._lib.mpm_solver_set_implicit(self._h, float(beta), int(max_iter), float(tol)), "set_implicit")
+
+    def solve_info(self) -> tuple:
+        """(iterations, |r| / |M v*|) of the last semi-implicit solve."""
+        it, res = C.c_int32(), C.c_float()
+        check(self._lib.mpm_solver_solve_info(self._h, C.byref(it), C.byref(res)), "solve_info")
+        return it.value, res.value
+
     def set_cfl(self, cfl: float):
         """CFL time step: cfl > 0 makes each step's dt min(dt, cfl h / max|v_p|); 0 restores the fixed dt."""
         check(self._lib.mpm_solver_set_cfl(self._h, float(cfl)), "set_cfl")

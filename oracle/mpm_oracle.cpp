@@ -373,6 +373,86 @@ inline Mat3<R> volumeTimesCauchyStress(Particle<R>& p) {
     return P;
 }
 
+// Cofactor matrix J F^-T of a 3x3 matrix by columns: c0 = f1 x f2,
+// c1 = f2 x f0, c2 = f0 x f1 (f_k = column k).
+template <class R>
+inline Vec3<R> cross3(const Vec3<R>& a, const Vec3<R>& b) {
+    return Vec3<R>{{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]}};
+}
+template <class R>
+inline Vec3<R> column(const Mat3<R>& A, int k) {
+    return Vec3<R>{{A(0, k), A(1, k), A(2, k)}};
+}
+template <class R>
+inline Mat3<R> cofactor(const Mat3<R>& F) {
+    Mat3<R> C{};
+    for (int k = 0; k < 3; ++k) {
+        Vec3<R> c = cross3(column(F, (k + 1) % 3), column(F, (k + 2) % 3));
+        for (int r = 0; r < 3; ++r) C(r, k) = c[r];
+    }
+    return C;
+}
+// Differential of the cofactor along dF (linear in dF).
+template <class R>
+inline Mat3<R> cofactorDifferential(const Mat3<R>& F, const Mat3<R>& dF) {
+    Mat3<R> C{};
+    for (int k = 0; k < 3; ++k) {
+        const int a = (k + 1) % 3, b = (k + 2) % 3;
+        Vec3<R> c1 = cross3(column(dF, a), column(F, b)), c2 = cross3(column(F, a), column(dF, b));
+        for (int r = 0; r < 3; ++r) C(r, k) = c1[r] + c2[r];
+    }
+    return C;
+}
+
+// dP/dF : dF at Fe for the first Piola stress P of the two models (the
+// stresses above are P Fe^T).  Fixed corotated: P = 2 mu (F - R) + la (J - 1)
+// cof F, dP = 2 mu (dF - dR) + la (dJ cof F + (J - 1) dcof F) with
+// dR = U W V^T, W_ij = (M_ij - M_ji) / (s_i + s_j), M = U^T dF V (the
+// rotation differential of the polar decomposition; Stomakhin et al. 2013,
+// "A material point method for snow simulation", supplementary notes).
+// Neo-Hookean: P = mu (F - F^-T) + la ln J F^-T,
+// dP = mu dF + (la ln J - mu) d(F^-T) + la (F^-T : dF) F^-T with
+// d(F^-T) = -F^-T dF^T F^-T.  mu, la are the hardened Lame parameters of Fp.
+template <class R>
+inline Mat3<R> stressDifferential(const Particle<R>& p, const Mat3<R>& dF) {
+    R mu, la;
+    plasticLame(p, mu, la);
+    const Mat3<R>& F = p.Fe;
+    const Mat3<R> C = cofactor(F);
+    const R J = det3(F);
+    Mat3<R> dP{};
+    if (p.model == MPM_MODEL_NEO_HOOKEAN) {
+        Mat3<R> FiT{};
+        for (int i = 0; i < 9; ++i) FiT.a[i] = C.a[i] / J;
+        Mat3<R> dFiT = matmul(matmul(FiT, transpose(dF)), FiT);
+        R dlnJ = 0;
+        for (int i = 0; i < 9; ++i) dlnJ += FiT.a[i] * dF.a[i];
+        const R lnJ = (R)std::log((double)J);
+        for (int i = 0; i < 9; ++i) dP.a[i] = mu * dF.a[i] - (la * lnJ - mu) * dFiT.a[i] + la * dlnJ * FiT.a[i];
+        return dP;
+    }
+    Mat3<R> U, V;
+    Vec3<R> s;
+    svd3(F, U, s, V);
+    const Mat3<R> M = matmul(matmul(transpose(U), dF), V);
+    Mat3<R> W{};
+    for (int i = 0; i < 3; ++i)
+        for (int j = i + 1; j < 3; ++j) {
+            R den = s[i] + s[j];
+            if (std::fabs(den) < (R)1e-6) den = den < 0 ? (R)-1e-6 : (R)1e-6;
+            const R w = (M(i, j) - M(j, i)) / den;
+            W(i, j) = w;
+            W(j, i) = -w;
+        }
+    const Mat3<R> dR = matmul(matmul(U, W), transpose(V));
+    const Mat3<R> dC = cofactorDifferential(F, dF);
+    R dJ = 0;
+    for (int i = 0; i < 9; ++i) dJ += C.a[i] * dF.a[i];
+    for (int i = 0; i < 9; ++i)
+        dP.a[i] = (R)2 * mu * (dF.a[i] - dR.a[i]) + la * (dJ * C.a[i] + (J - (R)1) * dC.a[i]);
+    return dP;
+}
+
 // updateDeformationGradient (:53-70).
 template <class R>
 inline void updateDeformationGradient(Particle<R>& p, const Mat3<R>& gradv, R dt) {
@@ -683,6 +763,152 @@ void Solver<R>::advectParticles(R dt) {
         for (int a = 0; a < 3; ++a) particles[i].x[a] += dt * particles[i].v[a];
 }
 
+// Hessian action and the semi-implicit solve (Stomakhin et al. 2013, section
+// 9: sum_j (I delta_ij + beta dt^2 m_i^-1 d2Phi/dx_i dx_j) v_j = v*_i, solved
+// here in the symmetric form (M + beta dt^2 H) v = M v* by conjugate
+// residual).  Unknowns are the nodes with m > FLT_EPSILON (the velocity
+// update's threshold, src/grid3d.cu:36-41).
+template <class R>
+void Solver<R>::hessianAction(const std::vector<Vec3<R>>& u, std::vector<Vec3<R>>& out) {
+    std::vector<Mat3<R>> T(particles.size());
+#pragma omp parallel for schedule(static) num_threads(threads)
+    for (long long i = 0; i < (long long)particles.size(); ++i) {
+        const Particle<R>& p = particles[i];
+        Mat3<R> G{};
+        forEachNode(p, [&](size_t gi, const Vec3<R>& gp) {
+            Vec3<R> g = weightGradient3D(desc.interpolation, p.x, gp, h);
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) G(a, b) += u[gi][a] * g[b];
+        });
+        Mat3<R> dP = stressDifferential(p, matmul(G, p.Fe));
+        Mat3<R> t = matmul(dP, transpose(p.Fe));
+        for (int k = 0; k < 9; ++k) t.a[k] *= p.volume0;
+        T[i] = t;
+    }
+    out.assign(grid.size(), Vec3<R>{});
+    scatterDeterministic([&](size_t i) {
+        const Particle<R>& p = particles[i];
+        forEachNode(p, [&](size_t gi, const Vec3<R>& gp) {
+            Vec3<R> g = weightGradient3D(desc.interpolation, p.x, gp, h);
+            for (int a = 0; a < 3; ++a) out[gi][a] += T[i](a, 0) * g[0] + T[i](a, 1) * g[1] + T[i](a, 2) * g[2];
+        });
+    });
+}
+
+template <class R>
+void Solver<R>::displacedForce(const std::vector<Vec3<R>>& d, std::vector<Vec3<R>>& out) {
+    std::vector<Mat3<R>> T(particles.size());
+    for (size_t i = 0; i < particles.size(); ++i) {
+        Particle<R> p = particles[i];
+        Mat3<R> G{};
+        forEachNode(p, [&](size_t gi, const Vec3<R>& gp) {
+            Vec3<R> g = weightGradient3D(desc.interpolation, p.x, gp, h);
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) G(a, b) += d[gi][a] * g[b];
+        });
+        const Mat3<R> F0 = p.Fe;
+        Mat3<R> A = Mat3<R>::identity();
+        for (int k = 0; k < 9; ++k) A.a[k] += G.a[k];
+        p.Fe = matmul(A, F0);
+        // tau = V0 P(F^) F^^T, so V0 P(F^) F0^T = tau F^^-T F0^T
+        const Mat3<R> tau = volumeTimesCauchyStress(p);
+        const Mat3<R> C = cofactor(p.Fe);
+        const R J = det3(p.Fe);
+        Mat3<R> FiT{};
+        for (int k = 0; k < 9; ++k) FiT.a[k] = C.a[k] / J;
+        T[i] = matmul(matmul(tau, FiT), transpose(F0));
+    }
+    out.assign(grid.size(), Vec3<R>{});
+    for (size_t i = 0; i < particles.size(); ++i) {
+        const Particle<R>& p = particles[i];
+        forEachNode(p, [&](size_t gi, const Vec3<R>& gp) {
+            Vec3<R> g = weightGradient3D(desc.interpolation, p.x, gp, h);
+            for (int a = 0; a < 3; ++a) out[gi][a] -= T[i](a, 0) * g[0] + T[i](a, 1) * g[1] + T[i](a, 2) * g[2];
+        });
+    }
+}
+
+template <class R>
+void Solver<R>::solveLinearSystem(R dt) {
+    last_iters = 0;
+    last_residual = 0;
+    if (!(beta > 0)) return;
+    // Conjugate residual preconditioned by the node masses (z = M^-1 r): the
+    // masses span orders of magnitude between the interior and the edge of a
+    // body, and the unpreconditioned iteration stalls on the light nodes.
+    const size_t nn = grid.size();
+    const R c = beta * dt * dt;
+    std::vector<char> act(nn);
+    std::vector<R> m(nn);
+    std::vector<Vec3<R>> x(nn), r(nn), z(nn), pv(nn), Az(nn), Ap(nn), hv;
+    for (size_t i = 0; i < nn; ++i) {
+        act[i] = grid[i].mass > (R)kFltEps;
+        m[i] = act[i] ? grid[i].mass : (R)0;
+        x[i] = act[i] ? grid[i].velocity_star : Vec3<R>{};
+    }
+    auto dot = [&](const std::vector<Vec3<R>>& a, const std::vector<Vec3<R>>& b) {
+        R s = 0;
+        for (size_t i = 0; i < nn; ++i)
+            if (act[i]) s += a[i][0] * b[i][0] + a[i][1] * b[i][1] + a[i][2] * b[i][2];
+        return s;
+    };
+    R bb = 0;
+    for (size_t i = 0; i < nn; ++i)
+        for (int a = 0; a < 3; ++a) bb += (m[i] * x[i][a]) * (m[i] * x[i][a]);
+    // x0 = v*: r0 = M v* - (M x0 + c H x0) = -c H v*
+    hessianAction(x, hv);
+    for (size_t i = 0; i < nn; ++i)
+        for (int a = 0; a < 3; ++a) {
+            r[i][a] = act[i] ? -c * hv[i][a] : (R)0;
+            z[i][a] = act[i] ? r[i][a] / m[i] : (R)0;
+        }
+    R rr = dot(r, r);
+    hessianAction(z, hv);
+    for (size_t i = 0; i < nn; ++i)
+        for (int a = 0; a < 3; ++a) {
+            Az[i][a] = act[i] ? m[i] * z[i][a] + c * hv[i][a] : (R)0;
+            pv[i][a] = z[i][a];
+            Ap[i][a] = Az[i][a];
+        }
+    R zAz = dot(z, Az);
+    auto apq = [&]() {  // (Ap, M^-1 Ap)
+        R s = 0;
+        for (size_t i = 0; i < nn; ++i)
+            if (act[i]) s += (Ap[i][0] * Ap[i][0] + Ap[i][1] * Ap[i][1] + Ap[i][2] * Ap[i][2]) / m[i];
+        return s;
+    };
+    R Apq = apq();
+    int k = 0;
+    for (; k < max_iter; ++k) {
+        if (rr <= tol * tol * bb || !(Apq > 0)) break;
+        const R alpha = zAz / Apq;
+        for (size_t i = 0; i < nn; ++i)
+            if (act[i])
+                for (int a = 0; a < 3; ++a) {
+                    x[i][a] += alpha * pv[i][a];
+                    r[i][a] -= alpha * Ap[i][a];
+                    z[i][a] -= alpha * (Ap[i][a] / m[i]);
+                }
+        rr = dot(r, r);
+        hessianAction(z, hv);
+        for (size_t i = 0; i < nn; ++i)
+            for (int a = 0; a < 3; ++a) Az[i][a] = act[i] ? m[i] * z[i][a] + c * hv[i][a] : (R)0;
+        const R zAz1 = dot(z, Az);
+        const R gam = zAz1 / zAz;
+        zAz = zAz1;
+        for (size_t i = 0; i < nn; ++i)
+            for (int a = 0; a < 3; ++a) {
+                pv[i][a] = z[i][a] + gam * pv[i][a];
+                Ap[i][a] = Az[i][a] + gam * Ap[i][a];
+            }
+        Apq = apq();
+    }
+    for (size_t i = 0; i < nn; ++i)
+        if (act[i]) grid[i].velocity_star = x[i];
+    last_iters = k;
+    last_residual = bb > 0 ? std::sqrt((double)rr / (double)bb) : 0.0;
+}
+
 template <class R>
 void Solver<R>::simulateOneStep() {
     R dt = (R)desc.dt;
@@ -699,6 +925,10 @@ void Solver<R>::simulateOneStep() {
     computeGravityForces();
     updateGridVelocities(dt);
     gridCollision(dt);
+    if (beta > 0) {  // semi-implicit: solve, then the boundary again on the solved velocities
+        solveLinearSystem(dt);
+        gridCollision(dt);
+    }
     gridToParticles(dt, (R)desc.blend);
     if (enable_particles_collision) particlesCollision(dt);
     advectParticles(dt);
@@ -930,6 +1160,45 @@ void orc_collision(int bits, const double* pos, const double* vel, const double*
         Vec3<double> r = applyBoundaryCollision<double>(p, v, a, b, friction);
         for (int i = 0; i < 3; ++i) out[i] = r[i];
     }
+}
+
+void orc_set_implicit(void* p, double beta, int max_iter, double tol) {
+    Handle* h = (Handle*)p;
+    auto set = [&](auto* s) {
+        using RR = typename std::remove_pointer<decltype(s)>::type::Real;
+        s->beta = (RR)beta;
+        s->max_iter = max_iter;
+        s->tol = (RR)tol;
+    };
+    if (h->f) set(h->f);
+    else set(h->d);
+}
+void orc_solve_linear_system(void* p, double dt) {
+    Handle* h = (Handle*)p;
+    if (h->f) h->f->solveLinearSystem((float)dt);
+    else h->d->solveLinearSystem(dt);
+}
+void orc_solve_info(void* p, int* iters, double* residual) {
+    Handle* h = (Handle*)p;
+    *iters = h->f ? h->f->last_iters : h->d->last_iters;
+    *residual = h->f ? h->f->last_residual : h->d->last_residual;
+}
+// which = 0: hessianAction(u), 1: displacedForce(u); u and out: nodes x 3
+void orc_grid_operator(void* p, int which, const double* u, double* out) {
+    Handle* h = (Handle*)p;
+    auto run = [&](auto* s) {
+        using RR = typename std::remove_pointer<decltype(s)>::type::Real;
+        const size_t nn = s->grid.size();
+        std::vector<Vec3<RR>> in(nn), res;
+        for (size_t i = 0; i < nn; ++i)
+            for (int a = 0; a < 3; ++a) in[i][a] = (RR)u[3 * i + a];
+        if (which == 0) s->hessianAction(in, res);
+        else s->displacedForce(in, res);
+        for (size_t i = 0; i < nn; ++i)
+            for (int a = 0; a < 3; ++a) out[3 * i + a] = (double)res[i][a];
+    };
+    if (h->f) run(h->f);
+    else run(h->d);
 }
 
 void orc_set_cfl(void* p, double cfl) {

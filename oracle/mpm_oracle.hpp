@@ -246,6 +246,13 @@ public:
     void gridToParticles(R dt, R blend);  // :316-379 / apic :326-388
     void particlesCollision(R dt);     // :428-445
     void advectParticles(R dt);        // :381-391
+    void solveLinearSystem(R dt);      // :312-314 (a TODO there): semi-implicit solve
+    // H u: the elastic Hessian applied to node velocities u (zero at massless
+    // nodes), out = sum_p V0 (dP/dF : (sum_j u_j grad w_jp^T) Fe) Fe^T grad w_ip
+    void hessianAction(const std::vector<Vec3<R>>& u, std::vector<Vec3<R>>& out);
+    // grid force -sum_p V0 P(F^) Fe^T grad w_ip with F^ = (I + sum_j d_j grad w_jp^T) Fe
+    // (nodes displaced by d): finite differences of it check hessianAction
+    void displacedForce(const std::vector<Vec3<R>>& d, std::vector<Vec3<R>>& out);
     void simulateOneStep();            // :100-125
 
     mpm_scene_desc desc;
@@ -259,6 +266,13 @@ public:
     R Dinv = 0;  // APIC: (k h^2)^-1, src/apic_mpm_solver3d.cu:151-157
     // Level-set collision object (include/collision_object3d.h:9-12): signed
     // distance per node, negative inside; applied after the grid boundary.
+    // semi-implicit update (beta > 0): (M + beta dt^2 H) v = M v*, conjugate
+    // residual to |r| <= tol |M v*| or max_iter iterations
+    R beta = 0;
+    int max_iter = 30;
+    R tol = (R)1e-5;
+    int last_iters = 0;
+    double last_residual = 0;
     // CFL time step: cfl > 0 makes each step's dt min(desc.dt, cfl h / max|v_p|)
     R cfl = 0;
     double time = 0;

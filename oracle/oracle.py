@@ -55,6 +55,10 @@ def load():
         "orc_collision": (None, [C.c_int, D, D, D, D, C.c_double, D]),
         "orc_set_level_set": (C.c_int, [P, D, C.c_double, D]),
         "orc_set_cfl": (None, [P, C.c_double]),
+        "orc_set_implicit": (None, [P, C.c_double, C.c_int, C.c_double]),
+        "orc_solve_linear_system": (None, [P, C.c_double]),
+        "orc_solve_info": (None, [P, C.POINTER(C.c_int), D]),
+        "orc_grid_operator": (None, [P, C.c_int, D, D]),
         "orc_time": (None, [P, D, D]),
         "orc_level_set_collision": (None, [C.c_int, C.POINTER(C.c_int), D, C.c_double, D, C.c_double, D, D, D, D]),
         "orc_stress": (None, [C.c_int, C.c_int, D, D, C.c_double, C.c_double, C.c_double, C.c_double, D, D]),
@@ -122,6 +126,30 @@ class OracleSolver:
         vel = np.ascontiguousarray(velocity, np.float64).reshape(3)
         if self.lib.orc_set_level_set(self.h, _dp(phi), float(friction), _dp(vel)):
             raise ValueError(self.lib.orc_last_error().decode())
+
+    def set_implicit(self, beta: float, max_iter: int = 30, tol: float = 1e-5):
+        self.lib.orc_set_implicit(self.h, float(beta), int(max_iter), float(tol))
+
+    def solve_linear_system(self, dt):
+        self.lib.orc_solve_linear_system(self.h, float(dt))
+
+    def solve_info(self) -> tuple:
+        it, res = C.c_int(), np.zeros(1)
+        self.lib.orc_solve_info(self.h, C.byref(it), _dp(res))
+        return it.value, float(res[0])
+
+    def hessian_action(self, u) -> np.ndarray:
+        return self._grid_op(0, u)
+
+    def displaced_force(self, d) -> np.ndarray:
+        return self._grid_op(1, d)
+
+    def _grid_op(self, which, u):
+        u = np.ascontiguousarray(u, np.float64).reshape(-1, 3)
+        assert u.shape[0] == self.res[0] * self.res[1] * self.res[2]
+        out = np.empty_like(u)
+        self.lib.orc_grid_operator(self.h, int(which), _dp(u), _dp(out))
+        return out
 
     def set_cfl(self, cfl: float):
         self.lib.orc_set_cfl(self.h, float(cfl))

@@ -183,7 +183,7 @@ struct SceneHost {
     // semi-implicit update (beta > 0) and its solver buffers (implicit.cu)
     float beta = 0.f, solve_tol = 1e-5f;
     int solve_max_iter = 50;
-    DevMem solve_m, solve_vec, solve_part, solve_status;
+    DevMem solve_m, solve_vec, solve_list, solve_part, solve_status;
     size_t nodes() const { return (size_t)desc.resolution[0] * desc.resolution[1] * desc.resolution[2]; }
     ~SceneHost() {
         for (int k = 0; k < 2; ++k) {
@@ -724,14 +724,15 @@ public:
         d.beta = s.beta;
         d.solve_tol = s.solve_tol;
         d.solve_max_iter = s.solve_max_iter;
-        d.solve = SolveDev{s.solve_m.as<float>(), s.solve_vec.as<float4>(), s.solve_part.as<double>(),
-                           s.solve_status.as<SolveStatus>()};
+        d.solve = SolveDev{s.solve_m.as<float>(), s.solve_vec.as<float4>(), s.solve_list.as<int>(),
+                           s.solve_part.as<double>(), s.solve_status.as<SolveStatus>()};
     }
     // Batch-wide buffers over the sorted particles and the cell keys.
     mpm_status ensureSolveBuffers() {
         if (!any_implicit_ || dirty_) return MPM_OK;
         const size_t n = std::max<size_t>(ntot_, 1);
         MPM_TRY(cell_range_.grow(sizeof(uint2) * (size_t)total_blocks_ * 64, "solver cell ranges"));
+        MPM_TRY(block_range_.grow(sizeof(uint2) * (size_t)total_blocks_, "solver block ranges"));
         MPM_TRY(solve_px_.grow(sizeof(float4) * n, "solver particle positions"));
         MPM_TRY(solve_prep_.grow(sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
         MPM_TRY(solve_T_.grow(sizeof(float4) * 3 * n, "solver particle stress differentials"));
@@ -751,7 +752,8 @@ public:
         if (beta > 0.f) {
             const size_t nodes = s.nodes();
             MPM_TRY(s.solve_m.grow(sizeof(float) * nodes, "solver node masses"));
-            MPM_TRY(s.solve_vec.grow(sizeof(float4) * 6 * nodes, "solver node vectors"));
+            MPM_TRY(s.solve_vec.grow(sizeof(float4) * kSolveVectors * nodes, "solver node vectors"));
+            MPM_TRY(s.solve_list.grow(sizeof(int) * nodes, "solver node list"));
             MPM_TRY(s.solve_part.grow(sizeof(double) * solvePartialDoubles(max_iter), "solver partial sums"));
             MPM_TRY(s.solve_status.grow(sizeof(SolveStatus), "solver status"));
             CUDA_TRY(cudaMemset(s.solve_status.p, 0, sizeof(SolveStatus)));
@@ -788,8 +790,8 @@ public:
     }
     void launchSolveAll(bool split) {
         SolveBuffers b{keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), cell_range_.as<uint2>(),
-                       (size_t)total_blocks_ * 64, solve_px_.as<float4>(), solve_prep_.as<float>(),
-                       solve_T_.as<float4>(), (uint32_t)ntot_};
+                       (size_t)total_blocks_ * 64, block_range_.as<uint2>(), (size_t)total_blocks_,
+                       solve_px_.as<float4>(), solve_prep_.as<float>(), solve_T_.as<float4>(), (uint32_t)ntot_};
         const std::vector<int> S = stencilSizes();
         launchSolve(ctx(), b, parity_, S.data(), (int)S.size(), maxSolveIters(), split);
     }
@@ -1627,7 +1629,7 @@ private:
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     bool any_cfl_ = false;     // some scene steps with a CFL dt (two more launches per step)
     bool any_implicit_ = false;  // some scene solves the semi-implicit update
-    DevMem cell_range_, solve_px_, solve_prep_, solve_T_;
+    DevMem cell_range_, block_range_, solve_px_, solve_prep_, solve_T_;
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order

@@ -66,18 +66,20 @@ struct CflState {
     double time;
 };
 
-// Semi-implicit solve of one scene (see implicit.cu).  vec holds six dense
-// node vectors of float4 (x, r, z, p, Ap, Az; .w unused); part holds the
-// per-block FP64 partial sums of the dot products, [quantity][slot][block].
+// Semi-implicit solve of one scene (see implicit.cu).  vec holds seven
+// dense node vectors of float4 (x, r, z, p, Ap, Az, h; .w unused); list the
+// nodes with mass; part the per-block FP64 partial sums of the dot
+// products, [quantity][slot][block].
 struct SolveStatus {
     int done_at;     // first iteration whose test found convergence (INT_MAX while running)
     int iters;
     float residual;  // |r| / |M v*| at the end
-    int pad;
+    int nactive;     // nodes in list
 };
 struct SolveDev {
     float* m;
     float4* vec;
+    int* list;
     double* part;
     SolveStatus* status;
 };

@@ -81,12 +81,15 @@ struct SolveBuffers {
     const uint32_t* perm;         // ntot
     uint2* cell_range;            // nkeys: first and end sorted position of each cell key
     size_t nkeys;
+    uint2* block_range;           // nblocks: the same per 4^3 block of cells (key >> 6)
+    size_t nblocks;
     float4* px;                   // ntot: position, mass (sorted order)
     float* prep;                  // kSolvePrepPlanes x ntot
     float4* T;                    // 3 x ntot: V0 dP Fe^T rows
     uint32_t ntot;
 };
 constexpr int kSolvePrepPlanes = 44;
+constexpr int kSolveVectors = 7;
 constexpr int kSolveBlocks = 512;  // node-kernel blocks per scene = partial sums per dot product
 inline size_t solvePartialDoubles(int max_iter) { return (size_t)4 * (size_t)(max_iter + 2) * kSolveBlocks; }
 // split: v* from and to the split-mode dense planes (no collision after);

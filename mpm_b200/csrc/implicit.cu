@@ -8,25 +8,32 @@
 //     H u = sum_p V0 (dP/dF : (sum_j u_j grad w_jp^T) Fe) Fe^T grad w_ip,
 // and solved by conjugate residual preconditioned with the node masses.
 //
-//   cellRangeKernel    first and end sorted position of every cell key
+//   cellRangeKernel    first and end sorted position of every cell key and
+//                      of every 4^3 block of cells
 //   solvePrepKernel    per sorted particle: Fe, its SVD, cofactor, J, ln J,
 //                      V0 mu and V0 la (hardened), model; position and mass
-//   solveMassKernel    node masses, x0 = v*, |M v*|^2
+//   solveInitKernel    node masses (the transfer's), x0 = v*, the other
+//                      vectors 0, |M v*|^2, list of the nodes with mass
 //   solveGatherKernel  per particle: G = sum_j u_j grad w^T, T = V0 dP(G Fe) Fe^T
-//   solveScatterKernel per node: h = sum_p T_p grad w_ip, then r or Az
-//   solveUpdateKernel, solveDirKernel   the vector updates of the iteration
+//   solveScatterKernel per listed node: h = sum_p T_p grad w_ip
+//   solveResidualKernel, solveAzKernel, solveUpdateKernel, solveDirKernel
+//                      the elementwise vector updates and dot products
 //   solveFinalKernel   v* = x (and the grid collision again in the fused step)
 //
-// Node kernels gather over the S^3 cells around a node and their particles in
-// sorted order, and every dot product is a set of per-block FP64 partials that
-// each consumer block reduces in block order: every sum has a fixed order, so
-// the solve is bitwise reproducible and a scene's result does not depend on
-// its batch-mates.  Convergence (|r| <= tol |M v*|) is decided on the device;
-// a scene that converged skips the remaining launches of the step.
+// A node's sum h is formed by one warp: the lanes share out the
+// particles of the S^3 cells around the node (flattened, in sorted order) and
+// the lane sums meet in a fixed shuffle tree, so a node's value does not
+// depend on which warp computes it.  Dot products come from the elementwise
+// kernels as per-block FP64 partials over a fixed node partition, which every
+// consumer block reduces in block order.  The solve is bitwise reproducible
+// and a scene's result does not depend on its batch-mates.  Convergence
+// (|r| <= tol |M v*|) is decided on the device; a scene that converged skips
+// the remaining launches of the step.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <climits>
+#include <type_traits>
 
 #include "engine_host.hpp"
 #include "mpm_math.cuh"
@@ -36,9 +43,9 @@ namespace mpm {
 
 namespace {
 
-enum { VX = 0, VR = 1, VZ = 2, VP = 3, VAP = 4, VAZ = 5 };       // node vectors
-enum { QRR = 0, QZAZ = 1, QAPQ = 2, QBB = 3 };                   // dot products
-enum { SCATTER_INIT = 0, SCATTER_AZ = 1 };
+enum { VX = 0, VR = 1, VZ = 2, VP = 3, VAP = 4, VAZ = 5, VH = 6 };  // node vectors
+enum { QRR = 0, QZAZ = 1, QAPQ = 2, QBB = 3 };                      // dot products
+static_assert(VH + 1 == kSolveVectors, "node vector count");
 
 static_assert(kSolveBlocks == 2 * kThreads, "partials are reduced two per thread");
 
@@ -47,6 +54,7 @@ struct SolveArgs {
     const uint32_t* sorted_keys;
     const uint32_t* perm;
     const uint2* cell_range;
+    const uint2* block_range;
     float4* px;
     float* prep;
     float4* T;
@@ -119,18 +127,69 @@ __device__ __forceinline__ void nodeWeight(const SceneDev& sc, const float* x, c
     }
 }
 
-// Visit the particles whose stencil covers node n: the S^3 base cells
-// n - S + 1 .. n (always inside the key range), each in sorted order.
-template <int S, class Fn>
-__device__ __forceinline__ void forNodeParticles(const SceneDev& sc, const SolveArgs& a, const int* n, Fn&& fn) {
-    for (int cz = 0; cz < S; ++cz)
-        for (int cy = 0; cy < S; ++cy)
-            for (int cx = 0; cx < S; ++cx) {
-                const int base[3] = {n[0] - S + 1 + cx, n[1] - S + 1 + cy, n[2] - S + 1 + cz};
-                const int k[3] = {S - 1 - cx, S - 1 - cy, S - 1 - cz};
-                const uint2 rg = a.cell_range[makeKey(sc, base)];
-                for (uint32_t p = rg.x; p < rg.y; ++p) fn(p, base, k);
-            }
+// Sum fn(p, base, k) over the particles whose stencil covers node n, by one
+// warp: the S^3 base cells n - S + 1 .. n (always inside the key range) in a
+// fixed order, their particles in sorted order, flattened and dealt to the
+// lanes round-robin; the lane sums meet in a fixed shuffle tree.  Every lane
+// returns the total.  sh: this warp's 2 S^3 + 1 ints of shared memory.
+template <int S, int C, class Fn>
+__device__ __forceinline__ void warpNodeSum(const SceneDev& sc, const SolveArgs& a, const int* n, int* sh, float* out,
+                                            Fn&& fn) {
+    constexpr int NC = S * S * S;
+    const int lane = threadIdx.x & 31;
+    int* first = sh;       // NC
+    int* start = sh + NC;  // NC + 1: flattened offset of each cell
+    int cnt[2] = {0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int ci = lane + 32 * h;
+        if (ci < NC) {
+            const int c[3] = {ci % S, (ci / S) % S, ci / (S * S)};
+            const int base[3] = {n[0] - S + 1 + c[0], n[1] - S + 1 + c[1], n[2] - S + 1 + c[2]};
+            const uint2 rg = a.cell_range[makeKey(sc, base)];
+            first[ci] = (int)rg.x;
+            cnt[h] = (int)(rg.y - rg.x);
+        }
+    }
+    // exclusive offsets in cell order: cells lane and 32 + lane
+    int v0 = cnt[0], v1 = cnt[1];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t0 = __shfl_up_sync(0xffffffffu, v0, o), t1 = __shfl_up_sync(0xffffffffu, v1, o);
+        if (lane >= o) {
+            v0 += t0;
+            v1 += t1;
+        }
+    }
+    const int tot0 = __shfl_sync(0xffffffffu, v0, 31);
+    if (lane < NC) start[lane] = v0 - cnt[0];
+    if (32 + lane < NC) start[32 + lane] = tot0 + v1 - cnt[1];
+    const int total = tot0 + __shfl_sync(0xffffffffu, v1, 31);
+    if (lane == 0) start[NC] = total;
+    __syncwarp();
+    float acc[C];
+#pragma unroll
+    for (int q = 0; q < C; ++q) acc[q] = 0.f;
+    for (int f = lane; f < total; f += 32) {
+        int lo = 0, hi = NC - 1;  // the cell with start[ci] <= f < start[ci + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (start[mid] <= f) lo = mid;
+            else hi = mid - 1;
+        }
+        const int c[3] = {lo % S, (lo / S) % S, lo / (S * S)};
+        const int base[3] = {n[0] - S + 1 + c[0], n[1] - S + 1 + c[1], n[2] - S + 1 + c[2]};
+        const int k[3] = {S - 1 - c[0], S - 1 - c[1], S - 1 - c[2]};
+        fn((uint32_t)(first[lo] + (f - start[lo])), base, k, acc);
+    }
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+        float v = acc[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        out[q] = __shfl_sync(0xffffffffu, v, 0);  // lane 0's tree order
+    }
+    __syncwarp();  // sh is reused by the warp's next node
 }
 
 __device__ __forceinline__ void ldMat(const float* prep, size_t stride, size_t i, int plane, float* m) {
@@ -190,17 +249,22 @@ __device__ __forceinline__ void mTm3(const float* A, const float* B, float* C) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-__global__ void cellRangeKernel(const uint32_t* __restrict__ keys, uint32_t n, uint2* __restrict__ range) {
+__global__ void cellRangeKernel(const uint32_t* __restrict__ keys, uint32_t n, uint2* __restrict__ range,
+                                uint2* __restrict__ block_range) {
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
         const uint32_t k = keys[i];
-        if (i == 0 || keys[i - 1] != k) range[k].x = i;
-        if (i + 1 == n || keys[i + 1] != k) range[k].y = i + 1;
+        const uint32_t kp = i > 0 ? keys[i - 1] : 0xffffffffu, kn = i + 1 < n ? keys[i + 1] : 0xffffffffu;
+        if (kp != k) range[k].x = i;
+        if (kn != k) range[k].y = i + 1;
+        if (i == 0 || (kp >> 6) != (k >> 6)) block_range[k >> 6].x = i;
+        if (i + 1 == n || (kn >> 6) != (k >> 6)) block_range[k >> 6].y = i + 1;
     }
 }
 
 __global__ void __launch_bounds__(kThreads) solvePrepKernel(SolveArgs a) {
     const SceneDev& sc = a.scenes[blockIdx.y];
     if (!solving(sc)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *sc.solve.status = SolveStatus{INT_MAX, 0, 0.f, 0};
     const float* f = sc.buf[a.parity].f;
     const uint16_t* mat = sc.buf[a.parity].mat;
     const size_t cap = sc.cap, st = a.ntot;
@@ -242,48 +306,58 @@ __global__ void __launch_bounds__(kThreads) solvePrepKernel(SolveArgs a) {
     }
 }
 
-template <int S>
-__global__ void __launch_bounds__(kThreads) solveMassKernel(SolveArgs a) {
+// Node masses, x0 = v*, the other vectors 0, |M v*|^2, and the list of the
+// nodes with mass.  The masses are the transfer's own: the split-mode grid
+// holds them densely; in the fused step the grid pass wrote (v*, m) for the
+// node blocks N (nodes 4N - 4 + L) next to a particle block N - (0|1, 0|1,
+// 0|1) that holds particles, and the other nodes have no mass this step.
+__global__ void __launch_bounds__(kThreads) solveInitKernel(SolveArgs a) {
     const SceneDev& sc = a.scenes[blockIdx.y];
-    if (!solving(sc) || sc.S != S) return;
+    if (!solving(sc)) return;
     const size_t nodes = sceneNodes(sc);
     float4* vec = sc.solve.vec;
     double acc = 0.0;
     for (size_t node = (size_t)blockIdx.x * kThreads + threadIdx.x; node < nodes;
          node += (size_t)kSolveBlocks * kThreads) {
-        int n[3];
-        nodeCoords(sc, node, n);
-        float m = 0.f;
-        forNodeParticles<S>(sc, a, n, [&](uint32_t p, const int* base, const int* k) {
-            const float4 q = a.px[p];
-            const float x[3] = {q.x, q.y, q.z};
-            float w[3], dw[3];
-            nodeWeight<S>(sc, x, base, k, w, dw);
-            m += q.w * (w[0] * w[1] * w[2]);
-        });
-        const bool act = m > kFltEps;
-        float vs[3] = {0.f, 0.f, 0.f};
-        if (act) {
-            if (a.split) {
+        float m = 0.f, vs[3] = {0.f, 0.f, 0.f};
+        if (a.split) {
+            m = sc.dbg[node];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) vs[c] = sc.dbg[(size_t)(7 + c) * nodes + node];
-            } else {
+            for (int c = 0; c < 3; ++c) vs[c] = sc.dbg[(size_t)(7 + c) * nodes + node];
+        } else {
+            int n[3];
+            nodeCoords(sc, node, n);
+            const int N[3] = {(n[0] + 4) >> 2, (n[1] + 4) >> 2, (n[2] + 4) >> 2};
+            bool written = false;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const int B[3] = {N[0] - (d & 1), N[1] - ((d >> 1) & 1), N[2] - (d >> 2)};
+                if (B[0] >= 0 && B[1] >= 0 && B[2] >= 0 && B[0] < sc.nb[0] && B[1] < sc.nb[1] && B[2] < sc.nb[2]) {
+                    const uint2 r = a.block_range[sc.block_base + (uint32_t)((B[2] * sc.nb[1] + B[1]) * sc.nb[0] + B[0])];
+                    written |= r.y > r.x;
+                }
+            }
+            if (written) {
                 const float4 v = sc.vstar[node];
+                m = v.w;
                 vs[0] = v.x;
                 vs[1] = v.y;
                 vs[2] = v.z;
             }
+        }
+        const bool act = m > kFltEps;
+        if (act) {
             acc += (double)(m * vs[0]) * (m * vs[0]) + (double)(m * vs[1]) * (m * vs[1]) +
                    (double)(m * vs[2]) * (m * vs[2]);
+            sc.solve.list[atomicAdd(&sc.solve.status->nactive, 1)] = (int)node;
         }
         sc.solve.m[node] = act ? m : 0.f;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        vec[(size_t)VX * nodes + node] = make_float4(vs[0], vs[1], vs[2], 0.f);
+        vec[(size_t)VX * nodes + node] = act ? make_float4(vs[0], vs[1], vs[2], 0.f) : z4;
 #pragma unroll
-        for (int v = VR; v <= VAZ; ++v) vec[(size_t)v * nodes + node] = z4;
+        for (int v = VR; v <= VH; ++v) vec[(size_t)v * nodes + node] = z4;
     }
     writePartial(acc, partSlot(sc, QBB, 0));
-    if (blockIdx.x == 0 && threadIdx.x == 0) *sc.solve.status = SolveStatus{INT_MAX, 0, 0.f, 0};
 }
 
 template <int S>
@@ -392,10 +466,41 @@ __global__ void __launch_bounds__(kThreads) solveGatherKernel(SolveArgs a, int s
     }
 }
 
+// h = sum_p T_p grad w_ip at the listed nodes (one warp per node).
 template <int S>
-__global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, int mode, int j, int k) {
+__global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, int k) {
     const SceneDev& sc = a.scenes[blockIdx.y];
     if (!solving(sc) || sc.S != S || blockDoneAt(sc) <= k) return;
+    __shared__ int sh[kThreads / 32][2 * S * S * S + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t nodes = sceneNodes(sc);
+    float4* h = sc.solve.vec + (size_t)VH * nodes;
+    const int na = sc.solve.status->nactive;
+    for (int li = blockIdx.x * (kThreads / 32) + warp; li < na; li += gridDim.x * (kThreads / 32)) {
+        const size_t node = (size_t)sc.solve.list[li];
+        int n[3];
+        nodeCoords(sc, node, n);
+        float out[3];
+        warpNodeSum<S, 3>(sc, a, n, sh[warp], out, [&](uint32_t p, const int* base, const int* kk, float* acc) {
+            const float4 q = a.px[p];
+            const float x[3] = {q.x, q.y, q.z};
+            float w[3], dw[3];
+            nodeWeight<S>(sc, x, base, kk, w, dw);
+            const float g[3] = {dw[0] * w[1] * w[2], w[0] * dw[1] * w[2], w[0] * w[1] * dw[2]};
+            const float4* Tp = a.T + 3 * (size_t)p;
+            const float4 t0 = Tp[0], t1 = Tp[1], t2 = Tp[2];
+            acc[0] += t0.x * g[0] + t0.y * g[1] + t0.z * g[2];
+            acc[1] += t1.x * g[0] + t1.y * g[1] + t1.z * g[2];
+            acc[2] += t2.x * g[0] + t2.y * g[1] + t2.z * g[2];
+        });
+        if (lane == 0) h[node] = make_float4(out[0], out[1], out[2], 0.f);
+    }
+}
+
+// x0 = v*: r0 = -c H v*, z0 = r0 / m, |r0|^2.
+__global__ void __launch_bounds__(kThreads) solveResidualKernel(SolveArgs a) {
+    const SceneDev& sc = a.scenes[blockIdx.y];
+    if (!solving(sc)) return;
     const size_t nodes = sceneNodes(sc);
     float4* vec = sc.solve.vec;
     const float c = sc.beta * sc.dt * sc.dt;
@@ -404,34 +509,33 @@ __global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, int 
          node += (size_t)kSolveBlocks * kThreads) {
         const float m = sc.solve.m[node];
         if (!(m > 0.f)) continue;
-        int n[3];
-        nodeCoords(sc, node, n);
-        float h[3] = {0.f, 0.f, 0.f};
-        forNodeParticles<S>(sc, a, n, [&](uint32_t p, const int* base, const int* kk) {
-            const float4 q = a.px[p];
-            const float x[3] = {q.x, q.y, q.z};
-            float w[3], dw[3];
-            nodeWeight<S>(sc, x, base, kk, w, dw);
-            const float g[3] = {dw[0] * w[1] * w[2], w[0] * dw[1] * w[2], w[0] * w[1] * dw[2]};
-            const float4* Tp = a.T + 3 * (size_t)p;
-            const float4 t0 = Tp[0], t1 = Tp[1], t2 = Tp[2];
-            h[0] += t0.x * g[0] + t0.y * g[1] + t0.z * g[2];
-            h[1] += t1.x * g[0] + t1.y * g[1] + t1.z * g[2];
-            h[2] += t2.x * g[0] + t2.y * g[1] + t2.z * g[2];
-        });
-        if (mode == SCATTER_INIT) {  // x0 = v*: r0 = -c H v*, z0 = r0 / m
-            const float r[3] = {-c * h[0], -c * h[1], -c * h[2]};
-            vec[(size_t)VR * nodes + node] = make_float4(r[0], r[1], r[2], 0.f);
-            vec[(size_t)VZ * nodes + node] = make_float4(r[0] / m, r[1] / m, r[2] / m, 0.f);
-            acc += (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
-        } else {  // Az = M z + c H z
-            const float3 z = ld3(vec[(size_t)VZ * nodes + node]);
-            const float Az[3] = {m * z.x + c * h[0], m * z.y + c * h[1], m * z.z + c * h[2]};
-            vec[(size_t)VAZ * nodes + node] = make_float4(Az[0], Az[1], Az[2], 0.f);
-            acc += (double)z.x * Az[0] + (double)z.y * Az[1] + (double)z.z * Az[2];
-        }
+        const float3 h = ld3(vec[(size_t)VH * nodes + node]);
+        const float r[3] = {-c * h.x, -c * h.y, -c * h.z};
+        vec[(size_t)VR * nodes + node] = make_float4(r[0], r[1], r[2], 0.f);
+        vec[(size_t)VZ * nodes + node] = make_float4(r[0] / m, r[1] / m, r[2] / m, 0.f);
+        acc += (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
     }
-    writePartial(acc, partSlot(sc, mode == SCATTER_INIT ? QRR : QZAZ, j));
+    writePartial(acc, partSlot(sc, QRR, 0));
+}
+
+// Az = M z + c H z, (z, Az) into slot j.
+__global__ void __launch_bounds__(kThreads) solveAzKernel(SolveArgs a, int j, int k) {
+    const SceneDev& sc = a.scenes[blockIdx.y];
+    if (!solving(sc) || blockDoneAt(sc) <= k) return;
+    const size_t nodes = sceneNodes(sc);
+    float4* vec = sc.solve.vec;
+    const float c = sc.beta * sc.dt * sc.dt;
+    double acc = 0.0;
+    for (size_t node = (size_t)blockIdx.x * kThreads + threadIdx.x; node < nodes;
+         node += (size_t)kSolveBlocks * kThreads) {
+        const float m = sc.solve.m[node];
+        if (!(m > 0.f)) continue;
+        const float3 z = ld3(vec[(size_t)VZ * nodes + node]), h = ld3(vec[(size_t)VH * nodes + node]);
+        const float Az[3] = {m * z.x + c * h.x, m * z.y + c * h.y, m * z.z + c * h.z};
+        vec[(size_t)VAZ * nodes + node] = make_float4(Az[0], Az[1], Az[2], 0.f);
+        acc += (double)z.x * Az[0] + (double)z.y * Az[1] + (double)z.z * Az[2];
+    }
+    writePartial(acc, partSlot(sc, QZAZ, j));
 }
 
 // p = z + gamma p, Ap = Az + gamma Ap (gamma = 0 at j = 0), partial (Ap, M^-1 Ap).
@@ -528,56 +632,51 @@ __global__ void __launch_bounds__(kThreads) solveFinalKernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
                  int max_iter, bool split) {
-    SolveArgs a{c.scenes, b.sorted_keys, b.perm, b.cell_range, b.px, b.prep, b.T, b.ntot, parity, split ? 1 : 0};
+    SolveArgs a{c.scenes, b.sorted_keys, b.perm,  b.cell_range, b.block_range, b.px,
+                b.prep,   b.T,           b.ntot, parity,       split ? 1 : 0};
     const dim3 pgrid(c.particle_blocks, (unsigned)c.nscenes), ngrid(kSolveBlocks, (unsigned)c.nscenes);
+    const dim3 wgrid((unsigned)c.num_sms * 8, (unsigned)c.nscenes);  // warp-per-node kernels
     uint64_t launches = 0;
     cudaMemsetAsync(b.cell_range, 0, sizeof(uint2) * b.nkeys, c.stream);
+    cudaMemsetAsync(b.block_range, 0, sizeof(uint2) * b.nblocks, c.stream);
     const unsigned kb = (unsigned)std::max<size_t>(
         1, std::min<size_t>((b.ntot + kThreads - 1) / kThreads, (size_t)c.num_sms * 8));
-    cellRangeKernel<<<kb, kThreads, 0, c.stream>>>(b.sorted_keys, b.ntot, b.cell_range);
+    cellRangeKernel<<<kb, kThreads, 0, c.stream>>>(b.sorted_keys, b.ntot, b.cell_range, b.block_range);
     solvePrepKernel<<<pgrid, kThreads, 0, c.stream>>>(a);
     launches += 2;
-    auto each = [&](auto&& fn) {
+    int kk = -1;
+    auto perS = [&](auto launch) {
         for (int i = 0; i < nstencils; ++i) {
-            fn(stencils[i]);
+            switch (stencils[i]) {
+                case 2: launch(std::integral_constant<int, 2>{}); break;
+                case 3: launch(std::integral_constant<int, 3>{}); break;
+                default: launch(std::integral_constant<int, 4>{}); break;
+            }
             ++launches;
         }
     };
-#define SOLVE_S(call)                \
-    [&](int S) {                     \
-        if (S == 2) call(2);         \
-        else if (S == 3) call(3);    \
-        else call(4);                \
-    }
-#define MASS(SS) solveMassKernel<SS><<<ngrid, kThreads, 0, c.stream>>>(a)
-#define GATHER_X(SS) solveGatherKernel<SS><<<pgrid, kThreads, 0, c.stream>>>(a, VX, -1)
-#define GATHER_Z(SS) solveGatherKernel<SS><<<pgrid, kThreads, 0, c.stream>>>(a, VZ, kk)
-#define SCATTER(SS) solveScatterKernel<SS><<<ngrid, kThreads, 0, c.stream>>>(a, mode, jj, kk)
-    each(SOLVE_S(MASS));
-    int mode = SCATTER_INIT, jj = 0, kk = -1;
-    each(SOLVE_S(GATHER_X));
-    each(SOLVE_S(SCATTER));
-    mode = SCATTER_AZ;
-    each(SOLVE_S(GATHER_Z));
-    each(SOLVE_S(SCATTER));
+    auto gatherX = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, c.stream>>>(a, VX, -1); };
+    auto gatherZ = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, c.stream>>>(a, VZ, kk); };
+    auto scatter = [&](auto S) { solveScatterKernel<decltype(S)::value><<<wgrid, kThreads, 0, c.stream>>>(a, kk); };
+    solveInitKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
+    perS(gatherX);
+    perS(scatter);
+    solveResidualKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
+    perS(gatherZ);
+    perS(scatter);
+    solveAzKernel<<<ngrid, kThreads, 0, c.stream>>>(a, 0, -1);
     solveDirKernel<<<ngrid, kThreads, 0, c.stream>>>(a, 0, -1);
-    ++launches;
+    launches += 4;
     for (kk = 0; kk < max_iter; ++kk) {
-        jj = kk + 1;
         solveUpdateKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk);
-        ++launches;
-        each(SOLVE_S(GATHER_Z));
-        each(SOLVE_S(SCATTER));
-        solveDirKernel<<<ngrid, kThreads, 0, c.stream>>>(a, jj, kk);
-        ++launches;
+        perS(gatherZ);
+        perS(scatter);
+        solveAzKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk + 1, kk);
+        solveDirKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk + 1, kk);
+        launches += 3;
     }
     solveFinalKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
     ++launches;
-#undef SOLVE_S
-#undef MASS
-#undef GATHER_X
-#undef GATHER_Z
-#undef SCATTER
     noteLaunches(launches);
 }
 

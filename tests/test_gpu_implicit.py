@@ -137,3 +137,20 @@ def test_back_to_explicit(gpu):
     b.step(5)
     for f in FIELDS:
         assert np.array_equal(a.download(f), b.download(f)), f
+
+
+def test_stiff_block_at_large_dt(gpu):
+    """The stiff block that blows up explicitly (tests/test_implicit.py) stays
+    bounded with beta = 1 and follows the oracle's implicit run."""
+    from test_implicit import jelly
+    sc = jelly(n=2000)
+    g = sc.solver()
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    g.set_implicit(1.0, max_iter=100, tol=1e-6)
+    o.set_implicit(1.0, max_iter=200, tol=1e-10)
+    g.step(20)
+    o.step(20)
+    v = g.download(_abi.FIELD_VELOCITY)
+    assert np.isfinite(v).all() and np.abs(v).max() < 0.5
+    assert relerr(g.download(_abi.FIELD_POSITION), o.get(_abi.FIELD_POSITION)) < 1e-4
+    assert relerr(v, o.get(_abi.FIELD_VELOCITY)) < 1e-2

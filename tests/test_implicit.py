@@ -90,3 +90,28 @@ def test_beta_zero_is_explicit():
     before = o.grid(_abi.GRID_VELOCITY_STAR).copy()
     o.solve_linear_system(dt)
     assert np.array_equal(o.grid(_abi.GRID_VELOCITY_STAR), before)
+
+
+def jelly(dt=1e-3, n=500):
+    """A stiff elastic block (E = 1e6, plasticity limits far away) with random
+    velocities, at 5x the explicit stability limit of its 16^3 grid."""
+    sc = scenes.tiny_scene(n=n, res=16, transfer=_abi.TRANSFER_APIC, interpolation=_abi.INTERP_QUADRATIC,
+                           gravity=0.0, velocity=(0.0, 0.0, 0.0))
+    m = sc.particles.materials[0]
+    m.youngs_modulus, m.critical_compression, m.critical_stretch, m.hardening = 1e6, 0.9, 4.0, 0.0
+    sc.particles.velocities = (0.5 * np.random.default_rng(1).normal(size=(sc.n, 3))).astype(np.float32)
+    sc.dt = dt
+    return sc
+
+
+def test_implicit_is_stable_where_explicit_blows_up():
+    sc = jelly()
+    vmax = {}
+    for beta in (0.0, 1.0):
+        o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+        o.set_implicit(beta, max_iter=100, tol=1e-8)
+        o.step(40)
+        v = o.get(_abi.FIELD_VELOCITY)
+        vmax[beta] = np.abs(v).max() if np.isfinite(v).all() else np.inf
+    assert vmax[0.0] > 100.0
+    assert vmax[1.0] < 0.5

@@ -95,3 +95,22 @@ def test_cli_runs_config(gpu, scene_dir):
     assert info["particles"] == 1212 and info["steps"] == 10
     pos = np.fromfile(out, np.float32).reshape(-1, 4)
     assert pos.shape == (1212, 4) and np.all(pos[:, 3] == 1) and np.isfinite(pos).all()
+
+
+def test_cli_implicit_cfl_density(gpu, scene_dir):
+    dens = scene_dir / "density.f32"
+    r = subprocess.run([os.path.join(ROOT, "mpm_b200", "mpm-run"), str(scene_dir / "scene.yaml"), "--steps", "10",
+                        "--apic", "--integration", "implicit", "--max-iter", "30", "--cfl", "0.3",
+                        "--density", str(dens)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    assert info["particles"] == 1212 and info["steps"] == 10
+    # CFL: no step is longer than the configured 1e-3 s
+    assert 0 < info["simulated_time"] <= 10 * 1e-3 * (1 + 1e-6)
+    d = np.fromfile(dens, np.float32)
+    assert d.size == 40 ** 3 and np.isfinite(d).all() and d.min() >= 0
+    # the density grid integrates to the total particle mass (0.002 per particle)
+    assert abs(d.astype(np.float64).sum() * 5e-3 ** 3 / (1212 * 0.002) - 1) < 1e-4
+    r = subprocess.run([os.path.join(ROOT, "mpm_b200", "mpm-run"), str(scene_dir / "scene.yaml"), "--integration",
+                        "sideways"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2

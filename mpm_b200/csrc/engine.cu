@@ -736,6 +736,8 @@ public:
         MPM_TRY(solve_px_.grow(sizeof(float4) * n, "solver particle positions"));
         MPM_TRY(solve_prep_.grow(sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
         MPM_TRY(solve_T_.grow(sizeof(float4) * 3 * n, "solver particle stress differentials"));
+        MPM_TRY(solve_iter_.grow(sizeof(int), "solver iteration counter"));
+        MPM_TRY(ensureSideStreams(1));  // the loop body of a captured solve is captured on side_[0]
         return MPM_OK;
     }
     // beta > 0: every step solves (M + beta dt^2 H) v = M v* after the grid
@@ -788,12 +790,14 @@ public:
             if (s->beta > 0.f) m = std::max(m, s->solve_max_iter);
         return m;
     }
-    void launchSolveAll(bool split) {
+    mpm_status launchSolveAll(bool split) {
         SolveBuffers b{keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), cell_range_.as<uint2>(),
                        (size_t)total_blocks_ * 64, block_range_.as<uint2>(), (size_t)total_blocks_,
-                       solve_px_.as<float4>(), solve_prep_.as<float>(), solve_T_.as<float4>(), (uint32_t)ntot_};
+                       solve_px_.as<float4>(), solve_prep_.as<float>(), solve_T_.as<float4>(), (uint32_t)ntot_,
+                       solve_iter_.as<int>()};
         const std::vector<int> S = stencilSizes();
-        launchSolve(ctx(), b, parity_, S.data(), (int)S.size(), maxSolveIters(), split);
+        CUDA_TRY(launchSolve(ctx(), b, parity_, S.data(), (int)S.size(), maxSolveIters(), split, side_[0]));
+        return MPM_OK;
     }
     // Split API: solveLinearSystem(dt) on the split-mode grid (v* of
     // updateGridVelocities / gridCollision), no collision after.
@@ -805,8 +809,7 @@ public:
         std::vector<SceneDev> saved = host_scenes_;
         for (auto& d : host_scenes_) d.dt = dt;
         MPM_TRY(uploadSceneTable());
-        launchSolveAll(true);
-        CUDA_TRY(cudaGetLastError());
+        MPM_TRY(launchSolveAll(true));
         host_scenes_ = saved;
         MPM_TRY(uploadSceneTable());
         return MPM_OK;
@@ -1126,7 +1129,7 @@ public:
             mark(KF_GRID, 0);
             for (auto& k : cs)
                 launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
-            if (any_implicit_) launchSolveAll(false);
+            if (any_implicit_) MPM_TRY(launchSolveAll(false));
             mark(KF_GRID, 1);
             collect(KF_GRID);
             mark(KF_G2P, 0);
@@ -1629,7 +1632,7 @@ private:
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     bool any_cfl_ = false;     // some scene steps with a CFL dt (two more launches per step)
     bool any_implicit_ = false;  // some scene solves the semi-implicit update
-    DevMem cell_range_, block_range_, solve_px_, solve_prep_, solve_T_;
+    DevMem cell_range_, block_range_, solve_px_, solve_prep_, solve_T_, solve_iter_;
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order

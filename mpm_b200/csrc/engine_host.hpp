@@ -87,6 +87,7 @@ struct SolveBuffers {
     float* prep;                  // kSolvePrepPlanes x ntot
     float4* T;                    // 3 x ntot: V0 dP Fe^T rows
     uint32_t ntot;
+    int* iter;                    // device iteration counter
 };
 constexpr int kSolvePrepPlanes = 44;
 constexpr int kSolveVectors = 7;
@@ -94,8 +95,10 @@ constexpr int kSolveBlocks = 512;  // node-kernel blocks per scene = partial sum
 inline size_t solvePartialDoubles(int max_iter) { return (size_t)4 * (size_t)(max_iter + 2) * kSolveBlocks; }
 // split: v* from and to the split-mode dense planes (no collision after);
 // else from and to the fused step's v* grid, with the grid collision after.
-void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
-                 int max_iter, bool split);
+// aux: an idle stream on which, inside a stream capture, the iteration body
+// is captured as the body of a conditional while node.
+cudaError_t launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
+                        int max_iter, bool split, cudaStream_t aux);
 
 // CFL time step of the scenes with cfl > 0: max |v|^2 over their live
 // particles, then dt = min(dt_max, cfl h / max|v|) into the scene table.

@@ -61,6 +61,7 @@ struct SolveArgs {
     uint32_t ntot;
     int parity;
     int split;
+    int* iter;  // device iteration counter of the loop
 };
 
 // Prep planes (stride ntot): F 0..8, U 9..17, V 18..26, s 27..29, cof F
@@ -361,8 +362,9 @@ __global__ void __launch_bounds__(kThreads) solveInitKernel(SolveArgs a) {
 }
 
 template <int S>
-__global__ void __launch_bounds__(kThreads) solveGatherKernel(SolveArgs a, int src, int k) {
+__global__ void __launch_bounds__(kThreads) solveGatherKernel(SolveArgs a, int src, const int* kp, int k0) {
     const SceneDev& sc = a.scenes[blockIdx.y];
+    const int k = kp ? *kp : k0;
     if (!solving(sc) || sc.S != S || blockDoneAt(sc) <= k) return;
     const size_t nodes = sceneNodes(sc), st = a.ntot;
     const float4* u = sc.solve.vec + (size_t)src * nodes;
@@ -468,8 +470,9 @@ __global__ void __launch_bounds__(kThreads) solveGatherKernel(SolveArgs a, int s
 
 // h = sum_p T_p grad w_ip at the listed nodes (one warp per node).
 template <int S>
-__global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, int k) {
+__global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, const int* kp, int k0) {
     const SceneDev& sc = a.scenes[blockIdx.y];
+    const int k = kp ? *kp : k0;
     if (!solving(sc) || sc.S != S || blockDoneAt(sc) <= k) return;
     __shared__ int sh[kThreads / 32][2 * S * S * S + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -519,8 +522,9 @@ __global__ void __launch_bounds__(kThreads) solveResidualKernel(SolveArgs a) {
 }
 
 // Az = M z + c H z, (z, Az) into slot j.
-__global__ void __launch_bounds__(kThreads) solveAzKernel(SolveArgs a, int j, int k) {
+__global__ void __launch_bounds__(kThreads) solveAzKernel(SolveArgs a, const int* kp, int j0, int k0) {
     const SceneDev& sc = a.scenes[blockIdx.y];
+    const int k = kp ? *kp : k0, j = kp ? k + 1 : j0;
     if (!solving(sc) || blockDoneAt(sc) <= k) return;
     const size_t nodes = sceneNodes(sc);
     float4* vec = sc.solve.vec;
@@ -539,8 +543,9 @@ __global__ void __launch_bounds__(kThreads) solveAzKernel(SolveArgs a, int j, in
 }
 
 // p = z + gamma p, Ap = Az + gamma Ap (gamma = 0 at j = 0), partial (Ap, M^-1 Ap).
-__global__ void __launch_bounds__(kThreads) solveDirKernel(SolveArgs a, int j, int k) {
+__global__ void __launch_bounds__(kThreads) solveDirKernel(SolveArgs a, const int* kp, int j0, int k0) {
     const SceneDev& sc = a.scenes[blockIdx.y];
+    const int k = kp ? *kp : k0, j = kp ? k + 1 : j0;
     if (!solving(sc) || blockDoneAt(sc) <= k) return;
     const size_t nodes = sceneNodes(sc);
     float4* vec = sc.solve.vec;
@@ -563,8 +568,9 @@ __global__ void __launch_bounds__(kThreads) solveDirKernel(SolveArgs a, int j, i
 }
 
 // Iteration k: convergence test, then x += alpha p, r -= alpha Ap, z -= alpha M^-1 Ap.
-__global__ void __launch_bounds__(kThreads) solveUpdateKernel(SolveArgs a, int k) {
+__global__ void __launch_bounds__(kThreads) solveUpdateKernel(SolveArgs a, const int* kp) {
     const SceneDev& sc = a.scenes[blockIdx.y];
+    const int k = *kp;
     if (!solving(sc) || blockDoneAt(sc) <= k) return;
     bool done = k >= sc.solve_max_iter;
     double zAz = 0.0, Apq = 0.0;
@@ -600,6 +606,23 @@ __global__ void __launch_bounds__(kThreads) solveUpdateKernel(SolveArgs a, int k
     writePartial(acc, partSlot(sc, QRR, k + 1));
 }
 
+// End of iteration k: is any scene still iterating (not converged by the
+// test of iteration k, k + 1 < its max_iter)?  Advances the counter and, in a
+// graph, sets the condition of the loop node.
+__global__ void solveCondKernel(SolveArgs a, int nscenes, cudaGraphConditionalHandle h, int use_cond) {
+    const int k = *a.iter;
+    int running = 0;
+    for (int i = threadIdx.x; i < nscenes; i += blockDim.x) {
+        const SceneDev& sc = a.scenes[i];
+        if (solving(sc) && sc.solve.status->done_at > k && k + 1 < sc.solve_max_iter) running = 1;
+    }
+    running = __syncthreads_or(running);
+    if (threadIdx.x == 0) {
+        *a.iter = k + 1;
+        if (use_cond) cudaGraphSetConditional(h, running ? 1u : 0u);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) solveFinalKernel(SolveArgs a) {
     const SceneDev& sc = a.scenes[blockIdx.y];
     if (!solving(sc)) return;
@@ -630,10 +653,10 @@ __global__ void __launch_bounds__(kThreads) solveFinalKernel(SolveArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
-                 int max_iter, bool split) {
-    SolveArgs a{c.scenes, b.sorted_keys, b.perm,  b.cell_range, b.block_range, b.px,
-                b.prep,   b.T,           b.ntot, parity,       split ? 1 : 0};
+cudaError_t launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
+                        int max_iter, bool split, cudaStream_t aux) {
+    SolveArgs a{c.scenes, b.sorted_keys, b.perm, b.cell_range, b.block_range, b.px, b.prep, b.T, b.ntot, parity,
+                split ? 1 : 0, b.iter};
     const dim3 pgrid(c.particle_blocks, (unsigned)c.nscenes), ngrid(kSolveBlocks, (unsigned)c.nscenes);
     const dim3 wgrid((unsigned)c.num_sms * 8, (unsigned)c.nscenes);  // warp-per-node kernels
     uint64_t launches = 0;
@@ -644,7 +667,6 @@ void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const in
     cellRangeKernel<<<kb, kThreads, 0, c.stream>>>(b.sorted_keys, b.ntot, b.cell_range, b.block_range);
     solvePrepKernel<<<pgrid, kThreads, 0, c.stream>>>(a);
     launches += 2;
-    int kk = -1;
     auto perS = [&](auto launch) {
         for (int i = 0; i < nstencils; ++i) {
             switch (stencils[i]) {
@@ -655,29 +677,70 @@ void launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const in
             ++launches;
         }
     };
-    auto gatherX = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, c.stream>>>(a, VX, -1); };
-    auto gatherZ = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, c.stream>>>(a, VZ, kk); };
-    auto scatter = [&](auto S) { solveScatterKernel<decltype(S)::value><<<wgrid, kThreads, 0, c.stream>>>(a, kk); };
-    solveInitKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
+    cudaStream_t st = c.stream;  // the stream of the iteration kernels
+    const int* kp = nullptr;
+    auto gatherX = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, st>>>(a, VX, nullptr, -1); };
+    auto gatherZ = [&](auto S) { solveGatherKernel<decltype(S)::value><<<pgrid, kThreads, 0, st>>>(a, VZ, kp, -1); };
+    auto scatter = [&](auto S) { solveScatterKernel<decltype(S)::value><<<wgrid, kThreads, 0, st>>>(a, kp, -1); };
+    solveInitKernel<<<ngrid, kThreads, 0, st>>>(a);
     perS(gatherX);
     perS(scatter);
-    solveResidualKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
+    solveResidualKernel<<<ngrid, kThreads, 0, st>>>(a);
     perS(gatherZ);
     perS(scatter);
-    solveAzKernel<<<ngrid, kThreads, 0, c.stream>>>(a, 0, -1);
-    solveDirKernel<<<ngrid, kThreads, 0, c.stream>>>(a, 0, -1);
+    solveAzKernel<<<ngrid, kThreads, 0, st>>>(a, nullptr, 0, -1);
+    solveDirKernel<<<ngrid, kThreads, 0, st>>>(a, nullptr, 0, -1);
+    cudaMemsetAsync(b.iter, 0, sizeof(int), st);
     launches += 4;
-    for (kk = 0; kk < max_iter; ++kk) {
-        solveUpdateKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk);
+    kp = b.iter;
+    auto body = [&](cudaGraphConditionalHandle h, int use_cond) {
+        solveUpdateKernel<<<ngrid, kThreads, 0, st>>>(a, kp);
         perS(gatherZ);
         perS(scatter);
-        solveAzKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk + 1, kk);
-        solveDirKernel<<<ngrid, kThreads, 0, c.stream>>>(a, kk + 1, kk);
-        launches += 3;
+        solveAzKernel<<<ngrid, kThreads, 0, st>>>(a, kp, 0, 0);
+        solveDirKernel<<<ngrid, kThreads, 0, st>>>(a, kp, 0, 0);
+        solveCondKernel<<<1, kThreads, 0, st>>>(a, c.nscenes, h, use_cond);
+        launches += 4;
+    };
+    // Inside a stream capture the iterations become a conditional while node
+    // (the body captured once on the auxiliary stream), so a converged solve
+    // launches nothing more; direct launches run max_iter bodies, whose
+    // kernels return at once after convergence.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(c.stream, &cs);
+    if (e != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusActive && aux) {
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        if ((e = cudaStreamGetCaptureInfo(c.stream, &cs, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+        cudaGraphConditionalHandle h;
+        if ((e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        if ((e = cudaGraphAddNode(&node, g, deps, nd, &p)) != cudaSuccess) return e;
+        cudaGraph_t bg = p.conditional.phGraph_out[0];
+        if ((e = cudaStreamBeginCaptureToGraph(aux, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess)
+            return e;
+        st = aux;
+        body(h, 1);
+        st = c.stream;
+        if ((e = cudaStreamEndCapture(aux, &bg)) != cudaSuccess) return e;
+        if ((e = cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies)) !=
+            cudaSuccess)
+            return e;
+    } else {
+        for (int it = 0; it < max_iter; ++it) body(0, 0);
     }
     solveFinalKernel<<<ngrid, kThreads, 0, c.stream>>>(a);
     ++launches;
     noteLaunches(launches);
+    return cudaGetLastError();
 }
 
 }  // namespace mpm

@@ -108,7 +108,8 @@ def test_cli_implicit_cfl_density(gpu, scene_dir):
     # CFL: no step is longer than the configured 1e-3 s
     assert 0 < info["simulated_time"] <= 10 * 1e-3 * (1 + 1e-6)
     d = np.fromfile(dens, np.float32)
-    assert d.size == 40 ** 3 and np.isfinite(d).all() and d.min() >= 0
+    # (a weight at the edge of the cubic stencil can round to -0 ... -1e-16)
+    assert d.size == 40 ** 3 and np.isfinite(d).all() and d.min() > -1e-6 * d.max()
     # the density grid integrates to the total particle mass (0.002 per particle)
     assert abs(d.astype(np.float64).sum() * 5e-3 ** 3 / (1212 * 0.002) - 1) < 1e-4
     r = subprocess.run([os.path.join(ROOT, "mpm_b200", "mpm-run"), str(scene_dir / "scene.yaml"), "--integration",

@@ -742,7 +742,7 @@ public:
         const size_t n = std::max<size_t>(ntot_, 1);
         MPM_TRY(cell_range_.grow(sizeof(uint2) * (size_t)total_blocks_ * 64, "solver cell ranges"));
         MPM_TRY(block_range_.grow(sizeof(uint2) * (size_t)total_blocks_, "solver block ranges"));
-        MPM_TRY(solve_px_.grow(sizeof(float4) * n, "solver particle positions"));
+        MPM_TRY(solve_pofs_.grow(sizeof(float4) * n, "solver stencil offsets"));
         MPM_TRY(solve_prep_.grow(sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
         MPM_TRY(solve_T_.grow(sizeof(float4) * 3 * n, "solver particle stress differentials"));
         MPM_TRY(solve_iter_.grow(sizeof(int), "solver iteration counter"));
@@ -802,7 +802,7 @@ public:
     mpm_status launchSolveAll(bool split) {
         SolveBuffers b{keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), cell_range_.as<uint2>(),
                        (size_t)total_blocks_ * 64, block_range_.as<uint2>(), (size_t)total_blocks_,
-                       solve_px_.as<float4>(), solve_prep_.as<float>(), solve_T_.as<float4>(), (uint32_t)ntot_,
+                       solve_pofs_.as<float4>(), solve_prep_.as<float>(), solve_T_.as<float4>(), (uint32_t)ntot_,
                        solve_iter_.as<int>()};
         const std::vector<int> S = stencilSizes();
         CUDA_TRY(launchSolve(ctx(), b, parity_, S.data(), (int)S.size(), maxSolveIters(), split, side_[0]));
@@ -1666,7 +1666,7 @@ private:
     bool dirty_ = true, keys_valid_ = false, sorted_valid_ = false;
     bool any_cfl_ = false;     // some scene steps with a CFL dt (two more launches per step)
     bool any_implicit_ = false;  // some scene solves the semi-implicit update
-    DevMem cell_range_, block_range_, solve_px_, solve_prep_, solve_T_, solve_iter_;
+    DevMem cell_range_, block_range_, solve_pofs_, solve_prep_, solve_T_, solve_iter_;
     int p2g_stage_ = 32;       // see checkP2GStage()
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order

@@ -83,7 +83,7 @@ struct SolveBuffers {
     size_t nkeys;
     uint2* block_range;           // nblocks: the same per 4^3 block of cells (key >> 6)
     size_t nblocks;
-    float4* px;                   // ntot: position, mass (sorted order)
+    float4* pofs;                 // ntot: stencil offsets (x - (o + h base)) / h (sorted order)
     float* prep;                  // kSolvePrepPlanes x ntot
     float4* T;                    // 3 x ntot: V0 dP Fe^T rows
     uint32_t ntot;

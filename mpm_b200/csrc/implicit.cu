@@ -11,7 +11,8 @@
 //   cellRangeKernel    first and end sorted position of every cell key and
 //                      of every 4^3 block of cells
 //   solvePrepKernel    per sorted particle: Fe, its SVD, cofactor, J, ln J,
-//                      V0 mu and V0 la (hardened), model; position and mass
+//                      V0 mu and V0 la (hardened), model; the offsets
+//                      (x - (o + h base)) / h of its stencil
 //   solveInitKernel    node masses (the transfer's), x0 = v*, the other
 //                      vectors 0, |M v*|^2, list of the nodes with mass
 //   solveGatherKernel  per particle: G = sum_j u_j grad w^T, T = V0 dP(G Fe) Fe^T
@@ -55,7 +56,7 @@ struct SolveArgs {
     const uint32_t* perm;
     const uint2* cell_range;
     const uint2* block_range;
-    float4* px;
+    float4* pofs;  // per sorted particle: stencil offsets d0 (xyz)
     float* prep;
     float4* T;
     uint32_t ntot;
@@ -115,17 +116,24 @@ __device__ __forceinline__ void nodeCoords(const SceneDev& sc, size_t node, int*
 }
 __device__ __forceinline__ float3 ld3(const float4& v) { return make_float3(v.x, v.y, v.z); }
 
-// Weight and gradient (per cell) of node base + k for a particle at x.
+// Weight and gradient of stencil node k of a particle with stencil offsets
+// d0 = (x - (o + h base)) / h (the distance is d0 - k, as in G2P).
 template <int S>
-__device__ __forceinline__ void nodeWeight(const SceneDev& sc, const float* x, const int* base, const int* k,
-                                           float* w, float* dw) {
+__device__ __forceinline__ void nodeWeight(const SceneDev& sc, const float4& d0, const int* k, float* w, float* dw) {
+    const float d[3] = {d0.x - (float)k[0], d0.y - (float)k[1], d0.z - (float)k[2]};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(sc.h, (float)base[a]));
-        const float d = __fdiv_rn(x[a] - gp0, sc.h) - (float)k[a];
-        w[a] = splineN<S>(d);
-        dw[a] = splineNDot<S>(d) * sc.inv_h;
+        w[a] = splineN<S>(d[a]);
+        dw[a] = splineNDot<S>(d[a]) * sc.inv_h;
     }
+}
+// Stencil base of a particle from its cell key (key = block << 6 | cell,
+// base + 4 = 4 block + cell per axis).
+__device__ __forceinline__ void keyBase(const SceneDev& sc, uint32_t key, int* base) {
+    const uint32_t lb = (key >> 6) - sc.block_base, c = key & 63u;
+    base[0] = 4 * (int)(lb % (uint32_t)sc.nb[0]) - 4 + (int)(c & 3u);
+    base[1] = 4 * (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]) - 4 + (int)((c >> 2) & 3u);
+    base[2] = 4 * (int)(lb / ((uint32_t)sc.nb[0] * sc.nb[1])) - 4 + (int)(c >> 4);
 }
 
 // Sum fn(p, base, k) over the particles whose stencil covers node n, by one
@@ -302,8 +310,16 @@ __global__ void __launch_bounds__(kThreads) solvePrepKernel(SolveArgs a) {
         p[(size_t)PMU * st] = V0 * mu;
         p[(size_t)PLA * st] = V0 * la;
         p[(size_t)PMODEL * st] = (float)md.model;
-        a.px[i] = make_float4(f[(size_t)(F_X + 0) * cap + slot], f[(size_t)(F_X + 1) * cap + slot],
-                              f[(size_t)(F_X + 2) * cap + slot], f[(size_t)F_MASS * cap + slot]);
+        const float x[3] = {f[(size_t)(F_X + 0) * cap + slot], f[(size_t)(F_X + 1) * cap + slot],
+                            f[(size_t)(F_X + 2) * cap + slot]};
+        int base[3];
+        float d0[3] = {0.f, 0.f, 0.f};
+        if (stencilBase(sc, x, base)) {  // else an outside particle: no stencil
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax)
+                d0[ax] = __fdiv_rn(x[ax] - __fadd_rn(sc.origin[ax], __fmul_rn(sc.h, (float)base[ax])), sc.h);
+        }
+        a.pofs[i] = make_float4(d0[0], d0[1], d0[2], 0.f);
     }
 }
 
@@ -372,19 +388,20 @@ __global__ void __launch_bounds__(kThreads) solveGatherKernel(SolveArgs a, int s
     for (uint32_t j = blockIdx.x * kThreads + threadIdx.x; j < sc.n; j += gridDim.x * kThreads) {
         const size_t i = (size_t)sc.key_offset + j;
         float4* To = a.T + 3 * i;
-        const float4 q = a.px[i];
-        const float x[3] = {q.x, q.y, q.z};
-        int base[3];
-        if ((a.sorted_keys[i] >> 6) >= outside || !stencilBase(sc, x, base)) {
+        const uint32_t key = a.sorted_keys[i];
+        if ((key >> 6) >= outside) {
             To[0] = To[1] = To[2] = make_float4(0.f, 0.f, 0.f, 0.f);
             continue;
         }
+        int base[3];
+        keyBase(sc, key, base);
+        const float4 q = a.pofs[i];
+        const float d0[3] = {q.x, q.y, q.z};
         float w[3][S], dw[3][S];
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-            const float gp0 = __fadd_rn(sc.origin[ax], __fmul_rn(sc.h, (float)base[ax]));
             float dk[S];
-            dk[0] = __fdiv_rn(x[ax] - gp0, sc.h);
+            dk[0] = d0[ax];
 #pragma unroll
             for (int kk = 1; kk < S; ++kk) dk[kk] = dk[0] - (float)kk;
             splineWeights<S>(dk, w[ax], dw[ax]);
@@ -485,10 +502,8 @@ __global__ void __launch_bounds__(kThreads) solveScatterKernel(SolveArgs a, cons
         nodeCoords(sc, node, n);
         float out[3];
         warpNodeSum<S, 3>(sc, a, n, sh[warp], out, [&](uint32_t p, const int* base, const int* kk, float* acc) {
-            const float4 q = a.px[p];
-            const float x[3] = {q.x, q.y, q.z};
             float w[3], dw[3];
-            nodeWeight<S>(sc, x, base, kk, w, dw);
+            nodeWeight<S>(sc, a.pofs[p], kk, w, dw);
             const float g[3] = {dw[0] * w[1] * w[2], w[0] * dw[1] * w[2], w[0] * w[1] * dw[2]};
             const float4* Tp = a.T + 3 * (size_t)p;
             const float4 t0 = Tp[0], t1 = Tp[1], t2 = Tp[2];
@@ -655,7 +670,7 @@ __global__ void __launch_bounds__(kThreads) solveFinalKernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 cudaError_t launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, const int* stencils, int nstencils,
                         int max_iter, bool split, cudaStream_t aux) {
-    SolveArgs a{c.scenes, b.sorted_keys, b.perm, b.cell_range, b.block_range, b.px, b.prep, b.T, b.ntot, parity,
+    SolveArgs a{c.scenes, b.sorted_keys, b.perm, b.cell_range, b.block_range, b.pofs, b.prep, b.T, b.ntot, parity,
                 split ? 1 : 0, b.iter};
     const dim3 pgrid(c.particle_blocks, (unsigned)c.nscenes), ngrid(kSolveBlocks, (unsigned)c.nscenes);
     const dim3 wgrid((unsigned)c.num_sms * 8, (unsigned)c.nscenes);  // warp-per-node kernels

@@ -728,19 +728,38 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
             float acc[F];
 #pragma unroll
             for (int f = 0; f < F; ++f) acc[f] = 0.f;
+            // The 8 tiles that overlap the node, in order e, and within each
+            // every work item of that block in item order.  The first item's
+            // values of Q tiles are loaded together (independent loads in
+            // flight), then summed in the same order as one by one.
+            constexpr int Q = F <= 4 ? 4 : 2;
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int de[3] = {e & 1, (e >> 1) & 1, (e >> 2) & 1};
-                const int ix = L[0] + 4 * de[0], iy = L[1] + 4 * de[1], iz = L[2] + 4 * de[2];
-                if (ix >= T || iy >= T || iz >= T) continue;
-                const int nbi = (dd[0] - de[0] + 1) + 3 * (dd[1] - de[1] + 1) + 9 * (dd[2] - de[2] + 1);
-                const int slot = nbSlot[nbi];
-                if (slot < 0) continue;
-                // every work item (tile) of that block, in item order
-                for (uint32_t s2 = (uint32_t)slot; s2 < (uint32_t)(slot + nbItems[nbi]); ++s2) {
-                    const float* tile = args.tiles + (size_t)s2 * args.tile_stride + ix + T * (iy + T * iz);
+            for (int hq = 0; hq < 8 / Q; ++hq) {
+                float v[Q][F];
+                const float* tp[Q];
+                int cnt[Q];
 #pragma unroll
-                    for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+                for (int q = 0; q < Q; ++q) {
+                    const int e = Q * hq + q;
+                    const int de[3] = {e & 1, (e >> 1) & 1, (e >> 2) & 1};
+                    const int ix = L[0] + 4 * de[0], iy = L[1] + 4 * de[1], iz = L[2] + 4 * de[2];
+                    const int nbi = (dd[0] - de[0] + 1) + 3 * (dd[1] - de[1] + 1) + 9 * (dd[2] - de[2] + 1);
+                    const int slot = (ix < T && iy < T && iz < T) ? nbSlot[nbi] : -1;
+                    cnt[q] = slot >= 0 ? nbItems[nbi] : 0;
+                    tp[q] = args.tiles + (size_t)(slot >= 0 ? slot : 0) * args.tile_stride + ix + T * (iy + T * iz);
+#pragma unroll
+                    for (int f = 0; f < F; ++f) v[q][f] = cnt[q] > 0 ? tp[q][f * TN] : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    if (cnt[q] <= 0) continue;
+#pragma unroll
+                    for (int f = 0; f < F; ++f) acc[f] += v[q][f];
+                    for (int s2 = 1; s2 < cnt[q]; ++s2) {
+                        const float* tile = tp[q] + (size_t)s2 * args.tile_stride;
+#pragma unroll
+                        for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+                    }
                 }
             }
             const size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);

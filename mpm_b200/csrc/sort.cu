@@ -477,67 +477,87 @@ constexpr int kPartTile = kThreads * kPartItems;     // 2048
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;   // outputs per CTA
 
+// One tile of kPartTile keys: item j * kThreads + threadIdx.x of the tile is
+// this thread's j-th (coalesced loads and stores).  A key is a mover if it
+// differs from the previous step's key at the same position.  Movers keep
+// their order in b, stayers in a: the rank of an item among the movers of
+// its tile comes from per-warp ballots and one scan over (round, warp) in
+// item order, the tile's offset from the decoupled look-back.
 __global__ void __launch_bounds__(kThreads) moverPartitionKernel(
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ prev, uint32_t n, uint32_t* __restrict__ a_keys,
     uint32_t* __restrict__ a_idx, uint32_t* __restrict__ b_keys, uint32_t* __restrict__ b_idx,
     uint32_t* __restrict__ m_out, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t ntiles,
     uint32_t* __restrict__ err) {
-    __shared__ uint32_t tile_s, excl_s, tot_s;
+    constexpr int kW = kThreads / 32;
+    __shared__ uint32_t tile_s, excl_s;
+    __shared__ uint32_t wcnt[kPartItems * kW];  // movers per (round, warp), then their exclusive scan
     if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint32_t tile = tile_s;
-    const size_t i0 = (size_t)tile * kPartTile + (size_t)threadIdx.x * kPartItems;
-    uint32_t k[kPartItems];
-    uint32_t movers = 0, mvmask = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t t0 = (size_t)tile * kPartTile;
+    uint32_t k[kPartItems], ball[kPartItems];
 #pragma unroll
     for (int j = 0; j < kPartItems; ++j) {
-        const size_t i = i0 + j;
+        const size_t i = t0 + (size_t)j * kThreads + threadIdx.x;
         const bool valid = i < n;
         k[j] = valid ? keys[i] : 0u;
         const uint32_t pk = valid ? prev[i] : 0u;
-        const bool mv = valid && k[j] != pk;
-        mvmask |= (mv ? 1u : 0u) << j;
-        movers += mv ? 1u : 0u;
-    }
-    const uint32_t before = blockExclusiveScan(movers, &tot_s);  // movers of earlier threads of the tile
-    if (threadIdx.x == 0) {
-        uint32_t excl = 0;
-        if (tile == 0) {
-            atomicExch(&status[0], kFlagPrefix | tot_s);
-        } else {
-            atomicExch(&status[tile], kFlagAgg | tot_s);
-            int t = (int)tile - 1;
-            int polls = 0;
-            while (t >= 0) {
-                const uint32_t w = *(volatile const uint32_t*)(status + t);
-                const uint32_t f = w & ~kCountMask;
-                if (f == 0) {
-                    if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
-                        atomicOr(err, 8u);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                excl += w & kCountMask;
-                if (f == kFlagPrefix) break;
-                --t;
-            }
-            atomicExch(&status[tile], kFlagPrefix | (excl + tot_s));
-        }
-        excl_s = excl;
-        if (tile == ntiles - 1) *m_out = excl + tot_s;
+        ball[j] = __ballot_sync(0xffffffffu, valid && k[j] != pk);
+        if (lane == 0) wcnt[j * kW + warp] = (uint32_t)__popc(ball[j]);
     }
     __syncthreads();
-    uint32_t mb = excl_s + before;  // movers before the current key
+    if (warp == 0) {  // exclusive scan of the kPartItems * kW counts, in item order
+        static_assert(kPartItems * kW == 64, "two counts per lane");
+        const uint32_t c0 = wcnt[2 * lane], c1 = wcnt[2 * lane + 1];
+        uint32_t x = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+        wcnt[2 * lane] = x - c0 - c1;
+        wcnt[2 * lane + 1] = x - c1;
+        if (lane == 0) {
+            uint32_t excl = 0;
+            if (tile == 0) {
+                atomicExch(&status[0], kFlagPrefix | tot);
+            } else {
+                atomicExch(&status[tile], kFlagAgg | tot);
+                int t = (int)tile - 1;
+                int polls = 0;
+                while (t >= 0) {
+                    const uint32_t w = *(volatile const uint32_t*)(status + t);
+                    const uint32_t f = w & ~kCountMask;
+                    if (f == 0) {
+                        if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
+                            atomicOr(err, 8u);
+                            break;
+                        }
+                        __nanosleep(32);
+                        continue;
+                    }
+                    excl += w & kCountMask;
+                    if (f == kFlagPrefix) break;
+                    --t;
+                }
+                atomicExch(&status[tile], kFlagPrefix | (excl + tot));
+            }
+            excl_s = excl;
+            if (tile == ntiles - 1) *m_out = excl + tot;
+        }
+    }
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int j = 0; j < kPartItems; ++j) {
-        const size_t i = i0 + j;
+        const size_t i = t0 + (size_t)j * kThreads + threadIdx.x;
         if (i >= n) break;
-        if (mvmask >> j & 1u) {
+        const uint32_t mb = excl_s + wcnt[j * kW + warp] + (uint32_t)__popc(ball[j] & lt);  // movers before it
+        if (ball[j] >> lane & 1u) {
             b_keys[mb] = k[j];
             b_idx[mb] = (uint32_t)i;
-            ++mb;
         } else {
             const uint32_t pa = (uint32_t)i - mb;  // stayers before it
             a_keys[pa] = k[j];
@@ -578,7 +598,8 @@ __global__ void __launch_bounds__(kThreads) mergeSplitKernel(const uint32_t* __r
 }
 
 // One CTA merges kMergeTile outputs: its stayer and mover ranges are staged in
-// shared memory, each thread finds its own split there and merges 8 outputs.
+// shared memory, each thread finds its own split there and merges 8 outputs
+// into a shared output tile, which the CTA then stores with unit stride.
 __global__ void __launch_bounds__(kThreads) mergeKernel(const uint32_t* __restrict__ a_keys,
                                                          const uint32_t* __restrict__ a_idx,
                                                          const uint32_t* __restrict__ b_keys,
@@ -588,7 +609,7 @@ __global__ void __launch_bounds__(kThreads) mergeKernel(const uint32_t* __restri
                                                          uint32_t* __restrict__ out_keys,
                                                          uint32_t* __restrict__ out_perm) {
     __shared__ unsigned long long sa[kMergeTile], sb[kMergeTile];
-    const uint32_t m = *m_dev, na = n - m;
+    __shared__ uint32_t ok[kMergeTile], op[kMergeTile];
     const uint32_t d0 = blockIdx.x * kMergeTile;
     if (d0 >= n) return;
     const uint32_t d1 = min(n, d0 + (uint32_t)kMergeTile);
@@ -599,22 +620,28 @@ __global__ void __launch_bounds__(kThreads) mergeKernel(const uint32_t* __restri
     for (uint32_t i = threadIdx.x; i < lb; i += kThreads) sb[i] = composite(b_keys[b0 + i], b_idx[b0 + i]);
     __syncthreads();
     const uint32_t dl = threadIdx.x * kMergeItems;
-    if (dl >= la + lb) return;
-    uint32_t lo = dl > lb ? dl - lb : 0u, hi = dl < la ? dl : la;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (sa[mid] < sb[dl - 1 - mid]) lo = mid + 1;
-        else hi = mid;
+    if (dl < la + lb) {
+        uint32_t lo = dl > lb ? dl - lb : 0u, hi = dl < la ? dl : la;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sa[mid] < sb[dl - 1 - mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        uint32_t ia = lo, ib = dl - lo;
+        const uint32_t dend = min(dl + (uint32_t)kMergeItems, la + lb);
+        for (uint32_t dd = dl; dd < dend; ++dd) {
+            const bool takeA = ib >= lb || (ia < la && sa[ia] < sb[ib]);
+            const unsigned long long v = takeA ? sa[ia++] : sb[ib++];
+            ok[dd] = (uint32_t)(v >> 32);
+            op[dd] = (uint32_t)v;
+        }
     }
-    uint32_t ia = lo, ib = dl - lo;
-    const uint32_t dend = min(dl + (uint32_t)kMergeItems, la + lb);
-    for (uint32_t dd = dl; dd < dend; ++dd) {
-        const bool takeA = ib >= lb || (ia < la && sa[ia] < sb[ib]);
-        const unsigned long long v = takeA ? sa[ia++] : sb[ib++];
-        out_keys[d0 + dd] = (uint32_t)(v >> 32);
-        out_perm[d0 + dd] = (uint32_t)v;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < la + lb; i += kThreads) {
+        out_keys[d0 + i] = ok[i];
+        out_perm[d0 + i] = op[i];
     }
-    (void)na;
+    (void)m_dev;
 }
 
 }  // namespace

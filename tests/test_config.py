@@ -161,6 +161,18 @@ int main(int argc, char**) {
                           chains::InterpolationType::QUADRATIC_BSPLINE, 1e-4f);
     s.simulateOneStep();
     s.switchIfEnableParticlesCollision();
+    chains::LevelSetCollisionObject3D obj;
+    obj.level_set.assign(16 * 16 * 16, 1.f);
+    obj.friction = 0.3f;
+    s.setCollisionObject(obj);
+    s.clearCollisionObject();
+    s.setCfl(0.4f);
+    s.setIntegrationType(chains::IntegrationType::SEMI_IMPLICIT, 20, 1e-5f);
+    s.solveLinearSystem(1e-4f);
+    std::vector<float> rho = s.density();
+    double t = s.simulatedTime();
+    (void)rho;
+    (void)t;
     int n = 0;
     auto cfg = chains::parseYAML("x.yaml");
     chains::APICMPMSolver3D a = chains::buildAPICMPMSolver3DFromYAML(cfg, n);

@@ -208,22 +208,35 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
             atomicExch(&status[0], kCFlagPrefix | tot);
         } else {
             atomicExch(&status[tile], kCFlagAgg | tot);
+            // 8 predecessor words per round trip (independent loads)
             int t = (int)tile - 1;
             int polls = 0;
-            while (t >= 0) {
-                const unsigned long long w = *(volatile const unsigned long long*)(status + t);
-                const unsigned long long f = w & kCFlagMask;
-                if (f == 0) {
+            bool done = false;
+            while (!done && t >= 0) {
+                unsigned long long w[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    w[q] = (t - q >= 0) ? *(volatile const unsigned long long*)(status + (t - q)) : kCFlagPrefix;
+                bool waiting = false;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (done || waiting) continue;
+                    const unsigned long long f = w[q] & kCFlagMask;
+                    if (f == 0) {  // not published yet: poll again from this tile
+                        waiting = true;
+                        continue;
+                    }
+                    excl += w[q] & ~kCFlagMask;
+                    --t;
+                    if (f == kCFlagPrefix) done = true;
+                }
+                if (waiting) {
                     if (++polls > (1 << 22)) {  // never expected: give up instead of hanging
                         atomicOr(err, 16u);
                         break;
                     }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += w & ~kCFlagMask;
-                if (f == kCFlagPrefix) break;
-                --t;
             }
             atomicExch(&status[tile], kCFlagPrefix | (excl + tot));
         }

@@ -525,22 +525,35 @@ __global__ void __launch_bounds__(kThreads) moverPartitionKernel(
                 atomicExch(&status[0], kFlagPrefix | tot);
             } else {
                 atomicExch(&status[tile], kFlagAgg | tot);
+                // kLookWidth predecessor words per round trip, as in the radix passes
                 int t = (int)tile - 1;
                 int polls = 0;
-                while (t >= 0) {
-                    const uint32_t w = *(volatile const uint32_t*)(status + t);
-                    const uint32_t f = w & ~kCountMask;
-                    if (f == 0) {
+                bool done = false;
+                while (!done && t >= 0) {
+                    uint32_t w[kLookWidth];
+#pragma unroll
+                    for (int q = 0; q < kLookWidth; ++q)
+                        w[q] = (t - q >= 0) ? *(volatile const uint32_t*)(status + (t - q)) : kFlagPrefix;
+                    bool waiting = false;
+#pragma unroll
+                    for (int q = 0; q < kLookWidth; ++q) {
+                        if (done || waiting) continue;
+                        const uint32_t f = w[q] & ~kCountMask;
+                        if (f == 0) {  // not published yet: poll again from this tile
+                            waiting = true;
+                            continue;
+                        }
+                        excl += w[q] & kCountMask;
+                        --t;
+                        if (f == kFlagPrefix) done = true;
+                    }
+                    if (waiting) {
                         if (++polls > kLookbackLimit) {  // never expected: give up instead of hanging
                             atomicOr(err, 8u);
                             break;
                         }
                         __nanosleep(32);
-                        continue;
                     }
-                    excl += w & kCountMask;
-                    if (f == kFlagPrefix) break;
-                    --t;
                 }
                 atomicExch(&status[tile], kFlagPrefix | (excl + tot));
             }

@@ -115,3 +115,49 @@ def test_implicit_is_stable_where_explicit_blows_up():
         vmax[beta] = np.abs(v).max() if np.isfinite(v).all() else np.inf
     assert vmax[0.0] > 100.0
     assert vmax[1.0] < 0.5
+
+
+@pytest.mark.parametrize("model", [_abi.MODEL_FIXED_COROTATED, _abi.MODEL_NEO_HOOKEAN])
+def test_hessian_at_large_strain(model):
+    """20 % deformations (rotation differential far from the identity)."""
+    sc = scenes.tiny_scene(n=300, res=16, transfer=_abi.TRANSFER_APIC, interpolation=_abi.INTERP_CUBIC)
+    sc.particles.materials[0].model = model
+    o = O.OracleSolver(sc.desc(), sc.particles, bits=64)
+    rng = np.random.default_rng(21)
+    A = rng.normal(size=(sc.n, 3, 3))
+    Q, _ = np.linalg.qr(A)
+    Q *= np.sign(np.linalg.det(Q))[:, None, None]  # proper rotations
+    Fe = Q @ (np.eye(3)[None] + 0.2 * rng.normal(size=(sc.n, 3, 3)))
+    o.set(_abi.FIELD_FE, Fe.reshape(sc.n, 9))
+    u = rng.normal(size=(_nodes(o), 3))
+    Hu = o.hessian_action(u)
+    eps = 1e-6
+    fd = -(o.displaced_force(eps * u) - o.displaced_force(-eps * u)) / (2 * eps)
+    assert np.abs(Hu - fd).max() < 1e-6 * np.abs(Hu).max()
+
+
+def test_hessian_rows_sum_to_zero_and_solve_conserves_momentum():
+    """The elastic energy is translation-invariant: sum_i (H u)_i = 0 for any
+    u over all nodes.  The solve's unknowns are the nodes with m > FLT_EPSILON
+    (the velocity update's threshold); the few lighter nodes at the edge of the
+    stencils drop their share of H x, so the grid momentum sum_i m_i v_i is
+    kept to ~1e-6 relative, not exactly."""
+    sc, o = _scene(seed=8)
+    rng = np.random.default_rng(4)
+    u = rng.normal(size=(_nodes(o), 3))
+    Hu = o.hessian_action(u)
+    assert np.abs(Hu.sum(0)).max() < 1e-9 * np.abs(Hu).max()
+    dt = 1e-3
+    o.reset_grid()
+    o.particles_to_grid()
+    o.update_grid_velocities(dt)  # no gravity, no boundary: only the elastic forces act
+    m = o.grid(_abi.GRID_MASS)
+    act = m > np.finfo(np.float32).eps
+    vs = o.grid(_abi.GRID_VELOCITY_STAR).copy()
+    o.set_implicit(1.0, max_iter=500, tol=1e-13)
+    o.solve_linear_system(dt)
+    v = o.grid(_abi.GRID_VELOCITY_STAR)
+    p0 = (m[act, None] * vs[act]).sum(0)
+    p1 = (m[act, None] * v[act]).sum(0)
+    assert np.abs(p1 - p0).max() < 1e-5 * np.abs(p0).max()
+    assert np.abs(v[act] - vs[act]).max() > 1e-3 * np.abs(vs[act]).max()  # the solve acted

@@ -15,7 +15,8 @@ from mpm_b200 import _abi
 from mpm_b200.config import parseYAML, parseYAMLString, readXYZFile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_CONFIG = "/root/reference/config"
+# the reference's own scene files, copied by tests/golden/reference/vendor.py
+REF_CONFIG = os.path.join(ROOT, "tests", "golden", "reference", "config")
 
 SAMPLE = """# snow scene in the reference's schema
 ParticleGroups:
@@ -89,7 +90,6 @@ def test_parse_sample_matches_pyyaml():
     assert cfg.gravity == pytest.approx(9.80665) and cfg.transfer == -1 and cfg.boundary == 0
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_CONFIG), reason="reference configs not present")
 @pytest.mark.parametrize("name", ["snow_cube.yaml", "snow_two_balls_sparse.yaml", "snow_two_balls.yaml",
                                   "snow_text.yaml", "snow_cylinder_dragon.yaml"])
 def test_parse_reference_configs(name):
@@ -140,7 +140,6 @@ def test_read_xyz_scales_by_stride(tmp_path):
     assert e.value.status == 3
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_CONFIG), reason="reference data not present")
 def test_read_reference_point_cloud():
     x = readXYZFile("../data/cube_sparse.xyz", 5e-3, base_dir=REF_CONFIG)
     assert x.shape == (11907, 3)

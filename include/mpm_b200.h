@@ -323,9 +323,13 @@ MPM_API mpm_status mpm_sort_keys(const uint32_t* keys, size_t n, int32_t bits, u
  * inside the library that every GPU loading the library keeps until the
  * process exits.  Limits: n <= MPM_SORT_NOALLOC_MAX_KEYS (larger n is
  * rejected with MPM_ERR_INVALID_ARG); all calls share the array, so calls
- * that overlap on the GPU race -- keep them on one stream.  The first call on
- * each device resolves the array's device address (cudaGetSymbolAddress), so
- * make that first call during set-up. */
+ * that overlap on the GPU race -- keep them on one stream.  The three buffers
+ * must not overlap (an in-place sort is rejected with MPM_ERR_INVALID_ARG).
+ * The call works on the current device (mpm_set_device): `stream` must
+ * belong to it, else MPM_ERR_INVALID_ARG.  The first call on each device
+ * resolves the array's device address (cudaGetSymbolAddress) and caches it
+ * for the process, so make that first call during set-up, and do not call
+ * across a cudaDeviceReset of that device. */
 #define MPM_SORT_NOALLOC_MAX_KEYS (1u << 20)
 MPM_API mpm_status mpm_sort_keys_device_noalloc(const uint32_t* keys, uint32_t n, int32_t bits,
                                                 uint32_t* sorted_keys, uint32_t* perm, void* stream);

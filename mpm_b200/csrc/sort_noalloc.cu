@@ -48,7 +48,9 @@ uint32_t* g_scratch_ptr[kMaxDevices] = {};
 // Device address of the scratch array on the current device.  Host code may
 // not use `g_sort_scratch` itself: on the host that name is only a stand-in
 // for the symbol, not a device address.  Resolved once per device, on the
-// first call made with that device current.
+// first call made with that device current, and cached for the life of the
+// process: a cudaDeviceReset unloads the library's module on that device, so
+// the cached address is not valid across a reset.
 mpm_status scratchForCurrentDevice(uint32_t** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -73,6 +75,36 @@ mpm_status scratchForCurrentDevice(uint32_t** out) {
     return MPM_OK;
 }
 
+// True when the n-word ranges starting at a and b share a word.
+bool rangesOverlap(const uint32_t* a, const uint32_t* b, uint32_t n) {
+    const uintptr_t pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = (uintptr_t)n * sizeof(uint32_t);
+    return pa < pb + len && pb < pa + len;
+}
+
+// The scratch address is the current device's, so the stream must belong to
+// that device: a stream of another device would run the passes on that device
+// against this device's scratch.  The legacy and per-thread default streams
+// (passed as null or their handles) belong to the current device.
+mpm_status checkStreamDevice(cudaStream_t stream) {
+    if (stream == nullptr || stream == cudaStreamLegacy || stream == cudaStreamPerThread) return MPM_OK;
+    int cur = -1, sdev = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess) e = cudaStreamGetDevice(stream, &sdev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return recordError(MPM_ERR_INVALID_ARG, (std::string("mpm_sort_keys_device_noalloc: invalid stream: ") +
+                                                 cudaGetErrorString(e)).c_str());
+    }
+    if (sdev != cur)
+        return recordError(MPM_ERR_INVALID_ARG,
+                           ("mpm_sort_keys_device_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                            " but device " + std::to_string(cur) +
+                            " is current; make the stream's device current (mpm_set_device) before the call")
+                               .c_str());
+    return MPM_OK;
+}
+
 }  // namespace
 }  // namespace mpm
 
@@ -89,8 +121,17 @@ extern "C" mpm_status mpm_sort_keys_device_noalloc(const uint32_t* keys, uint32_
     if (n == 0) return MPM_OK;
     if (!keys || !sorted_keys || !perm)
         return mpm::recordError(MPM_ERR_INVALID_ARG, "mpm_sort_keys_device_noalloc: null buffer");
+    // The first pass reads `keys` while it scatters into the outputs (or into
+    // the scratch pair, which later passes scatter back into the outputs), so
+    // the three buffers must be distinct: an in-place call would sort wrongly.
+    if (mpm::rangesOverlap(keys, sorted_keys, n) || mpm::rangesOverlap(keys, perm, n) ||
+        mpm::rangesOverlap(sorted_keys, perm, n))
+        return mpm::recordError(MPM_ERR_INVALID_ARG,
+                                "mpm_sort_keys_device_noalloc: keys, sorted_keys and perm must not overlap");
+    mpm_status st = mpm::checkStreamDevice(static_cast<cudaStream_t>(stream));
+    if (st != MPM_OK) return st;
     uint32_t* scratch = nullptr;
-    mpm_status st = mpm::scratchForCurrentDevice(&scratch);
+    st = mpm::scratchForCurrentDevice(&scratch);
     if (st != MPM_OK) return st;
     uint32_t* tmp_keys = scratch;
     uint32_t* tmp_vals = scratch + mpm::kMaxKeys;

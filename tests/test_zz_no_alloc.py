@@ -76,3 +76,30 @@ def test_noalloc_sort_rejects_oversized_input(gpu):
     st = lib.mpm_sort_keys_device_noalloc(C.c_void_p(1), MAX_KEYS + 1, 22, C.c_void_p(1), C.c_void_p(1), None)
     assert st == 1
     assert b"MPM_SORT_NOALLOC_MAX_KEYS" in lib.mpm_last_error_string()
+
+
+@pytest.mark.parametrize("n,bits", [(1000, 8), (2049, 32), (1, 5), (2047, 12)])
+def test_noalloc_sort_single_pass_and_ragged_sizes(gpu, n, bits):
+    """One pass (bits <= 8: the first pass writes straight into the caller's
+    outputs), inputs below one 2048-key tile, one key past a tile, and n = 1,
+    each against the allocating sort and a CPU stable sort."""
+    hi = (1 << bits) if bits < 32 else (1 << 32)
+    keys = np.random.default_rng(n * 7 + bits).integers(0, hi, n, dtype=np.uint64).astype(np.uint32)
+    got_k, got_p = _noalloc_sort(keys, bits)
+    ref_k, ref_p = _reference_sort(keys, bits)
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    assert np.array_equal(got_p, ref_p) and np.array_equal(got_p, order)
+    assert np.array_equal(got_k, ref_k) and np.array_equal(got_k, keys[order])
+
+
+def test_noalloc_sort_rejects_overlapping_buffers(gpu):
+    """An in-place call (keys == sorted_keys) or outputs that overlap are
+    refused before any device work: the passes read the input while they
+    scatter into the outputs."""
+    lib = _abi.load()
+    base = 1 << 20  # never dereferenced: the argument check comes first
+    for keys, out, perm in ((base, base, base + 65536), (base, base + 4 * 999, base + 65536),
+                            (base, base + 65536, base + 65536 + 4 * 100)):
+        st = lib.mpm_sort_keys_device_noalloc(C.c_void_p(keys), 1000, 16, C.c_void_p(out), C.c_void_p(perm), None)
+        assert st == 1
+        assert b"must not overlap" in lib.mpm_last_error_string()

@@ -149,17 +149,72 @@ def allsum(ws, x):
 
 # --- clocks -----------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event (throttle) reasons of one GPU, sampled
+    through NVML every ~2 ms by a thread while the timed region runs, plus one
+    sample on entry and one on exit (so even a region of a few milliseconds is
+    covered).  Falls back to `nvidia-smi -lms` when NVML is unavailable."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index=0):
         self.index = index
-        self.rows = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self.rows = []     # nvidia-smi fallback rows
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        # CUDA device indices count only the visible GPUs: find the GPU by the
+        # UUID CUDA reports for it, else by CUDA_VISIBLE_DEVICES, else by index
+        h = None
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            h = None
+        if h is None:
+            ids = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+            idx = int(ids[self.index]) if len(ids) > self.index and ids[self.index].isdigit() else self.index
+            h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        self.bits = [(name, getattr(pynvml, const)) for name, const in self.REASONS]
+        return pynvml, h
+
+    def _sample(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(sm), float(mx), int(rs)))
+
+    def _poll(self):
+        while not self.stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            self.stop.wait(0.002)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._sample()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "50", "-i", str(self.index)], stdout=subprocess.PIPE,
@@ -175,6 +230,13 @@ class ClockSampler:
             self.rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.t.join(timeout=5)
+            try:
+                self._sample()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -184,6 +246,11 @@ class ClockSampler:
             self.t.join(timeout=5)
 
     def summary(self):
+        if self.samples:
+            sm = [a for a, _, _ in self.samples]
+            reasons = sorted({name for _, _, r in self.samples for name, bit in self.bits if r & bit})
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(b for _, b, _ in self.samples),
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
@@ -191,7 +258,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": "nvidia-smi"}
 
 
 # --- roofline ---------------------------------------------------------------
@@ -246,12 +313,23 @@ def traffic_of(family, workload):
 
 
 # --- CPU and naive-GPU baselines --------------------------------------------------
-def cpu_rate(work, budget_s, steps_hint=None):
-    """Reference step math (oracle, FP32 restatement) on all host cores: full
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_rate(work, budget_s, steps_hint=None, threads=None):
+    """Reference step math (oracle, FP32 restatement) on the host cores: full
     steps of the workload's scenes, as many as fit the time budget.
     Returns (rate, threads, sample description, steps, seconds)."""
     from oracle import oracle as O
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     if len(work.scenes) == 1:
         sc = work.scenes[0]
         o = O.OracleSolver(sc.desc(), sc.particles, bits=32, threads=threads)
@@ -275,6 +353,27 @@ def cpu_rate(work, budget_s, steps_hint=None):
         if dt > budget_s:
             break
     return done / dt, threads, f"1 step of each of the first {used} scenes ({done} particle-steps)", 1, dt
+
+
+def cpu_single_thread(work, max_particles=65536):
+    """The same FP32 step math on one host thread, over a bounded sample: one
+    step (after one untimed step) of a seeded random subset of at most
+    max_particles particles of the workload's first scene, on its full grid."""
+    from oracle import oracle as O
+    from mpm_b200.solver import Particles
+    sc = work.scenes[0]
+    p = sc.particles
+    if sc.n > max_particles:
+        idx = np.sort(np.random.default_rng(0).choice(sc.n, max_particles, replace=False))
+        p = Particles(p.positions[idx], p.velocities[idx], p.mass[idx], p.materials,
+                      None if p.material is None else p.material[idx], None if p.volume is None else p.volume[idx])
+    o = O.OracleSolver(sc.desc(), p, bits=32, threads=1)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(1)
+    dt = time.perf_counter() - t0
+    return {"value": p.n / dt, "unit": METRIC, "cores": 1,
+            "sample": f"1 step of a seeded random {p.n}-particle subset of {sc.name} (full grid), after 1 untimed step"}
 
 
 def naive_rate(work, budget_s):
@@ -309,7 +408,8 @@ def run_reference(args, ws, rank):
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
            "config": work.config(1),
            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                            "sample": sample + " after 1 untimed step"},
+                            "sample": sample + " after 1 untimed step", "cpu_model": cpu_model(),
+                            "nproc": os.cpu_count()},
            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -377,7 +477,8 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, threads, sample, k, dt = cpu_rate(work, args.cpu_budget_s)
         cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
-               "sample": sample + " (oracle FP32, OpenMP)"}
+               "sample": sample + " (oracle FP32, OpenMP)", "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+               "single_thread": cpu_single_thread(work)}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
@@ -420,6 +521,12 @@ def run_forms(args, ws, local):
                       "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3,
                       "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st}
     solvers = [s.solver(device=local) for s in work.scenes]
+    # warm-up as for the batch: the first step decides the P2G staging size
+    # (read back at the synchronize), the next steps capture the step graphs
+    for g in solvers:
+        g.step(1)
+    for g in solvers:
+        g.synchronize()
     for g in solvers:
         g.step(3)
     for g in solvers:

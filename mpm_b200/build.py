@@ -19,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpm_b200.so")
 CLI = os.path.join(HERE, "mpm-run")
-# The image's default CXX (/opt/gcc) lacks parts of the runtime; the system g++ is complete.
+# Host compiler of the CLI: the system g++ (a CXX from the environment may be a
+# wrapper without the full C++ runtime); override with MPM_HOSTCXX.
 HOSTCXX = os.environ.get("MPM_HOSTCXX", "/usr/bin/g++")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -198,6 +198,10 @@ struct SceneHost {
 
 class Engine {
 public:
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    };
     Engine() {}
     ~Engine() {
         if (stream_) cudaStreamSynchronize(stream_);
@@ -229,17 +233,45 @@ public:
         }
         if (compact_fork_) cudaEventDestroy(compact_fork_);
         if (compact_join_) cudaEventDestroy(compact_join_);
+        releaseScratch();
+        if (host_word_) cudaFreeHost(host_word_);
+        if (stage_event_) cudaEventDestroy(stage_event_);
         if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    // Device memory of the engine (batch scratch, scene buffers) comes from
+    // the per-device stream-ordered pool in the order of the engine's stream:
+    // engines that are created and destroyed (solvers of a server, the
+    // benchmark's repeated constructions) reuse memory without cudaMalloc or
+    // the implicit device synchronization of cudaFree.
+    mpm_status alloc(DevMem& m, size_t b, const char* what) { return m.allocPooled(b, what, pool_, stream_); }
+    mpm_status grow(DevMem& m, size_t b, const char* what) {
+        if (m.p && m.bytes >= b) return MPM_OK;
+        return m.allocPooled(std::max(b, m.bytes + m.bytes / 2), what, pool_, stream_);
+    }
+    // Returns the engine's own buffers to the pool in the stream's order
+    // (called before the stream is destroyed).
+    void releaseScratch() {
+        DevMem* all[] = {&cell_range_, &block_range_, &solve_pofs_, &solve_prep_, &solve_T_, &solve_iter_,
+                         &keys_[0], &keys_[1], &vals_[0], &vals_[1], &sort_scratch_, &inc_scratch_,
+                         &compact_scratch_, &block_count_, &sbb_, &active_, &outside_, &counters_, &block_slot_,
+                         &tiles_, &scenes_dev_, &err_, &tmp_};
+        for (DevMem* m : all) m->release();
     }
 
     mpm_status init() {
         CUDA_TRY(cudaGetDevice(&device_));
+        {
+            mpm_status pst;
+            pool_ = scenePool(device_, &pst);
+            if (!pool_) return pst;
+        }
         CUDA_TRY(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_));
         CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CUDA_TRY(cudaStreamCreateWithFlags(&compact_stream_, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&compact_fork_, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&compact_join_, cudaEventDisableTiming));
-        MPM_TRY(err_.alloc(sizeof(uint32_t), "error flags"));
+        MPM_TRY(alloc(err_, sizeof(uint32_t), "error flags"));
         CUDA_TRY(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), stream_));
         for (int k = 0; k < KF_COUNT; ++k) {
             CUDA_TRY(cudaEventCreate(&ev_[k][0]));
@@ -307,9 +339,13 @@ public:
             MPM_TRY(sc->buf_f[b].allocPooled(sizeof(float) * NFIELDS * cap, "particle state", pool, stream_));
             MPM_TRY(sc->buf_pid[b].allocPooled(sizeof(uint32_t) * cap, "particle ids", pool, stream_));
             MPM_TRY(sc->buf_mat[b].allocPooled(sizeof(uint16_t) * cap, "particle materials", pool, stream_));
+            // With one material G2P does not copy the material ids between the
+            // buffers, so both start as material 0 (pool memory is reused and
+            // holds earlier contents); checkpoints save the plane as it is.
+            CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * cap, stream_));
         }
         const size_t nodes = sc->nodes();
-        MPM_TRY(sc->cfl_state.alloc(sizeof(CflState), "CFL state"));
+        MPM_TRY(alloc(sc->cfl_state, sizeof(CflState), "CFL state"));
         CUDA_TRY(cudaMemsetAsync(sc->cfl_state.p, 0, sizeof(CflState), stream_));
         MPM_TRY(sc->vstar.allocPooled(sizeof(float4) * nodes, "grid v*", pool, stream_));
         CUDA_TRY(cudaMemsetAsync(sc->vstar.p, 0, sizeof(float4) * nodes, stream_));
@@ -359,7 +395,7 @@ public:
         if (p.n > 0) {
             const bool has_vol = d.volume_mode == MPM_VOLUME_PRESCRIBED;
             const size_t n = p.n;
-            MPM_TRY(tmp_.grow(sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
+            MPM_TRY(grow(tmp_, sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
             float* staged = tmp_.as<float>();
             CUDA_TRY(cudaMemcpyAsync(staged, p.position, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
             CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
@@ -687,32 +723,32 @@ public:
         // batch scratch
         const size_t nk = std::max<size_t>(ntot, 1);
         for (int k = 0; k < 2; ++k) {
-            MPM_TRY(keys_[k].grow(sizeof(uint32_t) * nk, "keys"));
-            MPM_TRY(vals_[k].grow(sizeof(uint32_t) * nk, "values"));
+            MPM_TRY(grow(keys_[k], sizeof(uint32_t) * nk, "keys"));
+            MPM_TRY(grow(vals_[k], sizeof(uint32_t) * nk, "values"));
         }
-        MPM_TRY(sort_scratch_.grow(sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
-        MPM_TRY(inc_scratch_.grow(sizeof(uint32_t) * incrementalSortScratchWords(nk, key_bits_),
+        MPM_TRY(grow(sort_scratch_, sizeof(uint32_t) * onesweepScratchWords(nk, key_bits_), "sort scratch"));
+        MPM_TRY(grow(inc_scratch_, sizeof(uint32_t) * incrementalSortScratchWords(nk, key_bits_),
                                   "incremental sort scratch"));
-        MPM_TRY(compact_scratch_.grow(sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
+        MPM_TRY(grow(compact_scratch_, sizeof(unsigned long long) * compactScratchWords64((uint32_t)tb),
                                        "compaction scratch"));
-        MPM_TRY(block_count_.grow(sizeof(uint32_t) * tb, "block counts"));
+        MPM_TRY(grow(block_count_, sizeof(uint32_t) * tb, "block counts"));
         CUDA_TRY(cudaMemsetAsync(block_count_.p, 0, sizeof(uint32_t) * tb, stream_));
-        MPM_TRY(sbb_.grow(sizeof(uint32_t) * (ns + 1), "scene block bases"));
+        MPM_TRY(grow(sbb_, sizeof(uint32_t) * (ns + 1), "scene block bases"));
         CUDA_TRY(cudaMemcpyAsync(sbb_.p, sbb.data(), sizeof(uint32_t) * (ns + 1), cudaMemcpyHostToDevice, stream_));
         // work items: one per non-empty block plus one per further kBlockChunk particles
         max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
-        MPM_TRY(active_.grow(sizeof(BlockItem) * max_active_, "active blocks"));
-        MPM_TRY(outside_.grow(sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
+        MPM_TRY(grow(active_, sizeof(BlockItem) * max_active_, "active blocks"));
+        MPM_TRY(grow(outside_, sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
         // [0] work items, [1] outside items, [2] active nodes, [8 + 8k .. 13 + 8k] item
         // schedulers of the k-th stencil/transfer combination
-        MPM_TRY(counters_.alloc(sizeof(uint32_t) * 64, "counters"));
+        MPM_TRY(alloc(counters_, sizeof(uint32_t) * 64, "counters"));
         CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 64, stream_));
-        MPM_TRY(block_slot_.grow(sizeof(int32_t) * tb, "block slots"));
+        MPM_TRY(grow(block_slot_, sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
         for (auto& s : scenes_) maxS = std::max(maxS, s->S);
         tile_stride_ = (size_t)7 * tileNodes(maxS);
-        MPM_TRY(tiles_.grow(sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
-        MPM_TRY(scenes_dev_.grow(sizeof(SceneDev) * std::max(ns, 1), "scene table"));
+        MPM_TRY(grow(tiles_, sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
+        MPM_TRY(grow(scenes_dev_, sizeof(SceneDev) * std::max(ns, 1), "scene table"));
         CUDA_TRY(cudaMemcpyAsync(scenes_dev_.p, host_scenes_.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice,
                                  stream_));
         CUDA_TRY(cudaStreamSynchronize(stream_));
@@ -722,6 +758,7 @@ public:
         sorted_valid_ = false;
         incremental_ok_ = false;
         stage_check_ = true;
+        stage_pending_ = false;  // a read-back issued before the sync above is stale
         any_implicit_ = false;
         for (auto& s : scenes_) any_implicit_ |= s->beta > 0.f;
         MPM_TRY(ensureSolveBuffers());
@@ -740,12 +777,12 @@ public:
     mpm_status ensureSolveBuffers() {
         if (!any_implicit_ || dirty_) return MPM_OK;
         const size_t n = std::max<size_t>(ntot_, 1);
-        MPM_TRY(cell_range_.grow(sizeof(uint2) * (size_t)total_blocks_ * 64, "solver cell ranges"));
-        MPM_TRY(block_range_.grow(sizeof(uint2) * (size_t)total_blocks_, "solver block ranges"));
-        MPM_TRY(solve_pofs_.grow(sizeof(float4) * n, "solver stencil offsets"));
-        MPM_TRY(solve_prep_.grow(sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
-        MPM_TRY(solve_T_.grow(sizeof(float4) * 3 * n, "solver particle stress differentials"));
-        MPM_TRY(solve_iter_.grow(sizeof(int), "solver iteration counter"));
+        MPM_TRY(grow(cell_range_, sizeof(uint2) * (size_t)total_blocks_ * 64, "solver cell ranges"));
+        MPM_TRY(grow(block_range_, sizeof(uint2) * (size_t)total_blocks_, "solver block ranges"));
+        MPM_TRY(grow(solve_pofs_, sizeof(float4) * n, "solver stencil offsets"));
+        MPM_TRY(grow(solve_prep_, sizeof(float) * kSolvePrepPlanes * n, "solver particle data"));
+        MPM_TRY(grow(solve_T_, sizeof(float4) * 3 * n, "solver particle stress differentials"));
+        MPM_TRY(grow(solve_iter_, sizeof(int), "solver iteration counter"));
         MPM_TRY(ensureSideStreams(1));  // the loop body of a captured solve is captured on side_[0]
         return MPM_OK;
     }
@@ -762,11 +799,11 @@ public:
         SceneHost& s = *scenes_[idx];
         if (beta > 0.f) {
             const size_t nodes = s.nodes();
-            MPM_TRY(s.solve_m.grow(sizeof(float) * nodes, "solver node masses"));
-            MPM_TRY(s.solve_vec.grow(sizeof(float4) * kSolveVectors * nodes, "solver node vectors"));
-            MPM_TRY(s.solve_list.grow(sizeof(int) * nodes, "solver node list"));
-            MPM_TRY(s.solve_part.grow(sizeof(double) * solvePartialDoubles(max_iter), "solver partial sums"));
-            MPM_TRY(s.solve_status.grow(sizeof(SolveStatus), "solver status"));
+            MPM_TRY(grow(s.solve_m, sizeof(float) * nodes, "solver node masses"));
+            MPM_TRY(grow(s.solve_vec, sizeof(float4) * kSolveVectors * nodes, "solver node vectors"));
+            MPM_TRY(grow(s.solve_list, sizeof(int) * nodes, "solver node list"));
+            MPM_TRY(grow(s.solve_part, sizeof(double) * solvePartialDoubles(max_iter), "solver partial sums"));
+            MPM_TRY(grow(s.solve_status, sizeof(SolveStatus), "solver status"));
             CUDA_TRY(cudaMemset(s.solve_status.p, 0, sizeof(SolveStatus)));
         }
         s.beta = beta;
@@ -1067,50 +1104,95 @@ public:
     // (keys and stress produced by the previous G2P, no profiling) the step is
     // replayed from a CUDA graph captured once per (particle buffer, key
     // buffer) state; the launch sequence and its arguments only depend on it.
-    mpm_status stepOnce() {
+    bool steadyNow() const {
         bool stale = false;
         for (auto& s : scenes_) stale |= s->stress_stale;
-        const bool steady = use_graphs_ && keys_valid_ && incremental_ok_ && !stale && !profiling_ && !dirty_;
-        if (!steady) return stepBody();
-        GraphSlot& g = graphs_[parity_][kcur_];
+        return use_graphs_ && keys_valid_ && incremental_ok_ && !stale && !profiling_ && !dirty_ && !stage_check_;
+    }
+
+    // Captures the step of the current host state into g (the host state is
+    // left as it was: the capture only records the launches).  On a capture
+    // failure graphs are switched off for this engine and g stays empty.
+    mpm_status captureGraph(GraphSlot& g) {
         const int p0 = parity_, k0 = kcur_;
-        if (!g.exec) {
-            const uint64_t l0 = kernelLaunches();
-            sorted_valid_ = false;  // the graph must contain the sort
-            CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-            mpm_status st = stepBody();
-            cudaGraph_t graph = nullptr;
-            cudaError_t e = cudaStreamEndCapture(stream_, &graph);
-            // the capture only recorded the launches: restore the host state
-            parity_ = p0;
-            kcur_ = k0;
-            keys_valid_ = true;
-            if (st != MPM_OK || e != cudaSuccess) {
-                if (graph) cudaGraphDestroy(graph);
-                cudaGetLastError();
-                use_graphs_ = false;  // fall back to direct launches for this engine
-                return stepBody();
-            }
+        const uint64_t l0 = kernelLaunches();
+        sorted_valid_ = false;  // the graph must contain the sort
+        CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        mpm_status st = stepBody();
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+        parity_ = p0;
+        kcur_ = k0;
+        keys_valid_ = true;
+        if (st == MPM_OK && e == cudaSuccess) {
             e = cudaGraphInstantiate(&g.exec, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                g.exec = nullptr;
-                cudaGetLastError();
-                use_graphs_ = false;
-                return stepBody();
-            }
-            g.launches = kernelLaunches() - l0;
-            noteLaunches(0 - g.launches);  // captured, not run: counted at each replay instead
+            if (e != cudaSuccess) g.exec = nullptr;
         }
-        CUDA_TRY(cudaGraphLaunch(g.exec, stream_));
-        noteLaunches(g.launches);
-        // host state after the step, as stepBody() leaves it
+        if (graph) cudaGraphDestroy(graph);
+        if (st != MPM_OK || e != cudaSuccess) {
+            cudaGetLastError();
+            use_graphs_ = false;  // fall back to direct launches for this engine
+            noteLaunches(0 - (kernelLaunches() - l0));
+            return MPM_OK;
+        }
+        g.launches = kernelLaunches() - l0;
+        noteLaunches(0 - g.launches);  // captured, not run: counted at each replay instead
+        return MPM_OK;
+    }
+
+    // Host state after a replayed step of the state (p0, k0), as stepBody()
+    // leaves it.
+    void advanceReplayed(int p0, int k0) {
         sorted_ = graph_sorted_[p0][k0];
         parity_ = p0 ^ 1;
         kcur_ = 1 - sorted_;
         keys_valid_ = true;
         sorted_valid_ = false;
         incremental_ok_ = true;
+    }
+
+    // Captures, ahead of time, the graphs of the states the next steps visit
+    // (they alternate between particle buffers and key buffers), so that a
+    // timed run replays graphs from its first step instead of capturing inside
+    // its timed region.  Resolves a pending staging decision first.
+    mpm_status prepareGraphs() {
+        if (stage_pending_) {
+            CUDA_TRY(cudaEventSynchronize(stage_event_));
+            MPM_TRY(checkP2GStage());
+        }
+        const int p0 = parity_, k0 = kcur_, s0 = sorted_;
+        const bool kv = keys_valid_, sv = sorted_valid_, io = incremental_ok_;
+        for (int i = 0; i < 4 && steadyNow(); ++i) {
+            GraphSlot& g = graphs_[parity_][kcur_];
+            if (!g.exec) MPM_TRY(captureGraph(g));
+            if (!g.exec) break;
+            advanceReplayed(parity_, kcur_);
+        }
+        parity_ = p0;
+        kcur_ = k0;
+        sorted_ = s0;
+        keys_valid_ = kv;
+        sorted_valid_ = sv;
+        incremental_ok_ = io;
+        return MPM_OK;
+    }
+
+    // One fused simulateOneStep over every scene of the batch.  In steady state
+    // (keys and stress produced by the previous G2P, no profiling, staging
+    // size decided) the step is replayed from a CUDA graph captured once per
+    // (particle buffer, key buffer) state; the launch sequence and its
+    // arguments only depend on it.
+    mpm_status stepOnce() {
+        if (!steadyNow()) return stepBody();
+        GraphSlot& g = graphs_[parity_][kcur_];
+        const int p0 = parity_, k0 = kcur_;
+        if (!g.exec) {
+            MPM_TRY(captureGraph(g));
+            if (!g.exec) return stepBody();
+        }
+        CUDA_TRY(cudaGraphLaunch(g.exec, stream_));
+        noteLaunches(g.launches);
+        advanceReplayed(p0, k0);
         return MPM_OK;
     }
 
@@ -1122,7 +1204,7 @@ public:
             CUDA_TRY(cudaMemsetAsync(counters_.as<uint32_t>() + 2, 0, sizeof(uint32_t), stream_));
         }
         MPM_TRY(refreshStress());
-        if (any_cfl_) launchCfl(ctx(), parity_, max_n_);
+        if (any_cfl_) launchCfl(ctx(), parity_, max_n_, err_.as<uint32_t>());
         graph_sorted_[parity_][kcur_] = sorted_;
         const int next = 1 - sorted_;
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
@@ -1182,13 +1264,29 @@ public:
     // ones (fewer than 8 particles per cell on average: the smaller staging
     // buffer fits 3 CTAs per SM and the passes are rarely full).  Decided
     // once after the first step that follows a change of the scene set,
-    // from the number of work items of that step.
+    // from the number of work items of that step.  The count is read back
+    // asynchronously (a copy into pinned host memory and an event), so the
+    // host does not wait for the GPU: the steps that follow run with direct
+    // launches until the event has completed, and only then is the step
+    // captured as a CUDA graph (a change of staging size would drop it).
     mpm_status checkP2GStage() {
         if (!stage_check_) return MPM_OK;
+        if (!stage_pending_) {
+            if (!host_word_) {
+                CUDA_TRY(cudaHostAlloc((void**)&host_word_, sizeof(uint32_t), cudaHostAllocDefault));
+                CUDA_TRY(cudaEventCreateWithFlags(&stage_event_, cudaEventDisableTiming));
+            }
+            CUDA_TRY(cudaMemcpyAsync(host_word_, counters_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+            CUDA_TRY(cudaEventRecord(stage_event_, stream_));
+            stage_pending_ = true;
+            return MPM_OK;
+        }
+        const cudaError_t q = cudaEventQuery(stage_event_);
+        if (q == cudaErrorNotReady) return MPM_OK;
+        CUDA_TRY(q);
+        stage_pending_ = false;
         stage_check_ = false;
-        uint32_t items = 0;
-        CUDA_TRY(cudaStreamSynchronize(stream_));
-        CUDA_TRY(cudaMemcpy(&items, counters_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        const uint32_t items = *host_word_;
         const int stage = (items > 0 && ntot_ / items < 512) ? 16 : 32;
         if (stage != p2g_stage_) {
             p2g_stage_ = stage;
@@ -1256,6 +1354,7 @@ public:
     mpm_status timedStep(int n, float* ms) {
         if (!ms) return fail(MPM_ERR_INVALID_ARG, "null output");
         MPM_TRY(ensureReady());
+        MPM_TRY(prepareGraphs());
         CUDA_TRY(cudaEventRecord(ev_[0][0], stream_));
         for (int i = 0; i < n; ++i) {
             MPM_TRY(stepOnce());
@@ -1298,6 +1397,7 @@ public:
 
     mpm_status synchronize() {
         CUDA_TRY(cudaStreamSynchronize(stream_));
+        if (stage_pending_) MPM_TRY(checkP2GStage());  // its read-back has landed
         MPM_TRY(downloadWait());
         uint32_t e = 0;
         CUDA_TRY(cudaMemcpy(&e, err_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -1314,7 +1414,7 @@ public:
         bool changed = false;
         for (auto& s : scenes_)
             if (!s->dbg.p) {
-                MPM_TRY(s->dbg.alloc(sizeof(float) * 10 * s->nodes(), "dense debug grid"));
+                MPM_TRY(alloc(s->dbg, sizeof(float) * 10 * s->nodes(), "dense debug grid"));
                 CUDA_TRY(cudaMemsetAsync(s->dbg.p, 0, sizeof(float) * 10 * s->nodes(), stream_));
                 changed = true;
             }
@@ -1435,7 +1535,7 @@ public:
             return fail(MPM_ERR_INVALID_ARG, "B is only defined for APIC scenes");
         if (s.n == 0) return MPM_OK;
         const size_t bytes = sizeof(float) * per * s.n;
-        MPM_TRY(tmp_.alloc(bytes, "download buffer"));
+        MPM_TRY(alloc(tmp_, bytes, "download buffer"));
         LaunchCtx c = ctx();
         launchGatherField(c, idx, parity_, base, comps, mode, tmp_.as<float>());
         CUDA_TRY(cudaGetLastError());
@@ -1522,7 +1622,7 @@ public:
         // cell_vol_inv as the reference forms it: 1.0 / (h*h*h) in double, stored as float
         const float h = s.desc.stride;
         const float inv = (float)(1.0 / (double)(h * h * h));
-        MPM_TRY(tmp_.grow(sizeof(float) * nodes, "density buffer"));
+        MPM_TRY(grow(tmp_, sizeof(float) * nodes, "density buffer"));
         launchDensity(ctx(), s.vstar.as<float4>(), nodes, inv, tmp_.as<float>());
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemcpyAsync(host, tmp_.p, sizeof(float) * nodes, cudaMemcpyDeviceToHost, stream_));
@@ -1541,7 +1641,7 @@ public:
         SceneHost& s = *scenes_[idx];
         if (s.n == 0) return MPM_OK;
         const size_t bytes = sizeof(float) * per * s.n;
-        MPM_TRY(tmp_.alloc(bytes, "upload buffer"));
+        MPM_TRY(alloc(tmp_, bytes, "upload buffer"));
         CUDA_TRY(cudaMemcpyAsync(tmp_.p, host, bytes, cudaMemcpyHostToDevice, stream_));
         launchScatterField(ctx(), idx, parity_, base, comps, tmp_.as<float>());
         CUDA_TRY(cudaGetLastError());
@@ -1609,7 +1709,7 @@ public:
             for (size_t i = 0; i < nodes; ++i)
                 if (!std::isfinite(phi[i])) return fail(MPM_ERR_INVALID_ARG, "level set has a non-finite value");
             CUDA_TRY(cudaStreamSynchronize(stream_));  // earlier steps may still read the old values
-            MPM_TRY(s.phi.grow(sizeof(float) * nodes, "level set"));
+            MPM_TRY(grow(s.phi, sizeof(float) * nodes, "level set"));
             CUDA_TRY(cudaMemcpy(s.phi.p, phi, sizeof(float) * nodes, cudaMemcpyHostToDevice));
             s.has_phi = true;
             s.phi_friction = friction;
@@ -1657,6 +1757,10 @@ public:
 
 private:
     int device_ = 0, num_sms_ = 148;
+    cudaMemPool_t pool_ = nullptr;         // the device's scene pool (init)
+    uint32_t* host_word_ = nullptr;        // pinned: work-item count read back by checkP2GStage
+    cudaEvent_t stage_event_ = nullptr;    // completion of that read-back
+    bool stage_pending_ = false;
     cudaStream_t stream_ = nullptr;
     cudaStream_t compact_stream_ = nullptr;  // block compaction beside the sort
     cudaEvent_t compact_fork_ = nullptr, compact_join_ = nullptr;
@@ -1702,10 +1806,6 @@ private:
             }
         return MPM_OK;
     }
-    struct GraphSlot {
-        cudaGraphExec_t exec = nullptr;
-        uint64_t launches = 0;
-    };
     GraphSlot graphs_[2][2];          // [particle buffer parity][unsorted key buffer]
     int graph_sorted_[2][2] = {};     // sorted key buffer after the sort of that state
     bool use_graphs_ = getenv("MPM_NO_GRAPHS") == nullptr;

@@ -102,7 +102,8 @@ cudaError_t launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, c
 
 // CFL time step of the scenes with cfl > 0: max |v|^2 over their live
 // particles, then dt = min(dt_max, cfl h / max|v|) into the scene table.
-void launchCfl(const LaunchCtx& c, int parity, size_t max_n);
+// A non-finite particle speed sets ERR_NONFINITE in err.
+void launchCfl(const LaunchCtx& c, int parity, size_t max_n, uint32_t* err);
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out);
 void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in);
 size_t p2gSmemBytes(int S, int mode);

@@ -1509,16 +1509,25 @@ __global__ void densityKernel(const float4* __restrict__ vstar, size_t nodes, fl
         out[i] = vstar[i].w * inv_cell_vol;
 }
 // CFL time step (listed as unimplemented in the reference, README.md:60-67).
-__global__ void __launch_bounds__(kThreads) cflMaxKernel(const SceneDev* __restrict__ scenes, int parity) {
+// A non-finite speed (NaN or Inf velocity, or |v|^2 overflowing) would leave
+// dt without a bound (fmaxf drops NaN) or make it 0 (Inf): it raises
+// ERR_NONFINITE, which the next synchronize reports as MPM_ERR_NUMERIC, and is
+// left out of the maximum.
+__global__ void __launch_bounds__(kThreads) cflMaxKernel(const SceneDev* __restrict__ scenes, int parity,
+                                                         uint32_t* __restrict__ err) {
     const SceneDev& sc = scenes[blockIdx.y];
     if (!(sc.cfl > 0.f)) return;
     const float* f = sc.buf[parity].f;
     const size_t cap = sc.cap;
     float m = 0.f;
+    bool bad = false;
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
         const float vx = f[(F_V + 0) * cap + i], vy = f[(F_V + 1) * cap + i], vz = f[(F_V + 2) * cap + i];
-        m = fmaxf(m, __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+        const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+        if (isfinite(v2)) m = fmaxf(m, v2);
+        else bad = true;
     }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, ERR_NONFINITE);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     __shared__ float wm[kThreads / 32];
@@ -1545,11 +1554,11 @@ __global__ void cflFinalizeKernel(SceneDev* __restrict__ scenes, int nscenes) {
         st->time += (double)dt;
     }
 }
-void launchCfl(const LaunchCtx& c, int parity, size_t max_n) {
+void launchCfl(const LaunchCtx& c, int parity, size_t max_n, uint32_t* err) {
     noteLaunches(2);
     const unsigned bx = (unsigned)std::max<size_t>(
         1, std::min<size_t>((max_n + kThreads - 1) / kThreads, (size_t)c.num_sms * 4));
-    cflMaxKernel<<<dim3(bx, (unsigned)c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity);
+    cflMaxKernel<<<dim3(bx, (unsigned)c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, err);
     cflFinalizeKernel<<<1, 128, 0, c.stream>>>(const_cast<SceneDev*>(c.scenes), c.nscenes);
 }
 void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out) {

@@ -108,3 +108,22 @@ def test_checkpoint_carries_cfl_and_time(gpu, tmp_path, cls, transfer):
     # saved time + the resumed steps' sum: the same terms, grouped differently
     assert r.time()[1] == g.time()[1]
     assert r.time()[0] == pytest.approx(g.time()[0], rel=1e-12)
+
+
+@pytest.mark.parametrize("bad", [np.inf, np.nan])
+def test_non_finite_speed_is_reported(gpu, bad):
+    """A non-finite particle velocity in a CFL scene is reported by the next
+    synchronize (MPM_ERR_NUMERIC) instead of silently bounding dt by the
+    finite particles (NaN) or setting it to 0 (Inf)."""
+    sc = _fast(_abi.TRANSFER_APIC, _abi.INTERP_CUBIC)
+    g = sc.solver()
+    g.set_cfl(0.08)
+    g.step(1)
+    g.synchronize()
+    v = g.download(_abi.FIELD_VELOCITY)
+    v[5] = bad
+    g.upload(_abi.FIELD_VELOCITY, v)
+    g.step(1)
+    with pytest.raises(_abi.MPMError) as e:
+        g.synchronize()
+    assert e.value.status == 6

@@ -154,3 +154,24 @@ def test_stiff_block_at_large_dt(gpu):
     assert np.isfinite(v).all() and np.abs(v).max() < 0.5
     assert relerr(g.download(_abi.FIELD_POSITION), o.get(_abi.FIELD_POSITION)) < 1e-4
     assert relerr(v, o.get(_abi.FIELD_VELOCITY)) < 1e-2
+
+
+def test_graphed_and_direct_solves_agree_at_the_iteration_cap(gpu, monkeypatch):
+    """With tol = 0 every solve runs to max_iter.  Replayed from the step
+    graph the iterations are a conditional while node; with graphs off
+    (MPM_NO_GRAPHS, read when a solver is created) they are max_iter direct
+    launches of the same kernels.  Both give bitwise the same state and the
+    same iteration count and residual."""
+    sc = scenes.tiny_scene(n=6000, res=24, transfer=_abi.TRANSFER_APIC, interpolation=_abi.INTERP_QUADRATIC)
+    sc.dt = 1e-3
+    graphed = sc.solver()
+    monkeypatch.setenv("MPM_NO_GRAPHS", "1")
+    direct = sc.solver()
+    monkeypatch.delenv("MPM_NO_GRAPHS")
+    for s in (graphed, direct):
+        s.set_implicit(1.0, max_iter=12, tol=0.0)
+        s.step(6)
+    for f in FIELDS:
+        assert np.array_equal(graphed.download(f), direct.download(f)), f
+    assert graphed.solve_info() == direct.solve_info()
+    assert graphed.solve_info()[0] == 12

@@ -421,6 +421,8 @@ def run_ours(args, ws, rank, local):
     _abi.check(lib.mpm_set_device(local), "mpm_set_device")
     work = Work(args.workload, rank, ws, args.batch_scenes)
     g = work.engine()
+    # launch settings from the autotuner (its steps are real steps, before warm-up)
+    tuning = g.autotune(steps_per_candidate=3)
     g.step(args.warmup)
     g.synchronize()
     launches0 = C.c_uint64()
@@ -462,7 +464,7 @@ def run_ours(args, ws, rank, local):
 
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(work, args.steps, ws)
+        e2e = run_e2e(work, args.steps, ws, tuning)
 
     naive = None
     if rank == 0 and ws == 1 and not args.no_naive:
@@ -485,7 +487,7 @@ def run_ours(args, ws, rank, local):
                "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                "config": work.config(ws), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-               "gpu_launches": int(launches1.value - launches0.value), "clocks": clk.summary(),
+               "gpu_launches": int(launches1.value - launches0.value), "clocks": clk.summary(), "tuning": tuning,
                "stats": stats, "naive_gpu": naive, "forms": forms}
         print(json.dumps(out), flush=True)
 
@@ -506,6 +508,7 @@ def run_forms(args, ws, local):
     rank = int(os.environ.get("RANK", "0"))
     work = Work("batch64", rank, ws)  # with several GPUs the 64 scenes are split across ranks
     with work.engine(device=local) as b:
+        tuning = b.autotune(steps_per_candidate=3)
         b.step(3)
         b.synchronize()
         barrier(ws)
@@ -519,11 +522,13 @@ def run_forms(args, ws, local):
     out["batched"] = {"workload": "64 seeded scenes split over %d GPU(s); %d particles on rank %d" % (ws, work.n, rank),
                       "steps": steps,
                       "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3,
-                      "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st}
+                      "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st, "tuning": tuning}
     solvers = [s.solver(device=local) for s in work.scenes]
-    # warm-up as for the batch: the first step decides the P2G staging size
-    # (read back at the synchronize), the next steps capture the step graphs
+    # warm-up as for the batch: the autotuner (cached keys: one step), the
+    # first step decides a default P2G staging size (read back at the
+    # synchronize), the next steps capture the step graphs
     for g in solvers:
+        g.autotune(steps_per_candidate=3)
         g.step(1)
     for g in solvers:
         g.synchronize()
@@ -555,7 +560,7 @@ def run_forms(args, ws, local):
     return out
 
 
-def run_e2e(work, steps, ws):
+def run_e2e(work, steps, ws, tuning=None):
     """Same metric through the public API with host buffers: construct the
     solver (or batch) from pinned host arrays (H2D), then every step download
     every scene's (x, y, z, 1) positions into pinned host memory (D2H,
@@ -575,6 +580,11 @@ def run_e2e(work, steps, ws):
     barrier(ws)
     t0 = time.perf_counter()
     g = work.engine(scenes=pinned)
+    if tuning and not work.batched:  # the settings the autotuner chose for this scene
+        g.set_tuning(tuning["g2p_chunk"], tuning["p2g_stage"])
+    elif tuning:
+        for c in tuning["combinations"]:
+            g.set_tuning(c["g2p_chunk"], c["p2g_stage"], c["interpolation"], c["transfer"])
     for k in range(steps):
         g.step(1)
         if work.batched:

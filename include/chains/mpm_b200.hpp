@@ -116,6 +116,17 @@ public:
         check(mpm_solver_download_density(h_, out.data()), "density");
         return out;
     }
+    // writeToOpenVDB (include/mpm_solver3d.h:74): the density grid as an
+    // OpenVDB file with one FloatGrid named "density" (mpm_solver_write_vdb).
+    void writeToOpenVDB(std::string filePath) { check(mpm_solver_write_vdb(h_, filePath.c_str()), "writeToOpenVDB"); }
+    // Launch settings and the autotuner (mpm_solver_autotune); results are
+    // bitwise the same for any setting.
+    mpm_tuning autotune(int stepsPerCandidate = 3, int flags = 0) {
+        check(mpm_solver_autotune(h_, stepsPerCandidate, flags, nullptr), "autotune");
+        mpm_tuning t{};
+        check(mpm_solver_get_tuning(h_, &t), "autotune");
+        return t;
+    }
     // Applies the object in every grid collision (mpm_solver_set_level_set).
     void setCollisionObject(const LevelSetCollisionObject3D& obj) {
         const float v[3] = {obj.velocity.x, obj.velocity.y, obj.velocity.z};

@@ -294,6 +294,19 @@ MPM_API mpm_status mpm_solver_download_wait(mpm_solver* s);
  * an OpenVDB "density" grid; here it is returned headless (no OpenVDB file).
  * Does not change the particle state. */
 MPM_API mpm_status mpm_solver_download_density(mpm_solver* s, float* host_out);
+
+/* Write the density grid of the current state (mpm_solver_download_density)
+ * as an OpenVDB file: one FloatGrid named "density", background 0, the
+ * reference's default transform (voxel size 1: a voxel is a grid node
+ * index), the nodes with non-zero density active, in the standard 5-4-3 tree
+ * of 8^3 leaves (file format version 224, active-mask compression, no zip or
+ * blosc).  Replaces MPMSolver3D::writeToOpenVDB (include/mpm_solver3d.h:74,
+ * src/mpm_solver3d.cu:509-572), which needs the OpenVDB library; this writes
+ * the format directly. */
+MPM_API mpm_status mpm_solver_write_vdb(mpm_solver* s, const char* path);
+/* The same file from a caller's dense density array (res[0] x res[1] x res[2]
+ * floats, index x + X (y + Y z)); host only, no device work. */
+MPM_API mpm_status mpm_write_vdb_density(const float* density, const int32_t* resolution, const char* path);
 /* Download a dense grid field (res^3 * components floats).  Valid after
  * particles_to_grid() and the grid sub-steps of the split API, or after
  * mpm_solver_step when the solver keeps the dense debug grid. */
@@ -340,6 +353,43 @@ MPM_API mpm_status mpm_sort_keys_device_noalloc(const uint32_t* keys, uint32_t n
 MPM_API mpm_status mpm_solver_timed_step(mpm_solver* s, int32_t nsteps, float* ms);
 
 MPM_API mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out);
+
+/* Launch settings of the step kernels (no counterpart in the reference, whose
+ * thrust launches run one thread per particle or node).  They decide how the
+ * work is spread over the GPU and never the order of any sum, so every result
+ * is bitwise the same for any setting.
+ *   g2p_chunk: particles per G2P work item, MPM_G2P_CHUNK_MIN..MPM_G2P_CHUNK_MAX
+ *              (a grid block's particles are split into items of this size);
+ *   p2g_stage: particles staged per P2G warp pass, 16, 24 or 32 (0: chosen
+ *              from the particle density after the first step). */
+typedef struct mpm_tuning {
+    int32_t g2p_chunk;
+    int32_t p2g_stage;
+} mpm_tuning;
+#define MPM_G2P_CHUNK_MIN 256
+#define MPM_G2P_CHUNK_MAX 4096
+
+MPM_API mpm_status mpm_solver_get_tuning(mpm_solver* s, mpm_tuning* out);
+MPM_API mpm_status mpm_solver_set_tuning(mpm_solver* s, const mpm_tuning* t);
+
+/* Autotuner of the launch settings.  The key of a scene is its stencil
+ * (interpolation), its transfer and its bucket of particles per occupied cell
+ * (< 2, < 8, < 32, >= 32), measured by one step.  A key found in the tuning
+ * cache (this process's, then the per-device cache file) takes the cached
+ * settings; otherwise every G2P chunk of {256, 512, 1024, 2048, 4096} and
+ * every P2G staging size of {16, 24, 32} is timed with CUDA events around the
+ * P2G and G2P launches over `steps_per_candidate` steps (after one untimed
+ * step each) and the fastest of each is kept and cached.  The tuning steps
+ * are real steps of the simulation (they advance it; their results are those
+ * of any other settings); *steps_run (may be NULL) returns how many were
+ * taken.  The cache file is $MPM_TUNE_CACHE, else
+ * $XDG_CACHE_HOME/mpm_b200/tuning.txt, else ~/.cache/mpm_b200/tuning.txt.
+ * flags: MPM_TUNE_FORCE measures even cached keys; MPM_TUNE_NO_DISK neither
+ * reads nor writes the file. */
+#define MPM_TUNE_FORCE 1
+#define MPM_TUNE_NO_DISK 2
+MPM_API mpm_status mpm_solver_autotune(mpm_solver* s, int32_t steps_per_candidate, int32_t flags,
+                                       int32_t* steps_run);
 
 /* Total kernel launches issued by this library in this process. */
 MPM_API mpm_status mpm_kernel_launches(uint64_t* count);

@@ -42,6 +42,8 @@ MPM_API mpm_status mpm_batch_download_async(mpm_batch* b, int32_t scene_id, int3
 MPM_API mpm_status mpm_batch_download_wait(mpm_batch* b);
 /* Density grid of one scene (see mpm_solver_download_density). */
 MPM_API mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out);
+/* OpenVDB file of one scene's density grid (see mpm_solver_write_vdb). */
+MPM_API mpm_status mpm_batch_write_vdb(mpm_batch* b, int32_t scene_id, const char* path);
 /* Semi-implicit update of one scene (see mpm_solver_set_implicit). */
 MPM_API mpm_status mpm_batch_set_implicit(mpm_batch* b, int32_t scene_id, float beta, int32_t max_iter, float tol);
 MPM_API mpm_status mpm_batch_solve_info(mpm_batch* b, int32_t scene_id, int32_t* iterations, float* residual);
@@ -56,6 +58,15 @@ MPM_API mpm_status mpm_batch_num_scenes(const mpm_batch* b, int32_t* n);
 MPM_API mpm_status mpm_batch_scene_particles(const mpm_batch* b, int32_t scene_id, size_t* n);
 MPM_API mpm_status mpm_batch_scene_desc(const mpm_batch* b, int32_t scene_id, mpm_scene_desc* desc);
 MPM_API mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out);
+/* Launch settings (see mpm_tuning) of the batch's scenes of one
+ * (interpolation, transfer) combination; -1 in either selects every value
+ * (set) -- get needs both.  Combinations not set use the defaults. */
+MPM_API mpm_status mpm_batch_get_tuning(mpm_batch* b, int32_t interpolation, int32_t transfer, mpm_tuning* out);
+MPM_API mpm_status mpm_batch_set_tuning(mpm_batch* b, int32_t interpolation, int32_t transfer, const mpm_tuning* t);
+/* Autotuner (see mpm_solver_autotune), per (interpolation, transfer,
+ * particles-per-cell bucket) key of each combination in the batch: the batch's
+ * steps time every combination at once. */
+MPM_API mpm_status mpm_batch_autotune(mpm_batch* b, int32_t steps_per_candidate, int32_t flags, int32_t* steps_run);
 /* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */
 MPM_API mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms);
 MPM_API mpm_status mpm_batch_profile(mpm_batch* b, int32_t enable);

@@ -34,6 +34,15 @@ GRID_COMPONENTS = {0: 1, 1: 3, 2: 3, 3: 3}
 KERNEL_FAMILIES = ["keys", "sort", "compact", "stress", "p2g", "grid", "g2p"]
 
 
+# autotuner flags (mpm_solver_autotune)
+TUNE_FORCE, TUNE_NO_DISK = 1, 2
+G2P_CHUNK_MIN, G2P_CHUNK_MAX = 256, 4096
+
+
+class Tuning(C.Structure):
+    _fields_ = [("g2p_chunk", C.c_int32), ("p2g_stage", C.c_int32)]
+
+
 class Material(C.Structure):
     _fields_ = [("youngs_modulus", C.c_float), ("poisson_ratio", C.c_float), ("hardening", C.c_float),
                 ("critical_compression", C.c_float), ("critical_stretch", C.c_float), ("model", C.c_int32)]
@@ -126,6 +135,15 @@ SIGNATURES = {
     "mpm_solver_create_from_config": (C.c_int, [C.POINTER(Config), C.c_int32, C.POINTER(_P), C.POINTER(C.c_int32)]),
     "mpm_solver_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
     "mpm_batch_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
+    "mpm_solver_write_vdb": (C.c_int, [_P, C.c_char_p]),
+    "mpm_batch_write_vdb": (C.c_int, [_P, C.c_int32, C.c_char_p]),
+    "mpm_write_vdb_density": (C.c_int, [_F, C.POINTER(C.c_int32), C.c_char_p]),
+    "mpm_solver_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "mpm_solver_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "mpm_solver_autotune": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "mpm_batch_get_tuning": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(Tuning)]),
+    "mpm_batch_set_tuning": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(Tuning)]),
+    "mpm_batch_autotune": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "mpm_solver_timed_step": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_float)]),
     "mpm_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
     "mpm_batch_timed_step": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_float)]),

@@ -116,6 +116,10 @@ class Batch:
               "mpm_batch_download_density")
         return out.reshape(res[2], res[1], res[0])
 
+    def write_vdb(self, sid: int, path: str):
+        """OpenVDB file of one scene's density grid (see MPMSolver3D.writeToOpenVDB)."""
+        check(self._lib.mpm_batch_write_vdb(self._h, int(sid), os.fsencode(path)), "mpm_batch_write_vdb")
+
     def set_implicit(self, sid: int, beta: float, max_iter: int = 50, tol: float = 1e-5):
         """Semi-implicit update of one scene (see MPMSolver3D.set_implicit)."""
         check(self._lib.mpm_batch_set_implicit(self._h, int(sid), float(beta), int(max_iter), float(tol)),
@@ -154,6 +158,36 @@ class Batch:
 
     def download_wait(self):
         check(self._lib.mpm_batch_download_wait(self._h), "mpm_batch_download_wait")
+
+    def scene_desc(self, sid: int) -> _abi.SceneDesc:
+        d = _abi.SceneDesc()
+        check(self._lib.mpm_batch_scene_desc(self._h, int(sid), C.byref(d)), "mpm_batch_scene_desc")
+        return d
+
+    def tuning(self, interpolation: int, transfer: int) -> dict:
+        """Launch settings of the batch's scenes of one (interpolation,
+        transfer) combination."""
+        t = _abi.Tuning()
+        check(self._lib.mpm_batch_get_tuning(self._h, int(interpolation), int(transfer), C.byref(t)),
+              "mpm_batch_get_tuning")
+        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage)
+
+    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0, interpolation: int = -1, transfer: int = -1):
+        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage))
+        check(self._lib.mpm_batch_set_tuning(self._h, int(interpolation), int(transfer), C.byref(t)),
+              "mpm_batch_set_tuning")
+
+    def autotune(self, steps_per_candidate: int = 3, force: bool = False, use_disk: bool = True) -> dict:
+        """Autotuner over the batch's (stencil, transfer) combinations (see
+        MPMSolver3D.autotune); returns the settings per combination present
+        and the number of steps taken."""
+        flags = (_abi.TUNE_FORCE if force else 0) | (0 if use_disk else _abi.TUNE_NO_DISK)
+        run = C.c_int32(0)
+        check(self._lib.mpm_batch_autotune(self._h, int(steps_per_candidate), flags, C.byref(run)),
+              "mpm_batch_autotune")
+        combos = sorted({(self.scene_desc(sid).interpolation, self.scene_desc(sid).transfer) for sid in self._n})
+        return {"steps": int(run.value),
+                "combinations": [dict(interpolation=i, transfer=t, **self.tuning(i, t)) for i, t in combos]}
 
     def stats(self) -> dict:
         st = _abi.StepStats()

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xcompiler", "-ffp-contract=off"]
 
-SOURCES = ["sort.cu", "kernels.cu", "implicit.cu", "engine.cu", "sort_noalloc.cu", "config.cpp"]
+SOURCES = ["sort.cu", "kernels.cu", "implicit.cu", "engine.cu", "sort_noalloc.cu", "config.cpp", "vdb.cpp"]
 
 
 def _headers():

@@ -11,10 +11,14 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -35,6 +39,7 @@ static mpm_status fail(mpm_status st, const std::string& msg) {
 
 // Error recording for entry points defined in other translation units.
 mpm_status recordError(mpm_status st, const char* msg) { return fail(st, msg ? msg : ""); }
+mpm_status writeDensityVdb(const float* density, const int32_t* res, const char* path);  // vdb.cpp
 
 #define CUDA_TRY(call)                                                                                 \
     do {                                                                                               \
@@ -196,6 +201,58 @@ struct SceneHost {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Tuning cache of the autotuner: launch settings per (device, stencil size,
+// transfer, particles-per-cell bucket), kept for the process and in a text
+// file ("<device> <S> <transfer> <bucket> <g2p_chunk> <p2g_stage>" per line;
+// the last line of a key wins).
+// ---------------------------------------------------------------------------
+struct TuneCache {
+    std::mutex mu;
+    std::map<std::string, mpm_tuning> entries;
+    bool loaded = false;
+
+    static std::string path() {
+        if (const char* e = getenv("MPM_TUNE_CACHE")) return e;
+        std::string dir;
+        if (const char* x = getenv("XDG_CACHE_HOME")) dir = x;
+        else if (const char* h = getenv("HOME")) dir = std::string(h) + "/.cache";
+        else return "";
+        return dir + "/mpm_b200/tuning.txt";
+    }
+    static std::string key(const std::string& dev, int S, int transfer, int bucket) {
+        return dev + " " + std::to_string(S) + " " + std::to_string(transfer) + " " + std::to_string(bucket);
+    }
+    void load() {
+        if (loaded) return;
+        loaded = true;
+        const std::string p = path();
+        if (p.empty()) return;
+        FILE* f = fopen(p.c_str(), "r");
+        if (!f) return;
+        char dev[256];
+        int S, tr, bucket, chunk, stage;
+        while (fscanf(f, "%255s %d %d %d %d %d", dev, &S, &tr, &bucket, &chunk, &stage) == 6)
+            if (chunk >= (int)kMinG2PChunk && chunk <= (int)kMaxG2PChunk && (stage == 16 || stage == 24 || stage == 32))
+                entries[key(dev, S, tr, bucket)] = mpm_tuning{chunk, stage};
+        fclose(f);
+    }
+    void store(const std::string& k, const mpm_tuning& t, bool disk) {
+        entries[k] = t;
+        if (!disk) return;
+        const std::string p = path();
+        if (p.empty()) return;
+        // create the directories of the path (best effort)
+        for (size_t i = 1; i < p.size(); ++i)
+            if (p[i] == '/') mkdir(p.substr(0, i).c_str(), 0755);
+        if (FILE* f = fopen(p.c_str(), "a")) {
+            fprintf(f, "%s %d %d\n", k.c_str(), t.g2p_chunk, t.p2g_stage);
+            fclose(f);
+        }
+    }
+};
+static TuneCache g_tune_cache;
+
 class Engine {
 public:
     struct GraphSlot {
@@ -234,6 +291,9 @@ public:
         if (compact_fork_) cudaEventDestroy(compact_fork_);
         if (compact_join_) cudaEventDestroy(compact_join_);
         releaseScratch();
+        for (auto& e4 : tune_ev_)
+            for (auto e : e4)
+                if (e) cudaEventDestroy(e);
         if (host_word_) cudaFreeHost(host_word_);
         if (stage_event_) cudaEventDestroy(stage_event_);
         if (stream_) cudaStreamDestroy(stream_);
@@ -255,7 +315,7 @@ public:
         DevMem* all[] = {&cell_range_, &block_range_, &solve_pofs_, &solve_prep_, &solve_T_, &solve_iter_,
                          &keys_[0], &keys_[1], &vals_[0], &vals_[1], &sort_scratch_, &inc_scratch_,
                          &compact_scratch_, &block_count_, &sbb_, &active_, &outside_, &counters_, &block_slot_,
-                         &tiles_, &scenes_dev_, &err_, &tmp_};
+                         &tiles_, &scenes_dev_, &err_, &tmp_, &g2p_items_, &tmaps_};
         for (DevMem* m : all) m->release();
     }
 
@@ -688,6 +748,7 @@ public:
             d.transfer = s.desc.transfer;
             d.interp = s.desc.interpolation;
             d.S = s.S;
+            d.combo = comboIndex(s.S, s.desc.transfer);
             d.boundary = s.desc.boundary;
             d.sticky = s.desc.sticky_cells;
             d.pcoll = s.desc.particles_collision;
@@ -739,6 +800,8 @@ public:
         max_active_ = std::max<size_t>(1, std::min<size_t>(tb, nk) + nk / kBlockChunk + 1);
         MPM_TRY(grow(active_, sizeof(BlockItem) * max_active_, "active blocks"));
         MPM_TRY(grow(outside_, sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
+        g2p_cap_ = (uint32_t)(std::min<size_t>(tb, nk) + nk / kMinG2PChunk + 1);
+        MPM_TRY(grow(g2p_items_, sizeof(BlockItem) * g2p_cap_ * (size_t)combos().size(), "G2P items"));
         // [0] work items, [1] outside items, [2] active nodes, [8 + 8k .. 13 + 8k] item
         // schedulers of the k-th stencil/transfer combination
         MPM_TRY(alloc(counters_, sizeof(uint32_t) * 64, "counters"));
@@ -749,6 +812,22 @@ public:
         tile_stride_ = (size_t)7 * tileNodes(maxS);
         MPM_TRY(grow(tiles_, sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
         MPM_TRY(grow(scenes_dev_, sizeof(SceneDev) * std::max(ns, 1), "scene table"));
+        // TMA maps of each scene's v* and v grids (G2P stages its tiles with them)
+        {
+            std::vector<unsigned char> maps((size_t)2 * kTensorMapBytes * std::max(ns, 1), 0);
+            for (int i = 0; i < ns; ++i) {
+                const SceneDev& d = host_scenes_[i];
+                const int T = d.S + 3;
+                const char* e1 = encodeGridTensorMap(maps.data() + (size_t)2 * i * kTensorMapBytes, d.vstar, d.res, T);
+                const char* e2 = encodeGridTensorMap(maps.data() + (size_t)(2 * i + 1) * kTensorMapBytes,
+                                                     d.vold ? (const void*)d.vold : (const void*)d.vstar, d.res, T);
+                if (e1 || e2) return fail(MPM_ERR_CUDA, std::string("grid tensor map: ") + (e1 ? e1 : e2));
+            }
+            MPM_TRY(grow(tmaps_, maps.size(), "grid tensor maps"));
+            if (((uintptr_t)tmaps_.p & 63u) != 0) return fail(MPM_ERR_CUDA, "tensor map table not 64-byte aligned");
+            CUDA_TRY(cudaMemcpyAsync(tmaps_.p, maps.data(), maps.size(), cudaMemcpyHostToDevice, stream_));
+            CUDA_TRY(cudaStreamSynchronize(stream_));  // the host table is freed on return
+        }
         CUDA_TRY(cudaMemcpyAsync(scenes_dev_.p, host_scenes_.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice,
                                  stream_));
         CUDA_TRY(cudaStreamSynchronize(stream_));
@@ -890,6 +969,9 @@ public:
         a.sorted_keys = sorted_keys;
         a.perm = perm;
         a.active = active_.as<BlockItem>();
+        a.g2p_items = g2p_items_.as<BlockItem>();
+        a.g2p_cap = g2p_cap_;
+        a.combo = 0;
         a.counters = counters_.as<uint32_t>();
         a.outside = outside_.as<BlockItem>();
         a.block_slot = block_slot_.as<int32_t>();
@@ -900,6 +982,7 @@ public:
         a.err = err_.as<uint32_t>();
         a.stats = counters_.as<uint32_t>();
         a.sched = counters_.as<uint32_t>() + 8;
+        a.tmaps = tmaps_.as<unsigned char>();
         return a;
     }
 
@@ -909,6 +992,8 @@ public:
         bb.scene_block_base = sbb_.as<uint32_t>();
         bb.active = active_.as<BlockItem>();
         bb.outside = outside_.as<BlockItem>();
+        bb.g2p_items = g2p_items_.as<BlockItem>();
+        bb.g2p_cap = g2p_cap_;
         bb.counters = counters_.as<uint32_t>();
         bb.block_slot = block_slot_.as<int32_t>();
         return bb;
@@ -969,7 +1054,7 @@ public:
             CUDA_TRY(cudaStreamWaitEvent(compact_stream_, compact_fork_, 0));
             LaunchCtx cc = ctx();
             cc.stream = compact_stream_;
-            launchCompactOnesweep(cc, blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(),
+            launchCompactOnesweep(cc, blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, g2pChunks(),
                                   err_.as<uint32_t>());
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaEventRecord(compact_join_, compact_stream_));
@@ -997,7 +1082,7 @@ public:
             CUDA_TRY(cudaStreamWaitEvent(stream_, compact_join_, 0));
         } else {
             mark(KF_COMPACT, 0);
-            launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(),
+            launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, g2pChunks(),
                                   err_.as<uint32_t>());
             mark(KF_COMPACT, 1);
             collect(KF_COMPACT);
@@ -1020,6 +1105,12 @@ public:
             if (!found) c.push_back({s->S, s->desc.transfer});
         }
         return c;
+    }
+    int comboIndex(int S, int transfer) const {
+        auto cs = combos();
+        for (size_t k = 0; k < cs.size(); ++k)
+            if (cs[k].S == S && cs[k].transfer == transfer) return (int)k;
+        return 0;
     }
     std::vector<int> stencilSizes() const {
         std::vector<int> v;
@@ -1107,7 +1198,8 @@ public:
     bool steadyNow() const {
         bool stale = false;
         for (auto& s : scenes_) stale |= s->stress_stale;
-        return use_graphs_ && keys_valid_ && incremental_ok_ && !stale && !profiling_ && !dirty_ && !stage_check_;
+        return use_graphs_ && keys_valid_ && incremental_ok_ && !stale && !profiling_ && !dirty_ && !stage_check_ &&
+               !tune_run_;
     }
 
     // Captures the step of the current host state into g (the host state is
@@ -1210,7 +1302,7 @@ public:
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), keys_[next].as<uint32_t>());
         LaunchCtx c = ctx();
         auto cs = combos();
-        if (cs.size() > 1 && !profiling_ && !any_implicit_) {
+        if (cs.size() > 1 && !profiling_ && !any_implicit_ && !tune_run_) {
             // Scenes of different (stencil, transfer) combinations share no
             // items, tiles or nodes: their P2G -> grid -> G2P chains run
             // concurrently, combination k on side stream k - 1, each with its
@@ -1226,9 +1318,10 @@ public:
                     CUDA_TRY(cudaStreamWaitEvent(ck.stream, fork_, 0));
                 }
                 const int mode = cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP;
+                ck.p2g_stage = p2gStageOf(cs[k]);
                 launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
                 launchGrid(ck, ak, cs[k].S, mode, cs[k].transfer);
-                launchG2P(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true);
+                launchG2P(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
                 if (k > 0) {
                     CUDA_TRY(cudaEventRecord(join_[k - 1], ck.stream));
                     CUDA_TRY(cudaStreamWaitEvent(stream_, join_[k - 1], 0));
@@ -1236,8 +1329,14 @@ public:
             }
         } else {
             mark(KF_P2G, 0);
-            for (auto& k : cs)
-                launchP2G(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+            for (size_t k = 0; k < cs.size(); ++k) {
+                LaunchCtx ck = c;
+                ck.p2g_stage = p2gStageOf(cs[k]);
+                if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][0], stream_));
+                launchP2G(ck, a, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP,
+                          cs[k].transfer);
+                if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][1], stream_));
+            }
             mark(KF_P2G, 1);
             collect(KF_P2G);
             mark(KF_GRID, 0);
@@ -1247,7 +1346,11 @@ public:
             mark(KF_GRID, 1);
             collect(KF_GRID);
             mark(KF_G2P, 0);
-            for (auto& k : cs) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, true);
+            for (size_t k = 0; k < cs.size(); ++k) {
+                if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][2], stream_));
+                launchG2P(c, a, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
+                if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][3], stream_));
+            }
             mark(KF_G2P, 1);
             collect(KF_G2P);
         }
@@ -1257,6 +1360,180 @@ public:
         keys_valid_ = true;   // G2P wrote next step's keys and block counts (and stress)
         sorted_valid_ = false;
         incremental_ok_ = true;  // the live order is now this step's sorted order
+        return MPM_OK;
+    }
+
+    // ---- launch settings and the autotuner ---------------------------------
+    mpm_tuning tuningOf(int S, int transfer) const {
+        auto it = tuning_.find({S, transfer});
+        return it != tuning_.end() ? it->second : mpm_tuning{(int32_t)kDefaultG2PChunk, 0};
+    }
+    int p2gStageOf(const Combo& c) const {
+        const int st = tuningOf(c.S, c.transfer).p2g_stage;
+        return st ? st : p2g_stage_;
+    }
+    G2PChunks g2pChunks() const {
+        G2PChunks g;
+        for (int k = 0; k < kMaxCombos; ++k) g.v[k] = kDefaultG2PChunk;
+        auto cs = combos();
+        for (size_t k = 0; k < cs.size() && k < (size_t)kMaxCombos; ++k)
+            g.v[k] = (uint32_t)tuningOf(cs[k].S, cs[k].transfer).g2p_chunk;
+        return g;
+    }
+    static mpm_status validTuning(const mpm_tuning& t) {
+        if (t.g2p_chunk < (int)kMinG2PChunk || t.g2p_chunk > (int)kMaxG2PChunk)
+            return fail(MPM_ERR_INVALID_ARG, "g2p_chunk must be in [MPM_G2P_CHUNK_MIN, MPM_G2P_CHUNK_MAX]");
+        if (t.p2g_stage != 0 && t.p2g_stage != 16 && t.p2g_stage != 24 && t.p2g_stage != 32)
+            return fail(MPM_ERR_INVALID_ARG, "p2g_stage must be 0, 16, 24 or 32");
+        return MPM_OK;
+    }
+    // interpolation / transfer of -1 select every value.
+    mpm_status setTuning(int interp, int transfer, const mpm_tuning& t) {
+        MPM_TRY(validTuning(t));
+        if (interp < -1 || interp > MPM_INTERP_CUBIC_BSPLINE || transfer < -1 || transfer > MPM_TRANSFER_APIC)
+            return fail(MPM_ERR_INVALID_ARG, "unknown interpolation or transfer");
+        CUDA_TRY(cudaStreamSynchronize(stream_));  // graphs in flight keep their settings
+        for (int i = 0; i <= MPM_INTERP_CUBIC_BSPLINE; ++i)
+            for (int tr = 0; tr <= MPM_TRANSFER_APIC; ++tr)
+                if ((interp < 0 || interp == i) && (transfer < 0 || transfer == tr))
+                    tuning_[{stencilSize(i), tr}] = t;
+        dropGraphs();  // the captured launches carry the settings
+        return MPM_OK;
+    }
+    mpm_status getTuning(int interp, int transfer, mpm_tuning* out) const {
+        if (!out) return fail(MPM_ERR_INVALID_ARG, "null output");
+        if (interp < 0 || interp > MPM_INTERP_CUBIC_BSPLINE || transfer < 0 || transfer > MPM_TRANSFER_APIC)
+            return fail(MPM_ERR_INVALID_ARG, "unknown interpolation or transfer");
+        *out = tuningOf(stencilSize(interp), transfer);
+        return MPM_OK;
+    }
+
+    static int ppcBucket(double ppc) { return ppc < 2.0 ? 0 : ppc < 8.0 ? 1 : ppc < 32.0 ? 2 : 3; }
+
+    // Times one round of candidate settings: one untimed step, then `steps`
+    // steps with events around each combination's P2G and G2P launches;
+    // adds the per-combination times (ms) to p2g_ms / g2p_ms.
+    mpm_status tuneRound(int steps, std::vector<double>* p2g_ms, std::vector<double>* g2p_ms, int* run) {
+        MPM_TRY(stepBody());
+        advanceClock();
+        ++*run;
+        for (int i = 0; i < steps; ++i) {
+            MPM_TRY(stepBody());
+            advanceClock();
+            ++*run;
+            CUDA_TRY(cudaStreamSynchronize(stream_));
+            for (size_t k = 0; k < tune_ev_.size(); ++k) {
+                float a = 0.f, b = 0.f;
+                CUDA_TRY(cudaEventElapsedTime(&a, tune_ev_[k][0], tune_ev_[k][1]));
+                CUDA_TRY(cudaEventElapsedTime(&b, tune_ev_[k][2], tune_ev_[k][3]));
+                (*p2g_ms)[k] += a;
+                (*g2p_ms)[k] += b;
+            }
+        }
+        return MPM_OK;
+    }
+
+    mpm_status autotune(int steps, int flags, int* steps_run) {
+        int run = 0;
+        if (steps_run) *steps_run = 0;
+        if (steps < 1) return fail(MPM_ERR_INVALID_ARG, "steps_per_candidate must be >= 1");
+        MPM_TRY(ensureReady());
+        auto cs = combos();
+        const size_t nc = cs.size();
+        // device name (spaces replaced) for the cache key
+        cudaDeviceProp prop{};
+        CUDA_TRY(cudaGetDeviceProperties(&prop, device_));
+        std::string dev = prop.name;
+        for (auto& ch : dev)
+            if (ch == ' ') ch = '_';
+        std::map<std::pair<int, int>, mpm_tuning> saved = tuning_;
+        for (size_t k = 0; k < nc; ++k) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)kMaxG2PChunk, 0};
+        dropGraphs();
+        while (tune_ev_.size() < nc) {
+            std::array<cudaEvent_t, 4> e4{};
+            for (auto& e : e4) CUDA_TRY(cudaEventCreate(&e));
+            tune_ev_.push_back(e4);
+        }
+        tune_run_ = true;
+        struct Restore {
+            Engine* e;
+            ~Restore() {
+                e->tune_run_ = false;
+                e->dropGraphs();
+            }
+        } restore{this};
+        // Key step: with one G2P item per block (chunk 4096) the G2P item
+        // counts are the occupied blocks of each combination.
+        MPM_TRY(stepBody());
+        advanceClock();
+        ++run;
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        if (stage_pending_) MPM_TRY(checkP2GStage());
+        uint32_t cnt[kMaxCombos] = {};
+        CUDA_TRY(cudaMemcpy(cnt, counters_.as<uint32_t>() + kG2PCountWord, sizeof(cnt), cudaMemcpyDeviceToHost));
+        std::vector<std::string> keys(nc);
+        std::vector<bool> todo(nc, false);
+        bool any = false;
+        {
+            std::lock_guard<std::mutex> lock(g_tune_cache.mu);
+            if (!(flags & MPM_TUNE_NO_DISK)) g_tune_cache.load();
+            for (size_t k = 0; k < nc; ++k) {
+                size_t n = 0;
+                for (auto& sc : scenes_)
+                    if (sc->S == cs[k].S && sc->desc.transfer == cs[k].transfer) n += sc->n;
+                const double ppc = cnt[k] ? (double)n / (64.0 * cnt[k]) : 0.0;
+                keys[k] = TuneCache::key(dev, cs[k].S, cs[k].transfer, ppcBucket(ppc));
+                auto it = g_tune_cache.entries.find(keys[k]);
+                if (it != g_tune_cache.entries.end() && !(flags & MPM_TUNE_FORCE)) {
+                    saved[{cs[k].S, cs[k].transfer}] = it->second;
+                } else {
+                    todo[k] = true;
+                    any = true;
+                }
+            }
+        }
+        if (any) {
+            const uint32_t chunks[] = {256, 512, 1024, 2048, 4096};
+            const int stages[] = {16, 24, 32};
+            std::vector<double> best_g2p(nc, 1e30), p2g_sum[3], p2g_cnt(3, 0.0);
+            std::vector<uint32_t> best_chunk(nc, kDefaultG2PChunk);
+            for (auto& v : p2g_sum) v.assign(nc, 0.0);
+            // round r: G2P chunk r, P2G staging size r mod 3 (the two kernels
+            // do not depend on each other's setting)
+            for (int r = 0; r < 5; ++r) {
+                const int st = r % 3;
+                for (size_t k = 0; k < nc; ++k)
+                    if (todo[k]) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)chunks[r], stages[st]};
+                std::vector<double> pm(nc, 0.0), gm(nc, 0.0);
+                MPM_TRY(tuneRound(steps, &pm, &gm, &run));
+                for (size_t k = 0; k < nc; ++k) {
+                    if (gm[k] < best_g2p[k]) {
+                        best_g2p[k] = gm[k];
+                        best_chunk[k] = chunks[r];
+                    }
+                    p2g_sum[st][k] += pm[k];
+                }
+                p2g_cnt[st] += 1.0;
+            }
+            std::lock_guard<std::mutex> lock(g_tune_cache.mu);
+            for (size_t k = 0; k < nc; ++k) {
+                if (!todo[k]) continue;
+                int bs = 32;
+                double bt = 1e30;
+                for (int st = 0; st < 3; ++st) {
+                    const double t = p2g_sum[st][k] / p2g_cnt[st];
+                    if (t < bt) {
+                        bt = t;
+                        bs = stages[st];
+                    }
+                }
+                const mpm_tuning t{(int32_t)best_chunk[k], bs};
+                saved[{cs[k].S, cs[k].transfer}] = t;
+                g_tune_cache.store(keys[k], t, !(flags & MPM_TUNE_NO_DISK));
+            }
+        }
+        tuning_ = saved;
+        if (steps_run) *steps_run = run;
         return MPM_OK;
     }
 
@@ -1404,6 +1681,8 @@ public:
         if (e) {
             CUDA_TRY(cudaMemset(err_.p, 0, sizeof(uint32_t)));
             if (e & ERR_NONFINITE) return fail(MPM_ERR_NUMERIC, "non-finite particle position detected on the device");
+            if (e & ERR_WAIT_TIMEOUT)
+                return fail(MPM_ERR_TIMEOUT, "a bounded wait for a G2P grid tile gave up; recreate the solver");
             return fail(MPM_ERR_CUDA, "device error flag " + std::to_string(e));
         }
         return MPM_OK;
@@ -1480,7 +1759,11 @@ public:
         MPM_TRY(uploadSceneTable());
         StepArgs a = args(keys_[sorted_].as<uint32_t>(), vals_[sorted_].as<uint32_t>(), nullptr);
         LaunchCtx c = ctx();
-        for (auto& k : combos()) launchG2P(c, a, k.S, k.transfer == MPM_TRANSFER_APIC, false);
+        {
+            auto cs = combos();
+            for (size_t k = 0; k < cs.size(); ++k)
+                launchG2P(c, a, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, false, (int)k);
+        }
         CUDA_TRY(cudaGetLastError());
         host_scenes_ = saved;
         MPM_TRY(uploadSceneTable());
@@ -1772,6 +2055,11 @@ private:
     bool any_implicit_ = false;  // some scene solves the semi-implicit update
     DevMem cell_range_, block_range_, solve_pofs_, solve_prep_, solve_T_, solve_iter_;
     int p2g_stage_ = 32;       // see checkP2GStage()
+    uint32_t g2p_cap_ = 1;   // G2P items per combination (rebuild)
+    // launch settings per (stencil, transfer) combination (mpm_tuning)
+    std::map<std::pair<int, int>, mpm_tuning> tuning_;
+    bool tune_run_ = false;                          // autotune: sequential launches with events
+    std::vector<std::array<cudaEvent_t, 4>> tune_ev_;  // per combination: P2G start/end, G2P start/end
     bool stage_check_ = true;
     // the previous step's sorted keys are aligned with the live particle order
     // (sortLive may sort incrementally); MPM_FULL_SORT=1 always sorts all keys,
@@ -1789,7 +2077,7 @@ private:
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
     DevMem keys_[2], vals_[2], sort_scratch_, inc_scratch_, compact_scratch_, block_count_, sbb_, active_,
-        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_;
+        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_;
     bool profiling_ = false;
     cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)
     // side streams of the concurrent per-combination chains (stepBody)
@@ -2042,6 +2330,18 @@ mpm_status mpm_solver_download_density(mpm_solver* s, float* host_out) {
     MPM_TRY(check(s));
     return s->eng.downloadDensity(s->scene, host_out);
 }
+mpm_status mpm_solver_write_vdb(mpm_solver* s, const char* path) {
+    MPM_TRY(check(s));
+    if (!path) return mpm::fail(MPM_ERR_INVALID_ARG, "null path");
+    try {
+        const mpm_scene_desc& d = s->eng.scene(s->scene)->desc;
+        std::vector<float> rho((size_t)d.resolution[0] * d.resolution[1] * d.resolution[2]);
+        MPM_TRY(s->eng.downloadDensity(s->scene, rho.data()));
+        return mpm::writeDensityVdb(rho.data(), d.resolution, path);
+    } catch (const std::bad_alloc&) {
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+}
 mpm_status mpm_solver_download_grid(mpm_solver* s, int32_t field, float* host_out) {
     MPM_TRY(check(s));
     if (!host_out) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -2081,6 +2381,50 @@ mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out) {
 mpm_status mpm_batch_stats(mpm_batch* b, mpm_step_stats* out) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.stats(out);
+}
+mpm_status mpm_solver_get_tuning(mpm_solver* s, mpm_tuning* out) {
+    MPM_TRY(check(s));
+    const mpm_scene_desc& d = s->eng.scene(s->scene)->desc;
+    return s->eng.getTuning(d.interpolation, d.transfer, out);
+}
+mpm_status mpm_solver_set_tuning(mpm_solver* s, const mpm_tuning* t) {
+    MPM_TRY(check(s));
+    if (!t) return mpm::fail(MPM_ERR_INVALID_ARG, "null tuning");
+    const mpm_scene_desc& d = s->eng.scene(s->scene)->desc;
+    return s->eng.setTuning(d.interpolation, d.transfer, *t);
+}
+mpm_status mpm_solver_autotune(mpm_solver* s, int32_t steps_per_candidate, int32_t flags, int32_t* steps_run) {
+    MPM_TRY(check(s));
+    int run = 0;
+    mpm_status st;
+    try {
+        st = s->eng.autotune(steps_per_candidate, flags, &run);
+    } catch (const std::bad_alloc&) {
+        st = mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+    if (steps_run) *steps_run = run;
+    return st;
+}
+mpm_status mpm_batch_get_tuning(mpm_batch* b, int32_t interpolation, int32_t transfer, mpm_tuning* out) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.getTuning(interpolation, transfer, out);
+}
+mpm_status mpm_batch_set_tuning(mpm_batch* b, int32_t interpolation, int32_t transfer, const mpm_tuning* t) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    if (!t) return mpm::fail(MPM_ERR_INVALID_ARG, "null tuning");
+    return b->eng.setTuning(interpolation, transfer, *t);
+}
+mpm_status mpm_batch_autotune(mpm_batch* b, int32_t steps_per_candidate, int32_t flags, int32_t* steps_run) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    int run = 0;
+    mpm_status st;
+    try {
+        st = b->eng.autotune(steps_per_candidate, flags, &run);
+    } catch (const std::bad_alloc&) {
+        st = mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
+    if (steps_run) *steps_run = run;
+    return st;
 }
 mpm_status mpm_kernel_launches(uint64_t* count) {
     if (!count) return mpm::fail(MPM_ERR_INVALID_ARG, "null output");
@@ -2207,6 +2551,20 @@ mpm_status mpm_batch_download_wait(mpm_batch* b) {
 mpm_status mpm_batch_download_density(mpm_batch* b, int32_t scene_id, float* host_out) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     return b->eng.downloadDensity(scene_id, host_out);
+}
+mpm_status mpm_batch_write_vdb(mpm_batch* b, int32_t scene_id, const char* path) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    if (!path) return mpm::fail(MPM_ERR_INVALID_ARG, "null path");
+    try {
+        const mpm::SceneHost* sc = b->eng.scene(scene_id);
+        if (!sc) return mpm::fail(MPM_ERR_INVALID_ARG, "unknown scene id");
+        const mpm_scene_desc d = sc->desc;
+        std::vector<float> rho((size_t)d.resolution[0] * d.resolution[1] * d.resolution[2]);
+        MPM_TRY(b->eng.downloadDensity(scene_id, rho.data()));
+        return mpm::writeDensityVdb(rho.data(), d.resolution, path);
+    } catch (const std::bad_alloc&) {
+        return mpm::fail(MPM_ERR_OOM, "host allocation failed");
+    }
 }
 mpm_status mpm_batch_set_level_set(mpm_batch* b, int32_t scene_id, const float* phi, float friction,
                                    const float* velocity) {

@@ -22,10 +22,23 @@ namespace mpm {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSortTileKeys = kThreads * 8;  // keys per radix-sort tile (8 per thread)
-// Largest particle count of one P2G/G2P work item: denser blocks are split
-// into several items (each with its own P2G tile, merged in item order), so
-// one crowded block cannot serialize a whole step.
+// Work items: a block's sorted particles are split into
+// ceil(count / kBlockChunk) P2G items of nearly equal size (each with its own
+// P2G tile, merged in item order), so that one crowded block cannot serialize
+// a step.  The split fixes the order of P2G's sums, so it is a constant.
 constexpr uint32_t kBlockChunk = 4096;
+// G2P has no sums across particles, so its work items can be smaller without
+// changing any result: a block is split into ceil(count / chunk) G2P items,
+// which balances the persistent CTAs better than P2G's items.  The chunk is an
+// engine setting (autotuned) in [kMinG2PChunk, kMaxG2PChunk].
+constexpr uint32_t kMinG2PChunk = 256;
+constexpr uint32_t kMaxG2PChunk = 4096;
+constexpr uint32_t kDefaultG2PChunk = 1024;
+// Counter words: [0] work items, [1] outside items, [2] nodes with mass,
+// [8 + 8k .. 13 + 8k] work-item schedulers of combination k (k < 6),
+// [kG2PCountWord + k] G2P items of combination k.
+constexpr int kMaxCombos = 6;
+constexpr int kG2PCountWord = 56;
 
 enum Field : int {
     F_X = 0,
@@ -44,7 +57,12 @@ enum : uint32_t {
     ERR_NONFINITE = 1u,      // a particle position/velocity became NaN/Inf
     ERR_TILE_OVERFLOW = 2u,  // more active blocks than tile slots (never expected)
     ERR_INDEX = 4u,          // a permutation or stencil index failed its range check (never expected)
+    ERR_WAIT_TIMEOUT = 64u,  // a bounded wait for a TMA tile gave up (never expected)
 };
+
+// Bytes of one TMA tensor map (CUtensorMap) and the device-side table of
+// them: per scene, v* then v (PIC-FLIP; APIC repeats v*).
+constexpr int kTensorMapBytes = 128;
 
 struct ParticleBuf {
     float* f;        // NFIELDS * cap
@@ -97,6 +115,7 @@ struct SceneDev {
     uint32_t cap;          // plane stride of the particle buffers
     float dt, gravity, friction, blend, dinv;
     int transfer, interp, S, boundary, sticky, pcoll, nmat;
+    int combo;             // index of the scene's (stencil, transfer) combination in the batch
     int init_pass;         // 1: the mass pass of initialize() covers this scene
     ParticleBuf buf[2];
     float4* vstar;         // dense res^3
@@ -135,6 +154,10 @@ struct StepArgs {
     const uint32_t* sorted_keys; // N
     const uint32_t* perm;        // N: sorted position -> global old slot
     const BlockItem* active;
+    const BlockItem* g2p_items;  // G2P's finer work items: combination k's (any order) at
+                                 // g2p_items + k * g2p_cap, counters[kG2PCountWord + k] of them
+    uint32_t g2p_cap;
+    int combo;                   // the combination a G2P launch serves
     const uint32_t* counters;    // [0] active blocks, [1] outside blocks
     const BlockItem* outside;
     const int32_t* block_slot;   // dense: block -> slot or -1
@@ -145,6 +168,7 @@ struct StepArgs {
     uint32_t* err;               // error flags
     uint32_t* stats;             // [2]: nodes with mass written by the grid pass
     uint32_t* sched;             // work-item schedulers: [0..1] P2G, [4..5] G2P (zero between launches)
+    const unsigned char* tmaps;  // kTensorMapBytes x 2 per scene (64-byte aligned): TMA maps of v*, v
 };
 
 // Dynamic work-item scheduler of the persistent block kernels: sched[0]

@@ -28,7 +28,9 @@ struct BlockBuffers {
     uint32_t* scene_block_base;       // nscenes + 1
     BlockItem* active;                // max_active
     BlockItem* outside;               // nscenes
-    uint32_t* counters;               // [0] active, [1] outside
+    BlockItem* g2p_items;             // G2P work items, g2p_cap per combination
+    uint32_t g2p_cap;
+    uint32_t* counters;               // see kG2PCountWord
     int32_t* block_slot;              // total_blocks
 };
 
@@ -58,12 +60,16 @@ cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint
 // kernels.cu
 void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err);
 size_t compactScratchWords64(uint32_t total_blocks);
+// Particles per G2P work item of each (stencil, transfer) combination.
+struct G2PChunks {
+    uint32_t v[kMaxCombos];
+};
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
-                           unsigned long long* scratch, uint32_t* err);
+                           unsigned long long* scratch, uint32_t chunk, const G2PChunks& g2p_chunks, uint32_t* err);
 void launchStress(const LaunchCtx& c, int parity);
 void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
 void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
-void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused);
+void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused, int combo);
 void launchDenseGravity(const LaunchCtx& c);
 void launchDenseUpdate(const LaunchCtx& c, float dt);
 void launchDenseCollision(const LaunchCtx& c, float dt);
@@ -107,5 +113,8 @@ void launchCfl(const LaunchCtx& c, int parity, size_t max_n, uint32_t* err);
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out);
 void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in);
 size_t p2gSmemBytes(int S, int mode);
+// Writes the kTensorMapBytes TMA tensor map of a dense float4 grid (res[3]
+// nodes) with tile box T^3 to map (host memory); returns null or a message.
+const char* encodeGridTensorMap(void* map, const void* grid, const int* res, int T);
 
 }  // namespace mpm

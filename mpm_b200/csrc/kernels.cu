@@ -11,6 +11,7 @@
 //                   step's stress + particle collision + advection + next key
 //                   (src/mpm_solver3d.cu:316-391,428-445; apic :326-388)
 //   split-mode kernels for the reference's sub-step API.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -174,11 +175,25 @@ __device__ __forceinline__ unsigned long long blockExclusiveScanU64(unsigned lon
     return r;
 }
 
+// The particles [start, start + count) of block b as `items` work items of
+// nearly equal size: count / items each, the first count % items one more.
+__device__ __forceinline__ void splitItems(BlockItem* out, uint32_t b, uint32_t start, uint32_t count,
+                                           uint32_t items, uint32_t scene) {
+    const uint32_t base = count / items, rem = count % items;
+    uint32_t off = 0;
+    for (uint32_t q = 0; q < items; ++q) {
+        const uint32_t len = base + (q < rem ? 1u : 0u);
+        out[q] = BlockItem{b, start + off, len, scene};
+        off += len;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
     uint32_t* __restrict__ block_count, uint32_t total_blocks, const uint32_t* __restrict__ scene_block_base,
     int nscenes, BlockItem* __restrict__ active, BlockItem* __restrict__ outside, uint32_t* __restrict__ counters,
     int32_t* __restrict__ block_slot, unsigned long long* __restrict__ status, uint32_t* __restrict__ tile_counter,
-    uint32_t ntiles, uint32_t* __restrict__ err) {
+    uint32_t ntiles, uint32_t chunk, BlockItem* __restrict__ g2p_items, uint32_t g2p_cap, G2PChunks g2p_chunk,
+    const SceneDev* __restrict__ scenes, uint32_t* __restrict__ err) {
     __shared__ uint32_t tile_s;
     __shared__ unsigned long long tot, excl_s;
     if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
             const uint32_t c = block_count[b];
             const int s = sceneOfBlock(scene_block_base, nscenes, b);
             const bool out = (b == scene_block_base[s + 1] - 1);
-            const unsigned long long items = (c > 0 && !out) ? (unsigned long long)((c + kBlockChunk - 1) / kBlockChunk) : 0ull;
+            const unsigned long long items = (c > 0 && !out) ? (unsigned long long)((c + chunk - 1) / chunk) : 0ull;
             v = (items << 32) | (unsigned long long)c;
         }
         packed[j] = v;
@@ -245,6 +260,42 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
     }
     __syncthreads();
     run += excl_s;
+    // Slots of this thread's G2P items: one atomic per warp when every block
+    // of the warp that has items belongs to one combination (the common
+    // case), else one per block.
+    int scn[kCompactPer];
+    uint32_t gtot = 0;
+    int gcombo = -1;
+    bool mixed = false;
+#pragma unroll
+    for (int j = 0; j < kCompactPer; ++j) {
+        const uint32_t b = b0 + j;
+        scn[j] = 0;
+        if (b >= total_blocks) continue;
+        scn[j] = sceneOfBlock(scene_block_base, nscenes, b);
+        if ((packed[j] >> 32) == 0) continue;
+        const uint32_t count = (uint32_t)(packed[j] & 0xffffffffull);
+        const int k = scenes[scn[j]].combo;
+        gtot += (count + g2p_chunk.v[k] - 1) / g2p_chunk.v[k];
+        if (gcombo < 0) gcombo = k;
+        else mixed |= k != gcombo;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned has = __ballot_sync(0xffffffffu, gtot > 0);
+    const int lead = __shfl_sync(0xffffffffu, gcombo, has ? __ffs(has) - 1 : 0);
+    const bool warp_fast = __all_sync(0xffffffffu, gtot == 0 || (!mixed && gcombo == lead));
+    uint32_t gnext = 0;
+    if (warp_fast && has) {
+        uint32_t inc = gtot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        uint32_t base = 0;
+        if (lane == 31) base = atomicAdd(&counters[kG2PCountWord + lead], inc);
+        gnext = __shfl_sync(0xffffffffu, base, 31) + inc - gtot;
+    }
 #pragma unroll
     for (int j = 0; j < kCompactPer; ++j) {
         const uint32_t b = b0 + j;
@@ -253,23 +304,31 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
         const uint32_t count = (uint32_t)(v & 0xffffffffull);
         const uint32_t items = (uint32_t)(v >> 32);
         const uint32_t start = (uint32_t)(run & 0xffffffffull);
-        const int scene = sceneOfBlock(scene_block_base, nscenes, b);
+        const int scene = scn[j];
+        // a block's items have count / items particles, the first
+        // count % items of them one more (sizes differ by at most one)
         if (items) {
             const uint32_t slot = (uint32_t)(run >> 32);
-            for (uint32_t q = 0; q < items; ++q) {
-                const uint32_t off = q * kBlockChunk;
-                active[slot + q] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
-            }
+            splitItems(active + slot, b, start, count, items, (uint32_t)scene);
             block_slot[b] = (int32_t)slot;
+            // G2P's items of the block, in its combination's list at slots
+            // taken from a counter (their order does not matter)
+            const int k = scenes[scene].combo;
+            const uint32_t parts = (count + g2p_chunk.v[k] - 1) / g2p_chunk.v[k];
+            uint32_t g0;
+            if (warp_fast) {
+                g0 = gnext;
+                gnext += parts;
+            } else {
+                g0 = atomicAdd(&counters[kG2PCountWord + k], parts);
+            }
+            splitItems(g2p_items + (size_t)k * g2p_cap + g0, b, start, count, parts, (uint32_t)scene);
         } else {
             block_slot[b] = -1;
             if (count > 0) {
-                const uint32_t nitems = (count + kBlockChunk - 1) / kBlockChunk;
+                const uint32_t nitems = (count + chunk - 1) / chunk;
                 const uint32_t o = atomicAdd(&counters[1], nitems);
-                for (uint32_t q = 0; q < nitems; ++q) {
-                    const uint32_t off = q * kBlockChunk;
-                    outside[o + q] = BlockItem{b, start + off, min(kBlockChunk, count - off), (uint32_t)scene};
-                }
+                splitItems(outside + o, b, start, count, nitems, (uint32_t)scene);
             }
         }
         block_count[b] = 0;
@@ -336,6 +395,23 @@ __host__ __device__ constexpr int stageStride(int base, int groups) {
     return P;
 }
 
+// One lane's sums for one stencil node, in packed FP32 pairs so that the
+// x and y components go through one __ffma2_rn (two exactly rounded FMAs: the
+// same results as fmaf), and the mass with the z momentum:
+//   mz = (m, p_z), pxy = (p_x, p_y), fxy = (f_x, f_y), fz = f_z.
+// Field f of the tile layout (m, p[3], f[3]) is get(f).
+struct NodeAcc {
+    float2 mz, pxy, fxy;
+    float fz;
+    __device__ __forceinline__ void zero() {
+        mz = pxy = fxy = make_float2(0.f, 0.f);
+        fz = 0.f;
+    }
+    __device__ __forceinline__ float get(int f) const {
+        return f == 0 ? mz.x : f == 1 ? pxy.x : f == 2 ? pxy.y : f == 3 ? mz.y : f == 4 ? fxy.x : f == 5 ? fxy.y : fz;
+    }
+};
+
 template <int S, int MODE, int STAGE = 16>
 struct P2GLayout {
     static constexpr int F = modeFields(MODE);
@@ -350,7 +426,7 @@ struct P2GLayout {
     static constexpr int kStage = STAGE;              // particles staged per warp round
     static constexpr int kSlots = 32;                 // segment partials per round (<= 32: one per lane)
     static constexpr int kSeg = 96;                   // particles per segment (at most)
-    static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg
+    static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg + 1
     // dynamic shared memory: stage [kWarps][kStage][P] floats, partials
     // [kSlots][F][NS] floats, then the control ints (cellBeg[64], cellEnd[64],
     // segCell/segBeg/segEnd[kMaxSeg], ctl[4]); the kernel takes its pointers
@@ -395,14 +471,16 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
         const float* pf = sc.buf[args.parity].f;
         const size_t cap = sc.cap;
 
-        // Cell ranges inside the work item (keys are sorted by cell).
         for (int c = threadIdx.x; c < 64; c += kThreads) cellBeg[c] = cellEnd[c] = 0;
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
-            uint32_t g = it.start + i;
+        const uint32_t i0 = it.start, icount = it.count;
+
+        // Cell ranges inside the work item (keys are sorted by cell).
+        for (uint32_t i = threadIdx.x; i < icount; i += kThreads) {
+            uint32_t g = i0 + i;
             uint32_t c = args.sorted_keys[g] & 63u;
             if (i == 0 || (args.sorted_keys[g - 1] & 63u) != c) cellBeg[c] = (int)i;
-            if (i == it.count - 1 || (args.sorted_keys[g + 1] & 63u) != c) cellEnd[c] = (int)i + 1;
+            if (i == icount - 1 || (args.sorted_keys[g + 1] & 63u) != c) cellEnd[c] = (int)i + 1;
         }
         __syncthreads();
         // Segment list: every non-empty cell cut into runs of at most kSeg
@@ -466,16 +544,14 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                 const int s_first = r0 + __ffs(own) - 1, s_last = r0 + 31 - __clz(own);
                 const int cb = segBeg[s_first], ce = segEnd[s_last];
                 int cur = s_first;  // segment being summed
-                float acc[S][F];
+                NodeAcc acc[S];
 #pragma unroll
-                for (int c = 0; c < S; ++c)
-#pragma unroll
-                    for (int f = 0; f < F; ++f) acc[c][f] = 0.f;
+                for (int c = 0; c < S; ++c) acc[c].zero();
                 for (int g0 = cb; g0 < ce; g0 += L::kStage) {
                     const int np = min(L::kStage, ce - g0);
                     if (lane < np) {
                         float* my = st + lane * L::P;
-                        const uint32_t gs = it.start + (uint32_t)(g0 + lane);
+                        const uint32_t gs = i0 + (uint32_t)(g0 + lane);
                         uint32_t old = args.perm[gs] - sc.key_offset;
                         const bool bad = old >= sc.n;  // range check: flag and contribute nothing
                         if (bad) {
@@ -571,7 +647,7 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                             if (MODE == MODE_MASS) {
                                 const float mw = m * (pq[L::WB + na] * pq[L::WB + S + nb]);
 #pragma unroll
-                                for (int c = 0; c < S; ++c) acc[c][0] = fmaf(mw, pq[L::WB + 2 * S + c], acc[c][0]);
+                                for (int c = 0; c < S; ++c) acc[c].mz.x = fmaf(mw, pq[L::WB + 2 * S + c], acc[c].mz.x);
                                 continue;
                             }
                             // column factors: w = wab Z_c and
@@ -579,13 +655,16 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                             const float2 xa = *reinterpret_cast<const float2*>(pq + L::WB + 2 * na);
                             const float2 yb = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (S + nb));
                             const float wab = xa.x * yb.x, dab = xa.y * yb.x, adb = xa.x * yb.y;
-                            float T[6], u[3], hc2[3];
+                            float T[6];
+                            float2 uxy, mu;  // (u_x, u_y) and (m, u_z)
+                            float2 hxy = make_float2(0.f, 0.f);
+                            float hz = 0.f;
                             if (MODE == MODE_FLIP) {
                                 const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
                                 const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
                                 T[0] = s1.x; T[1] = s1.y; T[2] = s1.z; T[3] = s1.w; T[4] = s2.x; T[5] = s2.y;
-                                u[0] = s0.y; u[1] = s0.z; u[2] = s0.w;
-                                hc2[0] = hc2[1] = hc2[2] = 0.f;
+                                uxy = make_float2(s0.y, s0.z);
+                                mu = make_float2(m, s0.w);
                             } else {
                                 const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
                                 const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
@@ -594,34 +673,38 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                                 const float hC[9] = {s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, s2.w, s3.x};
                                 T[0] = s3.y; T[1] = s3.z; T[2] = s3.w; T[3] = s4.x; T[4] = s4.y; T[5] = s4.z;
                                 const float qv[3] = {s0.y, s0.z, s0.w};
+                                float u[3];
 #pragma unroll
-                                for (int i = 0; i < 3; ++i) {
-                                    u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, qv[i]));
-                                    hc2[i] = hC[3 * i + 2];
-                                }
+                                for (int i = 0; i < 3; ++i) u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, qv[i]));
+                                uxy = make_float2(u[0], u[1]);
+                                mu = make_float2(m, u[2]);
+                                hxy = make_float2(hC[2], hC[5]);
+                                hz = hC[8];
                             }
-                            const float A[3] = {fmaf(T[0], dab, T[3] * adb), fmaf(T[3], dab, T[1] * adb),
-                                                fmaf(T[4], dab, T[5] * adb)};
-                            const float Bz[3] = {T[4] * wab, T[5] * wab, T[2] * wab};
+                            const float2 Axy = make_float2(fmaf(T[0], dab, T[3] * adb), fmaf(T[3], dab, T[1] * adb));
+                            const float Az = fmaf(T[4], dab, T[5] * adb);
+                            const float2 Bxy = make_float2(T[4] * wab, T[5] * wab);
+                            const float Bz = T[2] * wab;
 #pragma unroll
                             for (int c = 0; c < S; ++c) {
                                 const float2 zc = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (2 * S + c));
                                 const float wgt = wab * zc.x;
-                                acc[c][0] = fmaf(m, wgt, acc[c][0]);
-                                if (c > 0 && MODE != MODE_FLIP) {
-#pragma unroll
-                                    for (int i = 0; i < 3; ++i) u[i] += hc2[i];
+                                const float2 w2 = make_float2(wgt, wgt), zx2 = make_float2(zc.x, zc.x),
+                                             zy2 = make_float2(zc.y, zc.y);
+                                if (c > 0 && MODE != MODE_FLIP) {  // u at node c: u += h C e_z, component-wise
+                                    uxy = __fadd2_rn(uxy, hxy);
+                                    mu.y += hz;
                                 }
+                                // m += m w and p_z += w u_z in one pair
+                                acc[c].mz = __ffma2_rn(mu, w2, acc[c].mz);
                                 if (MODE == MODE_APIC_FUSED) {
-#pragma unroll
-                                    for (int i = 0; i < 3; ++i)
-                                        acc[c][1 + i] = fmaf(zc.y, Bz[i], fmaf(zc.x, A[i], fmaf(wgt, u[i], acc[c][1 + i])));
+                                    // p += w u + Z_c A + Z'_c Bz (the order of the nested fmaf)
+                                    acc[c].pxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, __ffma2_rn(w2, uxy, acc[c].pxy)));
+                                    acc[c].mz.y = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].mz.y));
                                 } else {  // PIC-FLIP and SPLIT keep p and f apart
-#pragma unroll
-                                    for (int i = 0; i < 3; ++i) {
-                                        acc[c][1 + i] = fmaf(wgt, u[i], acc[c][1 + i]);
-                                        acc[c][4 + i] = fmaf(zc.y, Bz[i], fmaf(zc.x, A[i], acc[c][4 + i]));
-                                    }
+                                    acc[c].pxy = __ffma2_rn(w2, uxy, acc[c].pxy);
+                                    acc[c].fxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, acc[c].fxy));
+                                    acc[c].fz = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].fz));
                                 }
                             }
                         }
@@ -631,18 +714,19 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
                     // group 0 (fixed order, so the partial does not depend on
                     // timing), write its slot, start the next segment.
 #pragma unroll
-                    for (int c = 0; c < S; ++c)
+                    for (int c = 0; c < S; ++c) {
 #pragma unroll
                         for (int f = 0; f < F; ++f) {
-                            const float mine = acc[c][f];
+                            const float mine = acc[c].get(f);
                             float sum = mine;
 #pragma unroll
                             for (int g = 1; g < L::G; ++g)
                                 sum += __shfl_sync(0xffffffffu, mine, min(lane + g * L::PAIRS, 31));
-                            acc[c][f] = 0.f;
                             if (grp == 0)
                                 partial[(size_t)(cur - r0) * F * L::NS + f * L::NS + na + S * nb + L::PAIRS * c] = sum;
                         }
+                        acc[c].zero();
+                    }
                     ++cur;
                     }
                     __syncwarp();
@@ -763,16 +847,18 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
 #pragma unroll
                     for (int f = 0; f < F; ++f) v[q][f] = cnt[q] > 0 ? tp[q][f * TN] : 0.f;
                 }
+                // A block's items are summed first (from its first item's
+                // tile), then the block's total is added to the node.
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     if (cnt[q] <= 0) continue;
-#pragma unroll
-                    for (int f = 0; f < F; ++f) acc[f] += v[q][f];
                     for (int s2 = 1; s2 < cnt[q]; ++s2) {
                         const float* tile = tp[q] + (size_t)s2 * args.tile_stride;
 #pragma unroll
-                        for (int f = 0; f < F; ++f) acc[f] += tile[f * TN];
+                        for (int f = 0; f < F; ++f) v[q][f] += tile[f * TN];
                     }
+#pragma unroll
+                    for (int f = 0; f < F; ++f) acc[f] += v[q][f];
                 }
             }
             const size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);
@@ -1115,43 +1201,154 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
     if (sc.nmat > 1) sc.buf[args.parity ^ 1].mat[dst] = mid;
 }
 
+// ---------------------------------------------------------------------------
+// TMA (cp.async.bulk.tensor) and mbarrier helpers for G2P's grid tile.  The
+// tensor map of a scene's dense float4 grid is 4-D FP32: (component, x, y, z),
+// so the innermost box extent is one node's 16 bytes and every tile origin is
+// aligned whatever its x; nodes outside the grid read as zeros (OOB fill).
+// The maps cover this GPU's own grid memory; there is no multicast.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarInitFence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Orders this CTA's earlier generic-proxy accesses of shared memory before
+// later async-proxy (TMA) writes to it.
+__device__ __forceinline__ void fenceProxyAsyncShared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tensorMapAcquire(const void* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+}
+// Box of the 4-D map at (0, x, y, z) into dst, completing on bar.
+__device__ __forceinline__ void tmaLoadTile(void* dst, const void* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(smemAddr(dst)),
+        "l"(map), "r"(0), "r"(x), "r"(y), "r"(z), "r"(smemAddr(bar))
+        : "memory");
+}
+
+// Bounded wait for a tile: gives up after ~2^22 polls (seconds), raising
+// ERR_WAIT_TIMEOUT instead of hanging.  Returns false on a timeout.
+__device__ __forceinline__ bool waitTile(uint64_t* bar, unsigned parity, uint32_t* err) {
+    for (uint32_t i = 0; !mbarTryWait(bar, parity); ++i) {
+        if (i > (1u << 22)) {
+            if (threadIdx.x == 0) atomicOr(err, ERR_WAIT_TIMEOUT);
+            return false;
+        }
+        if (i > 64) __nanosleep(64);
+    }
+    return true;
+}
+
+// Origin (node index) of the (S+3)^3 tile of an active block: 4 B - 4 per axis.
+__device__ __forceinline__ void tileOrigin(const SceneDev& sc, uint32_t block, int* t0) {
+    const uint32_t lb = block - sc.block_base;
+    t0[0] = 4 * (int)(lb % (uint32_t)sc.nb[0]) - 4;
+    t0[1] = 4 * (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]) - 4;
+    t0[2] = 4 * (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1])) - 4;
+}
+
+// G2P: persistent CTAs take work items from this combination's list (then the
+// outside items).  While the particles of one item are updated, the tile of
+// v* (and v) of the next item is already on its way into the other of two
+// shared-memory buffers by TMA; one elected thread fetches the next item and
+// issues its copies, every thread waits on the buffer's mbarrier.
 template <int S, bool APIC>
 __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fused) {
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
-    __shared__ float4 tvs[TN];
-    __shared__ float4 tvo[APIC ? 1 : TN];
+    constexpr int TNP = (TN + 7) & ~7;  // buffers 128-byte aligned
+    constexpr unsigned kTileBytes = (unsigned)TN * 16u;
+    __shared__ __align__(128) float4 tvs[2][TNP];
+    __shared__ __align__(128) float4 tvo[APIC ? 1 : 2][APIC ? 8 : TNP];
     __shared__ float pre[kThreads * kPreStride];  // per-thread prefetch row: Fe, Fp, V0
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ uint32_t item_s[2];
     const int want = APIC ? MPM_TRANSFER_APIC : MPM_TRANSFER_PIC_FLIP;
-    const uint32_t nact = args.counters[0];
+    // this combination's own (finer) items of the active blocks, then the
+    // outside items of all scenes (the others' are skipped)
+    const uint32_t nact = args.counters[kG2PCountWord + args.combo];
+    const BlockItem* items = args.g2p_items + (size_t)args.combo * args.g2p_cap;
     const uint32_t nout = args.counters[1];
-    __shared__ uint32_t item_s;
-    for (;;) {
-        const uint32_t w = nextWorkItem(args.sched + 4, nact + nout, &item_s);
-        if (w >= nact + nout) break;
+    const uint32_t total = nact + nout;
+    uint32_t* sched = args.sched + 4;
+
+    // Thread 0: the next item (the last CTA to run out clears the scheduler,
+    // so every launch starts from zero), and its tile copies into buffer b.
+    auto fetch = [&](int b) {
+        const uint32_t w = atomicAdd(&sched[0], 1u);
+        if (w >= total && atomicAdd(&sched[1], 1u) == gridDim.x - 1) {
+            sched[0] = 0u;
+            sched[1] = 0u;
+        }
+        item_s[b] = w;
+        if (w < nact) {  // an active block of this combination: stage its tile
+            const BlockItem it = items[w];
+            const SceneDev& sc = args.scenes[it.scene];
+            int t0[3];
+            tileOrigin(sc, it.block, t0);
+            const unsigned char* maps = args.tmaps + (size_t)it.scene * 2 * kTensorMapBytes;
+            fenceProxyAsyncShared();
+            mbarExpectTx(&bar[b], APIC ? kTileBytes : 2u * kTileBytes);
+            tensorMapAcquire(maps);
+            tmaLoadTile(&tvs[b][0], maps, t0[0], t0[1], t0[2], &bar[b]);
+            if (!APIC) {
+                tensorMapAcquire(maps + kTensorMapBytes);
+                tmaLoadTile(&tvo[b][0], maps + kTensorMapBytes, t0[0], t0[1], t0[2], &bar[b]);
+            }
+        }
+    };
+    if (threadIdx.x == 0) {
+        mbarInit(&bar[0], 1);
+        mbarInit(&bar[1], 1);
+        mbarInitFence();
+        fetch(0);
+    }
+    __syncthreads();
+    unsigned phases = 0u;  // bit b: the parity of buffer b's next wait
+    for (int cur = 0;; cur ^= 1) {
+        const uint32_t w = item_s[cur];
+        if (w >= total) break;
+        // the next item's tile goes into the other buffer, which the previous
+        // item finished reading before the barrier at the end of its loop
+        if (threadIdx.x == 0) fetch(cur ^ 1);
         const bool inside = w < nact;
-        const BlockItem it = inside ? args.active[w] : args.outside[w - nact];
+        const BlockItem it = inside ? items[w] : args.outside[w - nact];
         const SceneDev& sc = args.scenes[it.scene];
-        if (sc.S != S || sc.transfer != want) continue;
         int t0[3] = {0, 0, 0};
         if (inside) {
-            const uint32_t lb = it.block - sc.block_base;
-            t0[0] = 4 * (int)(lb % (uint32_t)sc.nb[0]) - 4;
-            t0[1] = 4 * (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]) - 4;
-            t0[2] = 4 * (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1])) - 4;
-            for (int tn = threadIdx.x; tn < TN; tn += kThreads) {
-                const int n[3] = {t0[0] + tn % T, t0[1] + (tn / T) % T, t0[2] + tn / (T * T)};
-                const bool in = n[0] >= 0 && n[1] >= 0 && n[2] >= 0 && n[0] < sc.res[0] && n[1] < sc.res[1] &&
-                                n[2] < sc.res[2];
-                const size_t node = in ? (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]) : 0;
-                tvs[tn] = in ? sc.vstar[node] : make_float4(0.f, 0.f, 0.f, 0.f);
-                if (!APIC) tvo[tn] = in ? sc.vold[node] : make_float4(0.f, 0.f, 0.f, 0.f);
+            tileOrigin(sc, it.block, t0);
+            const bool ok = waitTile(&bar[cur], (phases >> cur) & 1u, args.err);
+            phases ^= 1u << cur;
+            if (__syncthreads_or(!ok)) {
+                // A tile never arrived (flagged; never expected): wait, again
+                // bounded, for the copies of the other buffer, then stop this
+                // CTA.  The host reports MPM_ERR_TIMEOUT.
+                if (item_s[cur ^ 1] < nact) waitTile(&bar[cur ^ 1], (phases >> (cur ^ 1)) & 1u, args.err);
+                return;
             }
-            __syncthreads();
         }
-        for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
-            particleUpdate<S, APIC>(args, sc, it.start + i, inside ? tvs : nullptr, APIC ? nullptr : tvo, t0,
-                                    fused != 0, pre + threadIdx.x * kPreStride);
+        if (inside || (sc.S == S && sc.transfer == want))
+            for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
+                particleUpdate<S, APIC>(args, sc, it.start + i, inside ? &tvs[cur][0] : nullptr,
+                                        APIC ? nullptr : &tvo[cur][0], t0, fused != 0,
+                                        pre + threadIdx.x * kPreStride);
+        __syncthreads();  // buffer cur is free again; item_s[cur ^ 1] is visible
     }
 }
 
@@ -1368,14 +1565,16 @@ size_t compactScratchWords64(uint32_t total_blocks) {
 }
 
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
-                           unsigned long long* scratch, uint32_t* err) {
+                           unsigned long long* scratch, uint32_t chunk, const G2PChunks& g2p_chunk, uint32_t* err) {
     const uint32_t ntiles = (uint32_t)((total_blocks + kCompactTile - 1) / kCompactTile);
     cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * compactScratchWords64(total_blocks), c.stream);
     cudaMemsetAsync(bb.counters, 0, sizeof(uint32_t) * 4, c.stream);
+    cudaMemsetAsync(bb.counters + kG2PCountWord, 0, sizeof(uint32_t) * kMaxCombos, c.stream);
     noteLaunches(1);
     compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
         bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,
-        bb.block_slot, scratch + 1, reinterpret_cast<uint32_t*>(scratch), ntiles, err);
+        bb.block_slot, scratch + 1, reinterpret_cast<uint32_t*>(scratch), ntiles, chunk, bb.g2p_items, bb.g2p_cap,
+        g2p_chunk, c.scenes, err);
 }
 
 void launchStress(const LaunchCtx& c, int parity) {
@@ -1393,20 +1592,9 @@ static void setP2GAttr() {
     }
 }
 
-// Particles staged per warp round in P2G: 32 (default: all lanes stage, half
-// the per-particle staging cost; measured 0.212 vs 0.221 ms on the 1M-particle
-// cubic APIC scene) or 16 (smaller shared-memory footprint).  MPM_P2G_STAGE=16
-// selects the latter.
-// MPM_P2G_STAGE=16|24|32 overrides the engine's choice (for measurements).
-static int p2gStageOverride() {
-    static int v = [] {
-        const char* e = getenv("MPM_P2G_STAGE");
-        const int k = e ? atoi(e) : 0;
-        return (k == 16 || k == 24 || k == 32) ? k : 0;
-    }();
-    return v;
-}
-
+// Particles staged per warp pass in P2G (16, 24 or 32): the engine's setting
+// (mpm_tuning.p2g_stage, or its choice from the particle density).  Every
+// size gives bitwise the same sums.
 template <int S, int MODE, int STAGE>
 static void p2gLaunch(const LaunchCtx& c, const StepArgs& a, int want) {
     setP2GAttr<S, MODE, STAGE>();
@@ -1415,7 +1603,7 @@ static void p2gLaunch(const LaunchCtx& c, const StepArgs& a, int want) {
 
 template <int S, int MODE>
 static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
-    switch (p2gStageOverride() ? p2gStageOverride() : c.p2g_stage) {
+    switch (c.p2g_stage) {
         case 16: p2gLaunch<S, MODE, 16>(c, a, want); break;
         case 24: p2gLaunch<S, MODE, 24>(c, a, want); break;
         default: p2gLaunch<S, MODE, 32>(c, a, want); break;
@@ -1452,8 +1640,10 @@ void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want
 #undef GRID_CASE
 }
 
-void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused) {
+void launchG2P(const LaunchCtx& c, const StepArgs& args, int S, bool apic, bool fused, int combo) {
     noteLaunches(1);
+    StepArgs a = args;
+    a.combo = combo;
 #define G2P_CASE(SS)                                                                                   \
     if (S == SS) {                                                                                     \
         if (apic) g2pKernel<SS, true><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, fused ? 1 : 0); \
@@ -1574,6 +1764,42 @@ void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int
 void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in) {
     noteLaunches(1);
     scatterFieldKernel<<<c.particle_blocks, kThreads, 0, c.stream>>>(c.scenes, scene, parity, field, comps, in);
+}
+
+// TMA tensor map of a dense float4 grid of res[0] x res[1] x res[2] nodes
+// (node index x + X (y + Y z)) as a 4-D FP32 tensor (component, x, y, z),
+// box (4, T, T, T), zero fill outside the grid.  The encoder is the driver's
+// cuTensorMapEncodeTiled, fetched once through the runtime.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encodeTiledFn() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+const char* encodeGridTensorMap(void* map, const void* grid, const int* res, int T) {
+    static_assert(sizeof(CUtensorMap) == kTensorMapBytes, "tensor map size");
+    EncodeTiledFn fn = encodeTiledFn();
+    if (!fn) return "cuTensorMapEncodeTiled is not available from the driver";
+    if (((uintptr_t)grid & 15u) != 0) return "grid buffer not 16-byte aligned";
+    const cuuint64_t dims[4] = {4, (cuuint64_t)res[0], (cuuint64_t)res[1], (cuuint64_t)res[2]};
+    const cuuint64_t strides[3] = {16, 16ull * (cuuint64_t)res[0], 16ull * (cuuint64_t)res[0] * (cuuint64_t)res[1]};
+    const cuuint32_t box[4] = {4, (cuuint32_t)T, (cuuint32_t)T, (cuuint32_t)T};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                          const_cast<void*>(grid), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? nullptr : "cuTensorMapEncodeTiled rejected the grid tensor map";
 }
 
 size_t p2gSmemBytes(int S, int mode) {

@@ -1,14 +1,15 @@
 // mpm_run.cpp -- headless driver: the reference's demo loop without the GUI.
 //
 //   mpm-run <config.yaml> [--steps N] [--apic] [--out positions.f32]
-//           [--density density.f32] [--cfl C]
+//           [--density density.f32] [--vdb density.vdb] [--cfl C]
 //           [--integration explicit|semi-implicit|implicit] [--max-iter N] [--tol T]
 //
 // parseYAML -> build{,APIC}MPMSolver3DFromYAML -> simulateOneStep() N times
 // (src/demo/mpm-pic-flip/main.cu:47-215 with the GL/ImGui parts replaced by
 // an optional raw float32 (x, y, z, 1) dump of the final positions, and the
-// VDB frame by an optional raw float32 density grid, res_z x res_y x res_x,
-// of the final state), and one JSON line with the timing.  --integration
+// VDB frame by an OpenVDB file of the final density grid (writeToOpenVDB) or
+// a raw float32 density grid, res_z x res_y x res_x), and one JSON line with
+// the timing.  --integration
 // picks the IntegrationType (include/enums.h:17-21), --cfl a CFL time step.
 #include <chrono>
 #include <cstdio>
@@ -21,12 +22,12 @@
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::fprintf(stderr,
-                     "usage: %s config.yaml [--steps N] [--apic] [--out file] [--density file] [--cfl C]\n"
+                     "usage: %s config.yaml [--steps N] [--apic] [--out file] [--density file] [--vdb file] [--cfl C]\n"
                      "       [--integration explicit|semi-implicit|implicit] [--max-iter N] [--tol T]\n",
                      argv[0]);
         return 2;
     }
-    std::string cfg_path = argv[1], out, density;
+    std::string cfg_path = argv[1], out, density, vdb;
     int steps = 100, max_iter = 50;
     float cfl = 0.f, tol = 1e-5f;
     bool apic = false;
@@ -36,6 +37,7 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "--apic")) apic = true;
         else if (!std::strcmp(argv[i], "--out") && i + 1 < argc) out = argv[++i];
         else if (!std::strcmp(argv[i], "--density") && i + 1 < argc) density = argv[++i];
+        else if (!std::strcmp(argv[i], "--vdb") && i + 1 < argc) vdb = argv[++i];
         else if (!std::strcmp(argv[i], "--cfl") && i + 1 < argc) cfl = (float)std::atof(argv[++i]);
         else if (!std::strcmp(argv[i], "--max-iter") && i + 1 < argc) max_iter = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--tol") && i + 1 < argc) tol = (float)std::atof(argv[++i]);
@@ -72,6 +74,7 @@ int main(int argc, char** argv) {
             double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             if (!out.empty()) write(out, solver.positions4());
             if (!density.empty()) write(density, solver.density());
+            if (!vdb.empty()) solver.writeToOpenVDB(vdb);
             std::printf(
                 "{\"particles\": %d, \"steps\": %d, \"seconds\": %.6f, \"particle_steps_per_s\": %.6e, "
                 "\"simulated_time\": %.9g}\n",

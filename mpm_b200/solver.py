@@ -285,6 +285,29 @@ class _SolverBase:
         check(self._lib.mpm_solver_stats(self._h, C.byref(st)), "stats")
         return dict(active_blocks=st.active_blocks, outside_blocks=st.outside_blocks, active_nodes=st.active_nodes)
 
+    # ---- launch settings (no counterpart in the reference) -----------------
+    def tuning(self) -> dict:
+        """Launch settings of the step kernels: particles per G2P work item and
+        particles staged per P2G pass (0 = chosen from density)."""
+        t = _abi.Tuning()
+        check(self._lib.mpm_solver_get_tuning(self._h, C.byref(t)), "get_tuning")
+        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage)
+
+    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0):
+        """Set the launch settings; results are bitwise the same for any."""
+        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage))
+        check(self._lib.mpm_solver_set_tuning(self._h, C.byref(t)), "set_tuning")
+
+    def autotune(self, steps_per_candidate: int = 3, force: bool = False, use_disk: bool = True) -> dict:
+        """Choose the launch settings for this scene's (stencil, transfer,
+        particles-per-cell bucket) from the tuning cache, or by timing the
+        candidates over real steps of the simulation (which advance it).
+        Returns the chosen settings and the number of steps taken."""
+        flags = (_abi.TUNE_FORCE if force else 0) | (0 if use_disk else _abi.TUNE_NO_DISK)
+        run = C.c_int32(0)
+        check(self._lib.mpm_solver_autotune(self._h, int(steps_per_candidate), flags, C.byref(run)), "autotune")
+        return dict(self.tuning(), steps=int(run.value))
+
     def download_into(self, field: int, ptr: int):
         """Download into caller memory at address ptr (e.g. pinned host memory)."""
         check(self._lib.mpm_solver_download(self._h, int(field), C.cast(C.c_void_p(ptr), C.POINTER(C.c_float))),
@@ -302,6 +325,13 @@ class _SolverBase:
         out = np.empty(self._res[0] * self._res[1] * self._res[2], np.float32)
         check(self._lib.mpm_solver_download_density(self._h, out.ctypes.data_as(C.POINTER(C.c_float))), "density")
         return out.reshape(self._res[2], self._res[1], self._res[0])
+
+    def writeToOpenVDB(self, filePath: str):
+        """OpenVDB file of the density grid of the current state: one FloatGrid
+        "density" (MPMSolver3D::writeToOpenVDB, src/mpm_solver3d.cu:509-572)."""
+        check(self._lib.mpm_solver_write_vdb(self._h, os.fsencode(filePath)), "writeToOpenVDB")
+
+    write_vdb = writeToOpenVDB
 
     def download_wait(self):
         check(self._lib.mpm_solver_download_wait(self._h), "download_wait")

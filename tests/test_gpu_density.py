@@ -65,3 +65,26 @@ def test_batch_density_equals_solo(gpu):
         g.step(5)
         assert np.array_equal(g.density(), d)
         g.close()
+
+
+def test_write_vdb_matches_density(gpu, tmp_path):
+    """writeToOpenVDB (solver) and write_vdb (batch) write the density grid
+    of the current state: read back, the active voxels hold exactly the
+    downloaded density and every non-zero node is active."""
+    from vdb_reader import read_vdb
+    from mpm_b200.batch import Batch
+    sc = scenes.tiny_scene(n=5000, res=24, transfer=_abi.TRANSFER_APIC, interpolation=_abi.INTERP_CUBIC)
+    g = sc.solver()
+    g.step(3)
+    g.writeToOpenVDB(str(tmp_path / "s.vdb"))
+    rho = g.density()  # (z, y, x)
+    vox = read_vdb(tmp_path / "s.vdb")["grids"][0]["voxels"]
+    dense = np.zeros_like(rho)
+    for (x, y, z), v in vox.items():
+        dense[z, y, x] = v
+    assert np.array_equal(dense, rho) and len(vox) == int(np.count_nonzero(rho))
+    with Batch() as b:
+        sid = b.add(sc)
+        b.step(3)
+        b.write_vdb(sid, str(tmp_path / "b.vdb"))
+    assert read_vdb(tmp_path / "b.vdb")["grids"][0]["voxels"] == vox

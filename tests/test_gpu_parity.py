@@ -424,3 +424,65 @@ def test_download_async_matches_sync(gpu):
         assert np.array_equal(got.numpy(), ref), f
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("transfer,interp", [(1, 2), (0, 1)])
+def test_results_do_not_depend_on_the_tuned_settings(gpu, transfer, interp):
+    """The settings the autotuner chooses -- particles per G2P work item and
+    particles staged per P2G pass -- change only how work is spread over the
+    CTAs, never the order of a sum, so every result is bitwise the same."""
+    sc = scenes.tiny_scene(n=60000, res=24, transfer=transfer, interpolation=interp)  # ~160 per cell
+    runs = []
+    for chunk, stage in ((1024, 0), (256, 16), (4096, 24), (512, 32)):
+        g = sc.solver()
+        g.set_tuning(g2p_chunk=chunk, p2g_stage=stage)
+        assert g.tuning() == dict(g2p_chunk=chunk, p2g_stage=stage)
+        g.step(3)
+        g.set_tuning(g2p_chunk=4096 if chunk != 4096 else 256, p2g_stage=32)  # changed mid-run
+        g.step(2)
+        runs.append({f: g.download(f) for f in _particle_fields(transfer)})
+        g.close()
+    for r in runs[1:]:
+        for f in _particle_fields(transfer):
+            assert np.array_equal(runs[0][f], r[f]), f
+
+
+def test_autotune_keeps_results_and_caches(gpu, tmp_path, monkeypatch):
+    """The autotuner's steps are ordinary steps (a tuned run equals an untuned
+    run of as many steps, bitwise), its choice is one of the candidates, and a
+    second solver with the same key takes it from the cache without steps."""
+    monkeypatch.setenv("MPM_TUNE_CACHE", str(tmp_path / "tuning.txt"))
+    sc = scenes.tiny_scene(n=30000, res=24, transfer=1, interpolation=2)
+    a = sc.solver()
+    got = a.autotune(steps_per_candidate=1)
+    assert got["g2p_chunk"] in (256, 512, 1024, 2048, 4096) and got["p2g_stage"] in (16, 24, 32)
+    assert got["steps"] == 1 + 5 * 2
+    a.step(2)
+    b = sc.solver()
+    b.step(got["steps"] + 2)
+    for f in _particle_fields(1):
+        assert np.array_equal(a.download(f), b.download(f)), f
+    assert (tmp_path / "tuning.txt").read_text().split()[-2:] == [str(got["g2p_chunk"]), str(got["p2g_stage"])]
+    c = sc.solver()
+    again = c.autotune(steps_per_candidate=1)
+    assert again["steps"] == 1 and again["g2p_chunk"] == got["g2p_chunk"] and again["p2g_stage"] == got["p2g_stage"]
+
+
+def test_batch_autotune_per_combination(gpu, tmp_path, monkeypatch):
+    """In a batch each (stencil, transfer) combination gets its own settings;
+    the tuned batch still equals the solo runs bitwise."""
+    from mpm_b200.batch import Batch
+    monkeypatch.setenv("MPM_TUNE_CACHE", str(tmp_path / "tuning.txt"))
+    specs = [dict(seed=41, n=8000, res=24, transfer=1, interpolation=2),
+             dict(seed=42, n=6000, res=20, transfer=0, interpolation=1)]
+    scs = [scenes.tiny_scene(**s) for s in specs]
+    with Batch() as b:
+        ids = [b.add(sc) for sc in scs]
+        rep = b.autotune(steps_per_candidate=1)
+        assert len(rep["combinations"]) == 2 and rep["steps"] == 11
+        b.step(3)
+        for sc, sid in zip(scs, ids):
+            g = sc.solver()
+            g.step(rep["steps"] + 3)
+            for f in _particle_fields(sc.transfer):
+                assert np.array_equal(b.download(sid, f), g.download(f)), (sc.name, f)

@@ -51,8 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served legs")
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
-    ap.add_argument("--serve-scale", type=float, default=0.02)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-scale", type=float, default=1.0)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-naive", action="store_true", help="skip the reference-naive GPU baseline leg")
     ap.add_argument("--naive-budget-s", type=float, default=10.0)
@@ -299,9 +299,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) per step of a kernel family from one ncu capture
-# (profiles/g2p_two_balls_128.md, p2g_two_balls_128.md, grid_two_balls_128.md,
-# p2g_g2p_batch16.md; batch64 scaled from its 16-scene subset by particles).
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a
+# kernel family, from ncu captures of this bench run separately (ncu --set full
+# --clock-control none -k regex:<kernel> -c 1 on `bench.py --steps 10 --warmup 3
+# --no-e2e --no-cpu-baseline --no-naive --no-forms`, per workload); ncu cannot
+# run inside the timed run, so these are not measured in the run they are
+# printed with.
+TRAFFIC_SOURCE = ("ncu capture of one launch of the kernel in a separate run of this bench on the same workload "
+                  "(dram__bytes_read.sum + dram__bytes_write.sum)")
 NCU_TRAFFIC = {
     "two_balls": {"g2p": 247.3e6, "p2g": 105.0e6, "grid": 4.4e6},
     "batch64": {"g2p": 1.996e9},
@@ -428,11 +433,15 @@ def run_ours(args, ws, rank, local):
     launches0 = C.c_uint64()
     launches1 = C.c_uint64()
     barrier(ws)
+    g.kernel_spans()  # restart the device-side kernel spans
     with ClockSampler(index=local) as clk:
         lib.mpm_kernel_launches(C.byref(launches0))
         ms = g.timed_step(args.steps)
         lib.mpm_kernel_launches(C.byref(launches1))
     barrier(ws)
+    # P2G / grid / G2P time per step measured on the device inside the timed,
+    # graph-replayed steps (first CTA start to last CTA end of each launch)
+    spans = g.kernel_spans()
     # Per-kernel times: the same steps again with CUDA events around every
     # kernel family on the library's stream (this mode launches the kernels
     # of a batch's stencil/transfer combinations one after another and
@@ -449,18 +458,23 @@ def run_ours(args, ws, rank, local):
     value = total / t_max
 
     # the roofline kernel: the longest family among those that move the
-    # state (the sort and compaction are overhead without algorithmic bytes)
-    fams = {k: v for k, v in prof.items() if k in ("p2g", "g2p", "grid")}
-    dom = max(fams, key=lambda k: fams[k][0] * fams[k][1])
-    dur = fams[dom][0] * 1e-3
+    # state (the sort and compaction are overhead without algorithmic bytes),
+    # timed inside the timed steps themselves
+    dom = max(spans, key=lambda k: spans[k][0])
+    dur = spans[dom][0] * 1e-3
     byt = algorithmic_bytes(work.scenes, dom, stats)
     peak, peak_kind = peaks()
     achieved = byt / dur / 1e9 if dur > 0 and byt > 0 else None
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": traffic_of(dom, work.name), "algorithmic_bytes": byt, "avg_launch_ms": fams[dom][0],
+            "traffic": traffic_of(dom, work.name), "traffic_source": TRAFFIC_SOURCE,
+            "algorithmic_bytes": byt, "avg_launch_ms": spans[dom][0],
+            "kernel_ms_in_step": {k: v[0] for k, v in spans.items()}, "span_steps": spans[dom][1],
+            "kernel_timing": "device-measured span of every launch (first CTA start to last CTA end, %globaltimer) "
+                             "inside the timed graph-replayed steps",
             "kernel_ms": {k: v[0] for k, v in prof.items()},
-            "kernel_timing": "CUDA events around each kernel family over %d further steps of the same run" % prof_steps}
+            "kernel_ms_timing": "CUDA events around each kernel family over %d further non-graph steps "
+                                "(sequential launches; includes the sort and compaction)" % prof_steps}
 
     e2e = None
     if not args.no_e2e:
@@ -512,7 +526,9 @@ def run_forms(args, ws, local):
         b.step(3)
         b.synchronize()
         barrier(ws)
+        b.kernel_spans()
         ms = b.timed_step(steps)
+        spans = b.kernel_spans()
         b.profile(True)
         b.timed_step(steps)
         prof = b.profile_read()
@@ -522,6 +538,7 @@ def run_forms(args, ws, local):
     out["batched"] = {"workload": "64 seeded scenes split over %d GPU(s); %d particles on rank %d" % (ws, work.n, rank),
                       "steps": steps,
                       "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3,
+                      "kernel_ms_in_step": {k: v[0] for k, v in spans.items()},
                       "kernel_ms": {k: v[0] for k, v in prof.items()}, "stats": st, "tuning": tuning}
     solvers = [s.solver(device=local) for s in work.scenes]
     # warm-up as for the batch: the autotuner (cached keys: one step), the
@@ -549,13 +566,15 @@ def run_forms(args, ws, local):
     out["plain"] = {"workload": "same 64 scenes as 64 solvers", "steps": steps,
                     "value": allsum(ws, float(work.n * steps)) / t, "ms_per_step": t / steps * 1e3}
     out["batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
-    reqs = scenes.serving_requests(rate=20.0, duration=args.serve_seconds, scale=args.serve_scale)
+    reqs = scenes.serving_requests(rate=20.0, duration=args.serve_seconds, scale=args.serve_scale, lazy=True)
     srv = Server(budget_bytes=150e9, device=local, keep_state=False)
     rep = srv.run(reqs, time_scale=1.0)
     srv.close()
     s = rep.summary()
-    s["stream"] = ("Poisson 20 req/s for %.0f s, particles log-uniform in [%d, %d], 100-500 steps each"
-                   % (args.serve_seconds, max(1, int(5000 * args.serve_scale)), int(2_000_000 * args.serve_scale)))
+    s["stream"] = ("Poisson 20 req/s for %.0f s, particles log-uniform in [%d, %d], 100-500 steps each, "
+                   "grid = bounding box + 4 cells (<= 128^3), 150 GB admission budget; scenes built from their "
+                   "seeds by a helper thread up to 2 s before arrival" % (
+                       args.serve_seconds, max(1, int(5000 * args.serve_scale)), int(2_000_000 * args.serve_scale)))
     out["served"] = s
     return out
 

@@ -396,6 +396,13 @@ MPM_API mpm_status mpm_kernel_launches(uint64_t* count);
 
 /* Timing of the solver's kernels: fills ms[k] with the average device time
  * of kernel family k over the last timed steps (see mpm_solver_profile). */
+/* Device-measured kernel times inside the ordinary (graph-replayed) step:
+ * for the families P2G, grid and G2P (k = 0, 1, 2) the time from the first
+ * CTA's start to the last CTA's end of each launch (%globaltimer), averaged
+ * per step since the last call (summed over the stencil/transfer
+ * combinations of a batch), and the number of steps; the counters restart.
+ * No counterpart in the reference. */
+MPM_API mpm_status mpm_solver_kernel_spans(mpm_solver* s, float* ms, int32_t* counts, int32_t nfamilies);
 MPM_API mpm_status mpm_solver_profile(mpm_solver* s, int32_t enable);
 MPM_API mpm_status mpm_solver_profile_read(mpm_solver* s, float* ms, int32_t* counts, int32_t nfamilies);
 

@@ -25,7 +25,8 @@ MPM_API mpm_status mpm_batch_destroy(mpm_batch* b);
 /* Upload a scene (initialized on the next step); returns its id. */
 MPM_API mpm_status mpm_batch_add_scene(mpm_batch* b, const mpm_scene_desc* desc,
                                const mpm_particles_in* particles, int32_t* scene_id);
-/* Release a scene's device state.  Waits for the batch's stream. */
+/* Release a scene's device state (returned to the memory pool after the
+ * batch's queued steps; does not wait for them). */
 MPM_API mpm_status mpm_batch_remove_scene(mpm_batch* b, int32_t scene_id);
 /* Checkpoint one scene of a batch / add a scene from a checkpoint (the
  * format of mpm_solver_save; a scene saved from a solver or a batch loads into
@@ -35,6 +36,15 @@ MPM_API mpm_status mpm_batch_load_scene(mpm_batch* b, const char* path, int32_t*
 /* Advance every scene nsteps steps (asynchronous). */
 MPM_API mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps);
 MPM_API mpm_status mpm_batch_synchronize(mpm_batch* b);
+/* Per-step device times for a serving loop that does not synchronize every
+ * step.  With timing on (enable = 1), every step is bracketed by two events;
+ * mpm_batch_step_times returns, without waiting, the device times (ms) of up
+ * to `capacity` steps that have completed, oldest first, in *count;
+ * mpm_batch_wait_steps blocks until at most `in_flight` timed steps are still
+ * queued or running (1 keeps the next step queued behind the running one). */
+MPM_API mpm_status mpm_batch_time_steps(mpm_batch* b, int32_t enable);
+MPM_API mpm_status mpm_batch_step_times(mpm_batch* b, float* ms, int32_t capacity, int32_t* count);
+MPM_API mpm_status mpm_batch_wait_steps(mpm_batch* b, int32_t in_flight);
 /* Download a particle field of one scene in its original particle order. */
 MPM_API mpm_status mpm_batch_download(mpm_batch* b, int32_t scene_id, int32_t field, float* host_out);
 /* Asynchronous form (see mpm_solver_download_async) and its wait. */
@@ -69,6 +79,8 @@ MPM_API mpm_status mpm_batch_set_tuning(mpm_batch* b, int32_t interpolation, int
 MPM_API mpm_status mpm_batch_autotune(mpm_batch* b, int32_t steps_per_candidate, int32_t flags, int32_t* steps_run);
 /* nsteps steps bracketed by events on the batch's stream; device ms in *ms. */
 MPM_API mpm_status mpm_batch_timed_step(mpm_batch* b, int32_t nsteps, float* ms);
+/* Kernel spans of the batch's steps (see mpm_solver_kernel_spans). */
+MPM_API mpm_status mpm_batch_kernel_spans(mpm_batch* b, float* ms, int32_t* counts, int32_t nfamilies);
 MPM_API mpm_status mpm_batch_profile(mpm_batch* b, int32_t enable);
 MPM_API mpm_status mpm_batch_profile_read(mpm_batch* b, float* ms, int32_t* counts, int32_t nfamilies);
 

@@ -30,6 +30,8 @@ FIELD_COMPONENTS = {0: 3, 1: 3, 2: 9, 3: 9, 4: 9, 5: 1, 6: 1, 7: 4, 8: 1, 9: 1}
 GRID_MASS, GRID_VELOCITY, GRID_FORCE, GRID_VELOCITY_STAR = 0, 1, 2, 3
 GRID_COMPONENTS = {0: 1, 1: 3, 2: 3, 3: 3}
 
+# kernel families of mpm_solver_kernel_spans (device-measured inside the step)
+SPAN_FAMILIES = ["p2g", "grid", "g2p"]
 # kernel families reported by mpm_solver_profile_read
 KERNEL_FAMILIES = ["keys", "sort", "compact", "stress", "p2g", "grid", "g2p"]
 
@@ -137,6 +139,11 @@ SIGNATURES = {
     "mpm_batch_stats": (C.c_int, [_P, C.POINTER(StepStats)]),
     "mpm_solver_write_vdb": (C.c_int, [_P, C.c_char_p]),
     "mpm_batch_write_vdb": (C.c_int, [_P, C.c_int32, C.c_char_p]),
+    "mpm_batch_time_steps": (C.c_int, [_P, C.c_int32]),
+    "mpm_solver_kernel_spans": (C.c_int, [_P, _F, C.POINTER(C.c_int32), C.c_int32]),
+    "mpm_batch_kernel_spans": (C.c_int, [_P, _F, C.POINTER(C.c_int32), C.c_int32]),
+    "mpm_batch_step_times": (C.c_int, [_P, _F, C.c_int32, C.POINTER(C.c_int32)]),
+    "mpm_batch_wait_steps": (C.c_int, [_P, C.c_int32]),
     "mpm_write_vdb_density": (C.c_int, [_F, C.POINTER(C.c_int32), C.c_char_p]),
     "mpm_solver_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mpm_solver_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),

@@ -116,6 +116,27 @@ class Batch:
               "mpm_batch_download_density")
         return out.reshape(res[2], res[1], res[0])
 
+    def time_steps(self, enable: bool = True):
+        """Bracket every step with events so that step_times() can report device
+        step times without synchronizing (for serving loops)."""
+        check(self._lib.mpm_batch_time_steps(self._h, 1 if enable else 0), "mpm_batch_time_steps")
+
+    def step_times(self, capacity: int = 256) -> list:
+        """Device times (ms) of the timed steps completed since the last call,
+        oldest first; does not wait."""
+        out, got = [], capacity
+        buf = (C.c_float * capacity)()
+        while got == capacity:
+            n = C.c_int32(0)
+            check(self._lib.mpm_batch_step_times(self._h, buf, capacity, C.byref(n)), "mpm_batch_step_times")
+            got = int(n.value)
+            out.extend(buf[:got])
+        return out
+
+    def wait_steps(self, in_flight: int = 1):
+        """Block until at most `in_flight` timed steps are queued or running."""
+        check(self._lib.mpm_batch_wait_steps(self._h, int(in_flight)), "mpm_batch_wait_steps")
+
     def write_vdb(self, sid: int, path: str):
         """OpenVDB file of one scene's density grid (see MPMSolver3D.writeToOpenVDB)."""
         check(self._lib.mpm_batch_write_vdb(self._h, int(sid), os.fsencode(path)), "mpm_batch_write_vdb")
@@ -188,6 +209,16 @@ class Batch:
         combos = sorted({(self.scene_desc(sid).interpolation, self.scene_desc(sid).transfer) for sid in self._n})
         return {"steps": int(run.value),
                 "combinations": [dict(interpolation=i, transfer=t, **self.tuning(i, t)) for i, t in combos]}
+
+    def kernel_spans(self) -> dict:
+        """Device-measured time per step (ms) of the P2G, grid and G2P launches
+        inside the ordinary graph-replayed steps since the last call, and the
+        number of steps: {family: (ms, steps)}."""
+        nf = len(_abi.SPAN_FAMILIES)
+        ms = (C.c_float * nf)()
+        cnt = (C.c_int32 * nf)()
+        check(self._lib.mpm_batch_kernel_spans(self._h, ms, cnt, nf), "mpm_batch_kernel_spans")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_abi.SPAN_FAMILIES)}
 
     def stats(self) -> dict:
         st = _abi.StepStats()

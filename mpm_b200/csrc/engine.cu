@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -291,6 +292,11 @@ public:
         if (compact_fork_) cudaEventDestroy(compact_fork_);
         if (compact_join_) cudaEventDestroy(compact_join_);
         releaseScratch();
+        for (auto& p : step_events_) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+        for (auto e : free_events_) cudaEventDestroy(e);
         for (auto& e4 : tune_ev_)
             for (auto e : e4)
                 if (e) cudaEventDestroy(e);
@@ -315,7 +321,7 @@ public:
         DevMem* all[] = {&cell_range_, &block_range_, &solve_pofs_, &solve_prep_, &solve_T_, &solve_iter_,
                          &keys_[0], &keys_[1], &vals_[0], &vals_[1], &sort_scratch_, &inc_scratch_,
                          &compact_scratch_, &block_count_, &sbb_, &active_, &outside_, &counters_, &block_slot_,
-                         &tiles_, &scenes_dev_, &err_, &tmp_, &g2p_items_, &tmaps_};
+                         &tiles_, &scenes_dev_, &err_, &tmp_, &g2p_items_, &tmaps_, &spans_};
         for (DevMem* m : all) m->release();
     }
 
@@ -427,11 +433,25 @@ public:
         }
         sc->nmat = nmaterials;
         MPM_TRY(sc->mats.allocPooled(sizeof(MaterialDev) * mats.size(), "materials", pool, stream_));
+        // from pageable memory: the copy has taken the data when it returns,
+        // so the host table may be freed without waiting for the stream
         CUDA_TRY(cudaMemcpyAsync(sc->mats.p, mats.data(), sizeof(MaterialDev) * mats.size(), cudaMemcpyHostToDevice,
                                  stream_));
-        CUDA_TRY(cudaStreamSynchronize(stream_));  // the host material table is freed on return
         *out = std::move(sc);
         return MPM_OK;
+    }
+
+    static bool anyPinned(std::initializer_list<const void*> ptrs) {
+        for (const void* p : ptrs) {
+            if (!p) continue;
+            cudaPointerAttributes a{};
+            if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+                cudaGetLastError();
+                return true;  // unknown: wait to be safe
+            }
+            if (a.type != cudaMemoryTypeUnregistered) return true;
+        }
+        return false;
     }
 
     int registerScene(std::unique_ptr<SceneHost> sc) {
@@ -472,8 +492,10 @@ public:
                                          stream_));
             else
                 CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * n, stream_));
-            // the caller's arrays may be freed once this returns
-            CUDA_TRY(cudaStreamSynchronize(stream_));
+            // The caller's arrays may be freed once this returns.  Copies from
+            // pageable memory have taken the data by then; copies from
+            // page-locked memory are asynchronous, so wait for those only.
+            if (anyPinned({p.position, p.velocity, p.mass, p.volume, p.material})) CUDA_TRY(cudaStreamSynchronize(stream_));
         }
         sc->need_init = true;
         sc->stress_stale = true;
@@ -681,7 +703,8 @@ public:
     mpm_status removeScene(int id) {
         for (size_t i = 0; i < scenes_.size(); ++i)
             if (scenes_[i]->id == id) {
-                CUDA_TRY(cudaStreamSynchronize(stream_));
+                // Its device memory returns to the pool in stream order (after
+                // the queued steps), so the host does not wait here.
                 scenes_.erase(scenes_.begin() + i);
                 dirty_ = true;
                 keys_valid_ = false;
@@ -805,6 +828,10 @@ public:
         // [0] work items, [1] outside items, [2] active nodes, [8 + 8k .. 13 + 8k] item
         // schedulers of the k-th stencil/transfer combination
         MPM_TRY(alloc(counters_, sizeof(uint32_t) * 64, "counters"));
+        if (!spans_.p) {
+            MPM_TRY(alloc(spans_, sizeof(unsigned long long) * kSpanWords * kMaxCombos, "kernel spans"));
+            MPM_TRY(resetSpans());
+        }
         CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 64, stream_));
         MPM_TRY(grow(block_slot_, sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
@@ -983,6 +1010,7 @@ public:
         a.stats = counters_.as<uint32_t>();
         a.sched = counters_.as<uint32_t>() + 8;
         a.tmaps = tmaps_.as<unsigned char>();
+        a.spans = nullptr;  // set per combination by the step
         return a;
     }
 
@@ -1313,6 +1341,7 @@ public:
                 LaunchCtx ck = c;
                 StepArgs ak = a;
                 ak.sched = counters_.as<uint32_t>() + 8 + 8 * k;
+                ak.spans = spans_.as<unsigned long long>() + (size_t)kSpanWords * k;
                 if (k > 0) {
                     ck.stream = side_[k - 1];
                     CUDA_TRY(cudaStreamWaitEvent(ck.stream, fork_, 0));
@@ -1332,23 +1361,31 @@ public:
             for (size_t k = 0; k < cs.size(); ++k) {
                 LaunchCtx ck = c;
                 ck.p2g_stage = p2gStageOf(cs[k]);
+                StepArgs ak = a;
+                ak.spans = spans_.as<unsigned long long>() + (size_t)kSpanWords * k;
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][0], stream_));
-                launchP2G(ck, a, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP,
+                launchP2G(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP,
                           cs[k].transfer);
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][1], stream_));
             }
             mark(KF_P2G, 1);
             collect(KF_P2G);
             mark(KF_GRID, 0);
-            for (auto& k : cs)
-                launchGrid(c, a, k.S, k.transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP, k.transfer);
+            for (size_t k = 0; k < cs.size(); ++k) {
+                StepArgs ak = a;
+                ak.spans = spans_.as<unsigned long long>() + (size_t)kSpanWords * k;
+                launchGrid(c, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP,
+                           cs[k].transfer);
+            }
             if (any_implicit_) MPM_TRY(launchSolveAll(false));
             mark(KF_GRID, 1);
             collect(KF_GRID);
             mark(KF_G2P, 0);
             for (size_t k = 0; k < cs.size(); ++k) {
+                StepArgs ak = a;
+                ak.spans = spans_.as<unsigned long long>() + (size_t)kSpanWords * k;
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][2], stream_));
-                launchG2P(c, a, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
+                launchG2P(c, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][3], stream_));
             }
             mark(KF_G2P, 1);
@@ -1361,6 +1398,41 @@ public:
         sorted_valid_ = false;
         incremental_ok_ = true;  // the live order is now this step's sorted order
         return MPM_OK;
+    }
+
+    // ---- kernel spans measured on the device ------------------------------
+    mpm_status resetSpans() {
+        std::vector<unsigned long long> init((size_t)kSpanWords * kMaxCombos, 0ull);
+        for (size_t i = 0; i < init.size(); i += 4) init[i] = ~0ull;
+        CUDA_TRY(cudaMemcpyAsync(spans_.p, init.data(), init.size() * sizeof(unsigned long long),
+                                 cudaMemcpyHostToDevice, stream_));
+        CUDA_TRY(cudaStreamSynchronize(stream_));  // the host table is freed on return
+        return MPM_OK;
+    }
+    // Per family (P2G, grid, G2P): the device time of the family's launches
+    // per step (summed over the stencil/transfer combinations) and the number
+    // of steps, since the last read; the counters restart.
+    mpm_status readSpans(float* ms, int32_t* counts, int n) {
+        if (!spans_.p) {
+            for (int f = 0; f < n; ++f) {
+                if (ms) ms[f] = 0.f;
+                if (counts) counts[f] = 0;
+            }
+            return MPM_OK;
+        }
+        std::vector<unsigned long long> v((size_t)kSpanWords * kMaxCombos);
+        CUDA_TRY(cudaStreamSynchronize(stream_));
+        CUDA_TRY(cudaMemcpy(v.data(), spans_.p, v.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        for (int f = 0; f < n && f < SPAN_FAMILIES; ++f) {
+            unsigned long long sum = 0, cnt = 0;
+            for (int k = 0; k < kMaxCombos; ++k) {
+                sum += v[(size_t)kSpanWords * k + 4 * f + 1];
+                cnt = std::max(cnt, v[(size_t)kSpanWords * k + 4 * f + 2]);
+            }
+            if (ms) ms[f] = cnt ? (float)((double)sum / (double)cnt * 1e-6) : 0.f;
+            if (counts) counts[f] = (int32_t)cnt;
+        }
+        return resetSpans();
     }
 
     // ---- launch settings and the autotuner ---------------------------------
@@ -1576,10 +1648,71 @@ public:
         if (n < 0) return fail(MPM_ERR_INVALID_ARG, "nsteps must be >= 0");
         MPM_TRY(ensureReady());
         for (int i = 0; i < n; ++i) {
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (step_timing_) {
+                MPM_TRY(timingEvent(&e0));
+                MPM_TRY(timingEvent(&e1));
+                CUDA_TRY(cudaEventRecord(e0, stream_));
+            }
             MPM_TRY(stepOnce());
+            if (step_timing_) {
+                CUDA_TRY(cudaEventRecord(e1, stream_));
+                step_events_.push_back({e0, e1});
+            }
             MPM_TRY(checkP2GStage());
             advanceClock();
         }
+        return MPM_OK;
+    }
+
+    // ---- per-step device times without host synchronization ---------------
+    // With step timing on, every step is bracketed by two events on the
+    // stream; stepTimes() hands out the device times of the steps that have
+    // completed (oldest first) without waiting, waitSteps() blocks until at
+    // most `in_flight` timed steps are still queued or running.
+    mpm_status timingEvent(cudaEvent_t* e) {
+        if (!free_events_.empty()) {
+            *e = free_events_.back();
+            free_events_.pop_back();
+            return MPM_OK;
+        }
+        CUDA_TRY(cudaEventCreate(e));
+        return MPM_OK;
+    }
+    mpm_status setStepTiming(bool on) {
+        step_timing_ = on;
+        if (!on) {
+            CUDA_TRY(cudaStreamSynchronize(stream_));
+            for (auto& p : step_events_) {
+                free_events_.push_back(p.first);
+                free_events_.push_back(p.second);
+            }
+            step_events_.clear();
+        }
+        return MPM_OK;
+    }
+    mpm_status stepTimes(float* ms, int cap, int* count) {
+        int k = 0;
+        while (!step_events_.empty() && k < cap) {
+            auto [e0, e1] = step_events_.front();
+            const cudaError_t q = cudaEventQuery(e1);
+            if (q == cudaErrorNotReady) break;
+            CUDA_TRY(q);
+            float t = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            if (ms) ms[k] = t;
+            ++k;
+            step_events_.pop_front();
+            free_events_.push_back(e0);
+            free_events_.push_back(e1);
+        }
+        if (count) *count = k;
+        return MPM_OK;
+    }
+    mpm_status waitSteps(int in_flight) {
+        if (in_flight < 0) return fail(MPM_ERR_INVALID_ARG, "in_flight must be >= 0");
+        const int n = (int)step_events_.size();
+        if (n > in_flight) CUDA_TRY(cudaEventSynchronize(step_events_[n - 1 - in_flight].second));
         return MPM_OK;
     }
 
@@ -2077,8 +2210,11 @@ private:
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
     DevMem keys_[2], vals_[2], sort_scratch_, inc_scratch_, compact_scratch_, block_count_, sbb_, active_,
-        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_;
+        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_, spans_;
     bool profiling_ = false;
+    bool step_timing_ = false;
+    std::deque<std::pair<cudaEvent_t, cudaEvent_t>> step_events_;
+    std::vector<cudaEvent_t> free_events_;
     cudaStream_t copy_stream_ = nullptr;  // asynchronous downloads (downloadAsync)
     // side streams of the concurrent per-combination chains (stepBody)
     static constexpr int kMaxSide = 5;
@@ -2531,6 +2667,29 @@ mpm_status mpm_batch_load_scene(mpm_batch* b, const char* path, int32_t* scene_i
 mpm_status mpm_batch_step(mpm_batch* b, int32_t nsteps) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
     GUARD(b->eng.step(nsteps));
+}
+mpm_status mpm_solver_kernel_spans(mpm_solver* s, float* ms, int32_t* counts, int32_t nfamilies) {
+    MPM_TRY(check(s));
+    return s->eng.readSpans(ms, counts, nfamilies);
+}
+mpm_status mpm_batch_kernel_spans(mpm_batch* b, float* ms, int32_t* counts, int32_t nfamilies) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.readSpans(ms, counts, nfamilies);
+}
+mpm_status mpm_batch_time_steps(mpm_batch* b, int32_t enable) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.setStepTiming(enable != 0);
+}
+mpm_status mpm_batch_step_times(mpm_batch* b, float* ms, int32_t capacity, int32_t* count) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    int n = 0;
+    mpm_status st = b->eng.stepTimes(ms, capacity, &n);
+    if (count) *count = n;
+    return st;
+}
+mpm_status mpm_batch_wait_steps(mpm_batch* b, int32_t in_flight) {
+    if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");
+    return b->eng.waitSteps(in_flight);
 }
 mpm_status mpm_batch_synchronize(mpm_batch* b) {
     if (!b) return mpm::fail(MPM_ERR_INVALID_ARG, "null batch");

@@ -169,7 +169,37 @@ struct StepArgs {
     uint32_t* stats;             // [2]: nodes with mass written by the grid pass
     uint32_t* sched;             // work-item schedulers: [0..1] P2G, [4..5] G2P (zero between launches)
     const unsigned char* tmaps;  // kTensorMapBytes x 2 per scene (64-byte aligned): TMA maps of v*, v
+    unsigned long long* spans;   // this combination's kernel time spans (see KernelSpan), or null
 };
+
+// Kernel time spans measured on the device inside the (graph-replayed) step:
+// per (family, combination) four words -- [0] the earliest CTA start of the
+// running launch (all ones between launches), [1] the sum of the launches'
+// spans in ns, [2] their count, [3] CTAs finished in the running launch.  The
+// last CTA to finish closes the span (%globaltimer, nanoseconds).
+enum KernelSpan : int { SPAN_P2G = 0, SPAN_GRID = 1, SPAN_G2P = 2, SPAN_FAMILIES = 3 };
+constexpr int kSpanWords = 4 * SPAN_FAMILIES;  // per combination
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void spanBegin(unsigned long long* spans, int family) {
+    if (spans && threadIdx.x == 0) atomicMin(&spans[4 * family], globalTimerNs());
+}
+__device__ __forceinline__ void spanEnd(unsigned long long* spans, int family) {
+    if (spans && threadIdx.x == 0) {
+        unsigned long long* sp = spans + 4 * family;
+        __threadfence();
+        if (atomicAdd(&sp[3], 1ull) == (unsigned long long)gridDim.x - 1) {
+            const unsigned long long t1 = globalTimerNs();
+            const unsigned long long t0 = atomicExch(&sp[0], ~0ull);
+            sp[1] += t1 - t0;
+            sp[2] += 1;
+            sp[3] = 0;
+        }
+    }
+}
 
 // Dynamic work-item scheduler of the persistent block kernels: sched[0]
 // hands out item indices, sched[1] counts the CTAs that have run out; the

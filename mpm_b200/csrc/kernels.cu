@@ -419,7 +419,6 @@ struct P2GLayout {
     static constexpr int PAIRS = S * S;               // (a, b) columns; a lane owns one column of S nodes
     static constexpr int G = 32 / PAIRS;              // particle groups per warp (one particle each per pass)
     static constexpr int TN = tileNodes(S);
-    static constexpr int TJ = (TN + kThreads - 1) / kThreads;
     static constexpr int SH = (MODE == MODE_MASS) ? 4 : (MODE == MODE_FLIP ? 12 : 20);  // shared floats
     static constexpr int WB = SH;                     // weight pairs start
     static constexpr int P = stageStride(SH + 6 * S, G);
@@ -427,19 +426,32 @@ struct P2GLayout {
     static constexpr int kSlots = 32;                 // segment partials per round (<= 32: one per lane)
     static constexpr int kSeg = 96;                   // particles per segment (at most)
     static constexpr int kMaxSeg = 128;               // >= 64 + kBlockChunk / kSeg + 1
-    // dynamic shared memory: stage [kWarps][kStage][P] floats, partials
-    // [kSlots][F][NS] floats, then the control ints (cellBeg[64], cellEnd[64],
-    // segCell/segBeg/segEnd[kMaxSeg], ctl[4]); the kernel takes its pointers
-    // from these offsets
-    static constexpr size_t kPartialOff = (size_t)kWarps * kStage * P;
-    static constexpr size_t kCtlOff = kPartialOff + (size_t)kSlots * F * NS;
     static constexpr int kCtlInts = 2 * 64 + 3 * kMaxSeg + 4;
-    static constexpr size_t smemBytes = kCtlOff * 4 + (size_t)kCtlInts * 4;
+    // dynamic shared memory of nw warps: stage [nw][kStage][P] floats,
+    // partials [kSlots][F][NS] floats, then the control ints (cellBeg[64],
+    // cellEnd[64], segCell/segBeg/segEnd[kMaxSeg], ctl[4]); the kernel takes
+    // its pointers from these offsets
+    static constexpr size_t smemFor(int nw) {
+        return ((size_t)nw * kStage * P + (size_t)kSlots * F * NS) * 4 + (size_t)kCtlInts * 4;
+    }
+    // Threads per CTA: where two CTAs of 12 warps fit an SM's shared memory
+    // (the cubic stencil, at most ~113 KB each), 24 warps per SM -- the
+    // register file's limit at 80 registers -- come from two CTAs of 12 warps;
+    // otherwise CTAs of 8 warps (three per SM where they fit).
+    static constexpr int NT = (S == 4 && smemFor(12) <= 113 * 1024) ? 384 : 256;
+    static constexpr int NW = NT / 32;
+    static constexpr int MIN_CTAS = NT == 384 ? 2 : (S == 4 ? 2 : 3);
+    static constexpr int TJ = (TN + NT - 1) / NT;
+    static constexpr size_t kPartialOff = (size_t)NW * kStage * P;
+    static constexpr size_t kCtlOff = kPartialOff + (size_t)kSlots * F * NS;
+    static constexpr size_t smemBytes = smemFor(NW);
+    static_assert(smemBytes == kCtlOff * 4 + (size_t)kCtlInts * 4, "layout");
     static_assert(kMaxSeg >= 64 + (int)(kBlockChunk / kSeg) + 1, "segment list too small");
 };
 
 template <int S, int MODE, int STAGE>
-__global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want_transfer) {
+__global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MODE, STAGE>::MIN_CTAS)
+    p2gKernel(StepArgs args, int want_transfer) {
     using L = P2GLayout<S, MODE, STAGE>;
     constexpr int F = L::F;
     extern __shared__ float4 smem4[];
@@ -460,6 +472,7 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
     const int grp = lane / L::PAIRS, na = (lane % L::PAIRS) % S, nb = (lane % L::PAIRS) / S;
     const bool lane_on = grp < L::G;
     const uint32_t nact = args.counters[0];
+    spanBegin(args.spans, SPAN_P2G);
     __shared__ uint32_t item_s;
     for (;;) {
         const uint32_t w = nextWorkItem(args.sched, nact, &item_s);
@@ -471,12 +484,12 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
         const float* pf = sc.buf[args.parity].f;
         const size_t cap = sc.cap;
 
-        for (int c = threadIdx.x; c < 64; c += kThreads) cellBeg[c] = cellEnd[c] = 0;
+        for (int c = threadIdx.x; c < 64; c += L::NT) cellBeg[c] = cellEnd[c] = 0;
         __syncthreads();
         const uint32_t i0 = it.start, icount = it.count;
 
         // Cell ranges inside the work item (keys are sorted by cell).
-        for (uint32_t i = threadIdx.x; i < icount; i += kThreads) {
+        for (uint32_t i = threadIdx.x; i < icount; i += L::NT) {
             uint32_t g = i0 + i;
             uint32_t c = args.sorted_keys[g] & 63u;
             if (i == 0 || (args.sorted_keys[g - 1] & 63u) != c) cellBeg[c] = (int)i;
@@ -737,7 +750,7 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
             // ---- gather phase: fixed-order merge of this round's segments ----
 #pragma unroll
             for (int j = 0; j < L::TJ; ++j) {
-                const int tn = threadIdx.x + j * kThreads;
+                const int tn = threadIdx.x + j * L::NT;
                 if (tn < L::TN) {
                     const int tx = tn % (S + 3), ty = (tn / (S + 3)) % (S + 3), tz = tn / ((S + 3) * (S + 3));
                     for (int sg = r0; sg < rend; ++sg) {
@@ -757,12 +770,13 @@ __global__ void __launch_bounds__(kThreads, 3) p2gKernel(StepArgs args, int want
         float* tile = args.tiles + (size_t)w * args.tile_stride;
 #pragma unroll
         for (int j = 0; j < L::TJ; ++j) {
-            const int tn = threadIdx.x + j * kThreads;
+            const int tn = threadIdx.x + j * L::NT;
             if (tn < L::TN)
 #pragma unroll
                 for (int f = 0; f < F; ++f) tile[f * L::TN + tn] = tacc[j][f];
         }
     }
+    spanEnd(args.spans, SPAN_P2G);
 }
 
 
@@ -786,6 +800,7 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
     // current one, index (ox + 1) + 3 (oy + 1) + 9 (oz + 1)
     __shared__ int nbSlot[27], nbItems[27];
     const uint32_t nact = args.counters[0];
+    spanBegin(args.spans, SPAN_GRID);
     for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
@@ -922,6 +937,7 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
         }
         __syncthreads();  // the neighbour table is rewritten for the next item
     }
+    spanEnd(args.spans, SPAN_GRID);
 }
 
 // ---------------------------------------------------------------------------
@@ -1096,11 +1112,44 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
         A[k] = dt * gv[k] + ((k % 4 == 0) ? 1.0f : 0.0f);
     }
     matmul3(A, Fe, Fn);
-    float U[9], V[9], s[3];
-    svd3(Fn, U, s, V);
     const uint16_t mid = sc.nmat > 1 ? sc.buf[args.parity].mat[old] : (uint16_t)0;
     const MaterialDev m = sc.mats[mid];
     const float hi = 1.0f + m.theta_s, lo = 1.0f - m.theta_c;
+    const float V0 = pre[18];
+    float mu, la, tau[6];
+    // Elastic fast path: no singular value can be clamped, so Fe = Fn and Fp
+    // stay as they are, and the stress comes from the polar rotation of Fn
+    // (no SVD).  Material bounds beyond 25 % always take the SVD path.
+    const float theta = fmaxf(m.theta_s, m.theta_c);
+    if (theta <= 0.25f && singularValuesInside(Fn, lo, hi)) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Fe[k] = Fn[k];
+        plasticLame(m, Fp, mu, la);
+        const float J = det3(Fn);
+        float P[9];  // 2 mu (F - R) for fixed corotated, mu F for Neo-Hookean
+        float diag;
+        if (m.model == MPM_MODEL_NEO_HOOKEAN) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) P[k] = mu * Fn[k];
+            diag = la * logf(J) - mu;
+        } else {
+            float R[9];
+            polarRotation(Fn, R, theta <= 0.1f ? 3 : 4);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) P[k] = 2.0f * mu * (Fn[k] - R[k]);
+            diag = la * (J - 1.0f) * J;
+        }
+        const int I[6] = {0, 1, 2, 0, 0, 1}, Jx[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            const int i = I[e], j = Jx[e];
+            float v = fmaf(P[3 * i + 2], Fn[3 * j + 2], fmaf(P[3 * i + 1], Fn[3 * j + 1], P[3 * i] * Fn[3 * j]));
+            if (e < 3) v += diag;
+            tau[e] = V0 * v;
+        }
+    } else {
+    float U[9], V[9], s[3];
+    svd3(Fn, U, s, V);
     bool clamped = false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -1135,8 +1184,6 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
         for (int k = 0; k < 9; ++k) Fe[k] = Fn[k];
     }
     // Next step's stress from the clamped SVD (Fe = U S V^T exactly).
-    const float V0 = pre[18];
-    float mu, la, tau[6];
     plasticLame(m, Fp, mu, la);
     if (m.model == MPM_MODEL_NEO_HOOKEAN) {
         bool proj = false;
@@ -1154,6 +1201,7 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
                                     U[3 * i + 2] * s[2] * V[3 * j + 2];
     }
     tauFromSvd(m.model, U, s, mu, la, V0, tau);
+    }
     if (fused) {
         if (sc.pcoll) {  // particlesCollision (src/mpm_solver3d.cu:428-445)
             float pos[3];
@@ -1313,6 +1361,7 @@ __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fuse
             }
         }
     };
+    spanBegin(args.spans, SPAN_G2P);
     if (threadIdx.x == 0) {
         mbarInit(&bar[0], 1);
         mbarInit(&bar[1], 1);
@@ -1350,6 +1399,7 @@ __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fuse
                                         pre + threadIdx.x * kPreStride);
         __syncthreads();  // buffer cur is free again; item_s[cur ^ 1] is visible
     }
+    spanEnd(args.spans, SPAN_G2P);
 }
 
 // ---------------------------------------------------------------------------
@@ -1598,7 +1648,8 @@ static void setP2GAttr() {
 template <int S, int MODE, int STAGE>
 static void p2gLaunch(const LaunchCtx& c, const StepArgs& a, int want) {
     setP2GAttr<S, MODE, STAGE>();
-    p2gKernel<S, MODE, STAGE><<<c.persistent_blocks, kThreads, P2GLayout<S, MODE, STAGE>::smemBytes, c.stream>>>(a, want);
+    p2gKernel<S, MODE, STAGE><<<c.persistent_blocks, P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MODE, STAGE>::smemBytes,
+                                c.stream>>>(a, want);
 }
 
 template <int S, int MODE>

@@ -276,6 +276,61 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* s, float* 
 }
 
 // ---------------------------------------------------------------------------
+// Elastic fast path of the plasticity update.  When no singular value of F
+// leaves (lo, hi), the clamp changes nothing (Fe = F, Fp unchanged) and the
+// stress needs only F and its rotation R = U V^T:
+//   fixed corotated  2 mu U diag(s (s - 1)) U^T = 2 mu (F - R) F^T,
+//   Neo-Hookean      mu U diag(s^2) U^T        = mu F F^T.
+// ---------------------------------------------------------------------------
+// Whether det F > 0 and every singular value of F lies strictly inside
+// (lo, hi): hi^2 I - F^T F and F^T F - lo^2 I both positive definite (leading
+// principal minors > 0, Sylvester).  A case this FP32 test cannot decide
+// (a singular value within rounding of a bound) reports false, and the
+// caller takes the SVD path, which clamps exactly.
+__device__ __forceinline__ bool singularValuesInside(const float* F, float lo, float hi) {
+    float c[3][3];  // F^T F
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = i; j < 3; ++j) c[i][j] = c[j][i] = fmaf(F[6 + i], F[6 + j], fmaf(F[3 + i], F[3 + j], F[i] * F[j]));
+    auto pd = [](float a00, float a11, float a22, float a01, float a02, float a12) {
+        const float m2 = fmaf(a00, a11, -a01 * a01);
+        const float d = a00 * fmaf(a11, a22, -a12 * a12) - a01 * fmaf(a01, a22, -a12 * a02) +
+                        a02 * fmaf(a01, a12, -a11 * a02);
+        return a00 > 0.f && m2 > 0.f && d > 0.f;
+    };
+    const float h2 = hi * hi, l2 = lo * lo;
+    return det3(F) > 0.f && pd(h2 - c[0][0], h2 - c[1][1], h2 - c[2][2], -c[0][1], -c[0][2], -c[1][2]) &&
+           pd(c[0][0] - l2, c[1][1] - l2, c[2][2] - l2, c[0][1], c[0][2], c[1][2]);
+}
+
+// Rotation of the polar decomposition F = R S by Newton's iteration
+// R <- (R + R^-T) / 2 from R = F (quadratic convergence; with every singular
+// value within 10 % of 1, three steps reach FP32 round-off, four within 25 %).
+// R^-T = cof(R) / det R.
+__device__ __forceinline__ void polarRotation(const float* F, float* R, int iterations) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) R[k] = F[k];
+#pragma unroll 1
+    for (int it = 0; it < iterations; ++it) {
+        float c[9];
+        c[0] = fmaf(R[4], R[8], -R[5] * R[7]);
+        c[1] = fmaf(R[5], R[6], -R[3] * R[8]);
+        c[2] = fmaf(R[3], R[7], -R[4] * R[6]);
+        c[3] = fmaf(R[2], R[7], -R[1] * R[8]);
+        c[4] = fmaf(R[0], R[8], -R[2] * R[6]);
+        c[5] = fmaf(R[1], R[6], -R[0] * R[7]);
+        c[6] = fmaf(R[1], R[5], -R[2] * R[4]);
+        c[7] = fmaf(R[2], R[3], -R[0] * R[5]);
+        c[8] = fmaf(R[0], R[4], -R[1] * R[3]);
+        const float det = fmaf(R[0], c[0], fmaf(R[1], c[1], R[2] * c[2]));
+        const float h = 0.5f / det;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) R[k] = fmaf(h, c[k], 0.5f * R[k]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // applyBoundaryCollision (src/collision_object3d.cu:7-54).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void boundaryCollision(const float* pos, float* vel, const float* lo, const float* hi,

@@ -7,8 +7,10 @@ a fixed seed, so every run sees identical inputs.
 """
 from __future__ import annotations
 
+import functools
+import threading
 from dataclasses import dataclass, field
-from typing import List
+from typing import Callable, List, Optional
 
 import numpy as np
 
@@ -101,15 +103,41 @@ def two_balls(seed: int = 1, n: int = 1048576, res: int = 128) -> Scene:
                  _abi.INTERP_CUBIC, steps=200)
 
 
-def _random_scene(rng, idx: int, n: int, res: int, transfer: int) -> Scene:
+def _in_sphere32(rng, n, center, radius):
+    """Uniform points in a ball, generated in float32 (the serving stream's
+    scenes: ~400M points over a 60 s stream)."""
+    out, have = [], 0
+    while have < n:
+        m = 2 * (n - have) + 64
+        p = rng.random((m, 3), dtype=np.float32)
+        p *= 2.0
+        p -= 1.0
+        r2 = p[:, 0] * p[:, 0]
+        r2 += p[:, 1] * p[:, 1]
+        r2 += p[:, 2] * p[:, 2]
+        p = p[r2 <= 1.0]
+        out.append(p)
+        have += p.shape[0]
+    x = np.concatenate(out)[:n] if len(out) > 1 else out[0][:n]
+    x *= np.float32(radius)
+    x += np.asarray(center, np.float32)
+    return np.ascontiguousarray(x)
+
+
+def _random_scene(rng, idx: int, n: int, res: int, transfer: int, fast: bool = False) -> Scene:
     extent = rng.uniform(0.1, 0.3)
     center = rng.uniform(0.2 + extent / 2, 0.8 - extent / 2, size=3)
     if rng.random() < 0.5:
-        x = _in_box(rng, n, center - extent / 2, center + extent / 2)
+        if fast:
+            x = rng.random((n, 3), dtype=np.float32)
+            x *= np.float32(extent)
+            x += (center - extent / 2).astype(np.float32)
+        else:
+            x = _in_box(rng, n, center - extent / 2, center + extent / 2)
         shape_vol = extent ** 3
         shape = "box"
     else:
-        x = _in_sphere(rng, n, center, extent / 2)
+        x = _in_sphere32(rng, n, center, extent / 2) if fast else _in_sphere(rng, n, center, extent / 2)
         shape_vol = 4.0 / 3.0 * np.pi * (extent / 2) ** 3
         shape = "sphere"
     d = rng.normal(size=3)
@@ -120,7 +148,7 @@ def _random_scene(rng, idx: int, n: int, res: int, transfer: int) -> Scene:
     vol = shape_vol / n
     p = Particles(x, v, DENSITY * vol, [mat], volume=np.full(n, vol, np.float32))
     return Scene(f"batch_{idx}_{shape}_{res}", p, (0.0, 0.0, 0.0), (res, res, res), 1.0 / res, 1e-4, transfer,
-                 _abi.INTERP_QUADRATIC, steps=100, meta=dict(extent=extent, shape=shape))
+                 _abi.INTERP_QUADRATIC, steps=100, meta=dict(extent=extent, shape=shape, center=center))
 
 
 def batched_scenes(seed: int = 2, count: int = 64, n_min: int = 10_000, n_max: int = 500_000,
@@ -161,18 +189,65 @@ def large_slab(seed: int = 3, n: int = 8_388_608, res: int = 256) -> Scene:
                  _abi.INTERP_CUBIC, steps=50)
 
 
-@dataclass
 class Request:
-    rid: int
-    arrival: float
-    scene: Scene
+    """A scene-simulation request: arrival time and the scene (particles and
+    step count).  A lazy request builds its scene from its seed when first
+    asked for it (materialize(), or the `scene` attribute), as a client's
+    upload would arrive; `n` is known up front."""
+
+    def __init__(self, rid: int, arrival: float, scene: Optional[Scene] = None, n: int = 0,
+                 factory: Optional[Callable[[], Scene]] = None):
+        self.rid = rid
+        self.arrival = arrival
+        self.n = scene.n if scene is not None else n
+        self._scene = scene
+        self._factory = factory
+        self._lock = threading.Lock()
+
+    def materialize(self) -> Scene:
+        with self._lock:
+            if self._scene is None:
+                self._scene = self._factory()
+            return self._scene
+
+    @property
+    def scene(self) -> Scene:
+        return self.materialize()
+
+    def release(self):
+        """Drop the host copy of the particles (after the upload)."""
+        with self._lock:
+            self._scene = None
+
+
+def _serving_scene(seed: int, rid: int, n: int, transfer: int) -> Scene:
+    srng = np.random.default_rng(np.random.SeedSequence([seed, rid]))
+    srng.uniform()  # the draw of n (made by the caller from the same stream)
+    base = _random_scene(srng, rid, n, 128, transfer, fast=True)
+    # Fit the grid to the shape's bounding box + 4 cells (origin stays 0: the
+    # reference's stencil range ignores the grid origin).
+    h = 1.0 / 128
+    x = base.particles.positions
+    half = base.meta["extent"] / 2
+    lo = (base.meta["center"] - half).astype(np.float32)
+    shift = (np.float32(4 * h) - lo).astype(np.float32)
+    x += shift
+    hi = base.meta["center"] + half + shift
+    base.resolution = tuple(int(min(128, np.ceil(float(e) / h) + 4)) for e in hi)
+    base.stride = h
+    base.steps = int(srng.integers(100, 501))
+    base.name = f"req_{rid}"
+    return base
 
 
 def serving_requests(seed: int = 4, rate: float = 20.0, duration: float = 60.0, n_min: int = 5_000,
-                     n_max: int = 2_000_000, scale: float = 1.0, max_requests: int | None = None) -> List[Request]:
+                     n_max: int = 2_000_000, scale: float = 1.0, max_requests: int | None = None,
+                     lazy: bool = False) -> List[Request]:
     """Poisson arrivals; each request is a random scene as in the batched set
     with N log-uniform in [5k, 2M], a grid of the scene's bounding box plus a
-    4-cell margin (at most 128^3) and a step count uniform in [100, 500]."""
+    4-cell margin (at most 128^3) and a step count uniform in [100, 500].
+    lazy: build each scene only when it is first asked for (a full-size stream
+    holds ~400M particles)."""
     rng = np.random.default_rng(seed)
     t, reqs = 0.0, []
     while True:
@@ -183,21 +258,8 @@ def serving_requests(seed: int = 4, rate: float = 20.0, duration: float = 60.0, 
         srng = np.random.default_rng(np.random.SeedSequence([seed, rid]))
         n = max(1, int(round(np.exp(srng.uniform(np.log(n_min), np.log(n_max))) * scale)))
         transfer = _abi.TRANSFER_APIC if rid % 2 == 0 else _abi.TRANSFER_PIC_FLIP
-        base = _random_scene(srng, rid, n, 128, transfer)
-        # Fit the grid to the bounding box + 4 cells (origin stays 0: the
-        # reference's stencil range ignores the grid origin).
-        h = 1.0 / 128
-        x = base.particles.positions
-        lo = x.min(0)
-        shift = (4 * h - lo).astype(np.float32)
-        x = x + shift
-        res = tuple(int(min(128, np.ceil(float(e) / h) + 4)) for e in x.max(0))
-        base.particles.positions = np.ascontiguousarray(x, np.float32)
-        base.resolution = res
-        base.stride = h
-        base.steps = int(srng.integers(100, 501))
-        base.name = f"req_{rid}"
-        reqs.append(Request(rid, t, base))
+        factory = functools.partial(_serving_scene, seed, rid, n, transfer)
+        reqs.append(Request(rid, t, n=n, factory=factory) if lazy else Request(rid, t, factory()))
     return reqs
 
 

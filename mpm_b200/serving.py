@@ -15,6 +15,7 @@ Reported: per-step latency (p50/p99 of the batched step), time to completion
 """
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional
@@ -101,18 +102,56 @@ class Server:
     def close(self):
         self.batch.close()
 
-    def run(self, requests, time_scale: float = 1.0, max_wall_s: Optional[float] = None) -> ServeReport:
+    def run(self, requests, time_scale: float = 1.0, max_wall_s: Optional[float] = None,
+            prefetch_s: float = 2.0) -> ServeReport:
         """Replay `requests` (mpm_b200.scenes.Request, arrival-ordered).
         Arrival times are divided by `time_scale` (10 replays a 60 s stream in
-        6 s).  Requests larger than the whole budget are rejected."""
+        6 s).  Requests larger than the whole budget are rejected.
+
+        The loop keeps the GPU fed: step k + 1 is queued before the host waits
+        for step k (at most one step in flight behind the running one), and
+        per-step latencies are the device times of the steps, read from events
+        without synchronizing.  A request whose last step has been queued is
+        retired once that step has completed: its final state is downloaded
+        (keep_state) and its memory returns to the pool in stream order.  Scene
+        uploads do not wait for the GPU; a change of the scene set costs one
+        rebuild of the scene table at the next step.  Lazy requests
+        (scenes.serving_requests(lazy=True)) are built by a helper thread up to
+        prefetch_s ahead of their arrival, as a client's upload would arrive,
+        and their host copy is dropped once uploaded."""
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         live: Dict[int, dict] = {}  # scene id -> request bookkeeping
+        done_queue: List[int] = []   # scene ids whose last step is queued
         used = 0.0
         results, lat, sizes, rejected = [], [], [], []
         psteps = 0
+        self.batch.time_steps(True)
         t0 = self.clock()
         qi = 0
         waiting: List = []
+        stop = threading.Event()
+
+        def prefetch():
+            for req in pending:
+                while not stop.is_set() and req.arrival / time_scale > self.clock() - t0 + prefetch_s:
+                    time.sleep(0.01)
+                if stop.is_set():
+                    return
+                req.materialize()
+
+        helper = threading.Thread(target=prefetch, daemon=True)
+        helper.start()
+
+        def retire(sid):
+            nonlocal used
+            rec = live.pop(sid)
+            req = rec["req"]
+            state = {f: self.batch.download(sid, f) for f in FIELDS_OUT} if self.keep_state else {}
+            self.batch.remove(sid)
+            used -= rec["need"]
+            results.append(RequestResult(req.rid, rec["n"], rec["steps"], req.arrival / time_scale,
+                                         rec["admitted"], self.clock() - t0, state))
+
         while qi < len(pending) or waiting or live:
             now = self.clock() - t0
             if max_wall_s is not None and now > max_wall_s:
@@ -120,6 +159,13 @@ class Server:
             while qi < len(pending) and pending[qi].arrival / time_scale <= now:
                 waiting.append(pending[qi])
                 qi += 1
+            # retire the requests whose last step has been queued, once it has
+            # completed (the scene set changes anyway: the next step rebuilds)
+            if done_queue:
+                self.batch.wait_steps(0)
+                for sid in done_queue:
+                    retire(sid)
+                done_queue = []
             # admission: first fit in arrival order against the memory budget
             still = []
             for req in waiting:
@@ -128,37 +174,40 @@ class Server:
                     rejected.append(req.rid)
                     continue
                 if used + need <= self.budget:
-                    sid = self.batch.add(req.scene)
-                    live[sid] = dict(req=req, left=req.scene.steps, need=need, admitted=self.clock() - t0)
+                    sc = req.scene
+                    sid = self.batch.add(sc)
+                    live[sid] = dict(req=req, left=sc.steps, need=need, admitted=self.clock() - t0, n=sc.n,
+                                     steps=sc.steps)
                     used += need
+                    if req._factory is not None:
+                        req.release()  # uploaded: the host copy is no longer needed
                 else:
                     still.append(req)
             waiting = still
-            if not live:
+            stepping = [sid for sid in live if live[sid]["left"] > 0]
+            if not stepping:
                 if qi < len(pending):  # idle until the next arrival
                     delay = pending[qi].arrival / time_scale - (self.clock() - t0)
                     if delay > 0:
                         time.sleep(min(delay, 0.05))
                 continue
-            # one batched step of every in-flight scene
-            ts = self.clock()
+            # one batched step of every in-flight scene, queued behind the running one
             self.batch.step(1)
-            self.batch.synchronize()
-            lat.append((self.clock() - ts) * 1e3)
-            sizes.append(len(live))
-            psteps += self.batch.num_particles
-            # retire finished requests
-            for sid in list(live):
-                rec = live[sid]
-                rec["left"] -= 1
-                if rec["left"] <= 0:
-                    req = rec["req"]
-                    state = {f: self.batch.download(sid, f) for f in FIELDS_OUT} if self.keep_state else {}
-                    self.batch.remove(sid)
-                    used -= rec["need"]
-                    results.append(RequestResult(req.rid, req.scene.n, req.scene.steps, req.arrival / time_scale,
-                                                 rec["admitted"], self.clock() - t0, state))
-                    del live[sid]
+            sizes.append(len(stepping))
+            psteps += sum(live[sid]["n"] for sid in stepping)
+            for sid in stepping:
+                live[sid]["left"] -= 1
+                if live[sid]["left"] == 0:
+                    done_queue.append(sid)
+            self.batch.wait_steps(1)
+            lat.extend(self.batch.step_times())
+        stop.set()
+        helper.join()
+        self.batch.synchronize()
+        for sid in done_queue:
+            retire(sid)
+        lat.extend(self.batch.step_times())
+        self.batch.time_steps(False)
         wall = self.clock() - t0
         return ServeReport(results, lat, sizes, psteps, wall, rejected)
 

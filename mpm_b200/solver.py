@@ -280,6 +280,16 @@ class _SolverBase:
         check(self._lib.mpm_solver_timed_step(self._h, int(nsteps), C.byref(ms)), "timed_step")
         return float(ms.value)
 
+    def kernel_spans(self) -> dict:
+        """Device-measured time per step (ms) of the P2G, grid and G2P launches
+        inside the ordinary graph-replayed steps since the last call, and the
+        number of steps: {family: (ms, steps)}."""
+        nf = len(_abi.SPAN_FAMILIES)
+        ms = (C.c_float * nf)()
+        cnt = (C.c_int32 * nf)()
+        check(self._lib.mpm_solver_kernel_spans(self._h, ms, cnt, nf), "mpm_solver_kernel_spans")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_abi.SPAN_FAMILIES)}
+
     def stats(self) -> dict:
         st = _abi.StepStats()
         check(self._lib.mpm_solver_stats(self._h, C.byref(st)), "stats")

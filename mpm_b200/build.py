@@ -28,6 +28,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xcompiler", "-ffp-contract=off"]
 
+# Extra nvcc flags (space separated) for builds of variants, e.g. a -D of a
+# launch-bound setting.
+EXTRA = os.environ.get("MPM_NVCC_EXTRA", "").split()
+
 SOURCES = ["sort.cu", "kernels.cu", "implicit.cu", "engine.cu", "sort_noalloc.cu", "config.cpp", "vdb.cpp"]
 
 
@@ -66,7 +70,7 @@ def build(verbose: bool = False) -> str:
         o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if _stale(o, [s] + headers):
-            jobs.append([NVCC, *ARCH, *FLAGS, "-c", s, "-o", o])
+            jobs.append([NVCC, *ARCH, *FLAGS, *EXTRA, "-c", s, "-o", o])
     if jobs:
         with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
             list(ex.map(lambda c: _run(c, verbose), jobs))

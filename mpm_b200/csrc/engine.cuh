@@ -70,7 +70,9 @@ struct ParticleBuf {
     uint16_t* mat;   // cap
 };
 
-struct MaterialDev {
+// 16-byte aligned (sizeof 32) so that G2P can bulk-copy a scene's first
+// material into shared memory.
+struct alignas(16) MaterialDev {
     float mu0, lambda0, xi, theta_c, theta_s;
     int model;
 };
@@ -102,7 +104,9 @@ struct SolveDev {
     SolveStatus* status;
 };
 
-struct SceneDev {
+// 16-byte aligned (sizeof a multiple of 16) so that the block kernels can
+// bulk-copy a scene's entry into shared memory.
+struct alignas(16) SceneDev {
     float origin[3];
     float h, inv_h, range;
     float target[3];

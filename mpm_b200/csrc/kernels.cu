@@ -474,18 +474,28 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
     const uint32_t nact = args.counters[0];
     spanBegin(args.spans, SPAN_P2G);
     __shared__ uint32_t item_s;
+    __shared__ SceneDev sc_s;
     for (;;) {
         const uint32_t w = nextWorkItem(args.sched, nact, &item_s);
         if (w >= nact) break;
         const BlockItem it = args.active[w];
-        const SceneDev& sc = args.scenes[it.scene];
-        if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
-        if (MODE == MODE_MASS && !sc.init_pass) continue;
-        const float* pf = sc.buf[args.parity].f;
-        const size_t cap = sc.cap;
-
+        {
+            const SceneDev& scg = args.scenes[it.scene];
+            if (scg.S != S || (want_transfer >= 0 && scg.transfer != want_transfer)) continue;
+            if (MODE == MODE_MASS && !scg.init_pass) continue;
+        }
+        // the scene's entry into shared memory: the staging reads its fields
+        // per particle
+        if (warp == 0) {
+            const int4* src = reinterpret_cast<const int4*>(args.scenes + it.scene);
+            int4* dst = reinterpret_cast<int4*>(&sc_s);
+            for (int q = lane; q < (int)(sizeof(SceneDev) / 16); q += 32) dst[q] = src[q];
+        }
         for (int c = threadIdx.x; c < 64; c += L::NT) cellBeg[c] = cellEnd[c] = 0;
         __syncthreads();
+        const SceneDev& sc = sc_s;
+        const float* pf = sc.buf[args.parity].f;
+        const size_t cap = sc.cap;
         const uint32_t i0 = it.start, icount = it.count;
 
         // Cell ranges inside the work item (keys are sorted by cell).
@@ -948,7 +958,7 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
 template <int S, bool APIC>
 __device__ __forceinline__ void particleUpdate(const StepArgs& args, const SceneDev& sc, uint32_t gs,
                                                const float4* tvs, const float4* tvo, const int* t0, bool fused,
-                                               float* pre) {
+                                               float* pre, const MaterialDev& mat0) {
     constexpr int T = S + 3;
     const float* pf = sc.buf[args.parity].f;
     float* nf = sc.buf[args.parity ^ 1].f;
@@ -1113,7 +1123,7 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
     }
     matmul3(A, Fe, Fn);
     const uint16_t mid = sc.nmat > 1 ? sc.buf[args.parity].mat[old] : (uint16_t)0;
-    const MaterialDev m = sc.mats[mid];
+    const MaterialDev m = sc.nmat > 1 ? sc.mats[mid] : mat0;
     const float hi = 1.0f + m.theta_s, lo = 1.0f - m.theta_c;
     const float V0 = pre[18];
     float mu, la, tau[6];
@@ -1311,22 +1321,49 @@ __device__ __forceinline__ void tileOrigin(const SceneDev& sc, uint32_t block, i
     t0[2] = 4 * (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1])) - 4;
 }
 
+// Bulk copy (cp.async.bulk) of bytes from global to shared memory, completing
+// on bar; both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulkLoad(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smemAddr(bar)) : "memory");
+}
+
 // G2P: persistent CTAs take work items from this combination's list (then the
-// outside items).  While the particles of one item are updated, the tile of
-// v* (and v) of the next item is already on its way into the other of two
-// shared-memory buffers by TMA; one elected thread fetches the next item and
-// issues its copies, every thread waits on the buffer's mbarrier.
+// outside items).  One elected thread produces: it fetches the next item and
+// copies, by TMA, the item's tile of v* (and v), its scene entry and the
+// scene's first material into one of two shared-memory slots, completing on
+// the slot's "full" mbarrier.  Every warp consumes: it waits on "full",
+// updates its particles of the item and arrives on the slot's "empty"
+// mbarrier; the producer refills a slot only when all warps have released it.
+// So warps run up to one item apart instead of meeting at a CTA barrier after
+// every item, and the particle update reads the scene and material from
+// shared memory.
+// Resident G2P CTAs per SM the register budget is fitted to: 2 gives 128
+// registers a thread and no spills (two-ball G2P 0.132 -> 0.117 ms against 3
+// CTAs at 80 registers, which spill ~150 bytes a thread).
+#ifndef MPM_G2P_MIN_CTAS
+#define MPM_G2P_MIN_CTAS 2
+#endif
 template <int S, bool APIC>
-__global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fused) {
+__global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs args, int fused) {
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
     constexpr int TNP = (TN + 7) & ~7;  // buffers 128-byte aligned
     constexpr unsigned kTileBytes = (unsigned)TN * 16u;
+    static_assert(sizeof(SceneDev) % 16 == 0 && sizeof(MaterialDev) % 16 == 0, "bulk copies need 16-byte sizes");
     __shared__ __align__(128) float4 tvs[2][TNP];
     __shared__ __align__(128) float4 tvo[APIC ? 1 : 2][APIC ? 8 : TNP];
     __shared__ float pre[kThreads * kPreStride];  // per-thread prefetch row: Fe, Fp, V0
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ SceneDev scs[2];
+    __shared__ MaterialDev mat0[2];
+    __shared__ BlockItem its[2];
     __shared__ uint32_t item_s[2];
+    __shared__ __align__(8) uint64_t full[2], empty[2];
     const int want = APIC ? MPM_TRANSFER_APIC : MPM_TRANSFER_PIC_FLIP;
     // this combination's own (finer) items of the active blocks, then the
     // outside items of all scenes (the others' are skipped)
@@ -1335,69 +1372,88 @@ __global__ void __launch_bounds__(kThreads, 3) g2pKernel(StepArgs args, int fuse
     const uint32_t nout = args.counters[1];
     const uint32_t total = nact + nout;
     uint32_t* sched = args.sched + 4;
+    const int lane = threadIdx.x & 31;
 
-    // Thread 0: the next item (the last CTA to run out clears the scheduler,
-    // so every launch starts from zero), and its tile copies into buffer b.
-    auto fetch = [&](int b) {
-        const uint32_t w = atomicAdd(&sched[0], 1u);
-        if (w >= total && atomicAdd(&sched[1], 1u) == gridDim.x - 1) {
-            sched[0] = 0u;
-            sched[1] = 0u;
+    // Producer (thread 0): the next item (the last CTA to run out clears the
+    // scheduler, so every launch starts from zero) into slot b -- its scene
+    // entry, the scene's first material and, for an active block, the tile
+    // of v* (and v) -- completing on full[b].  After the first index past the
+    // end it only hands out the end marker.
+    bool ran_out = false;
+    auto produce = [&](int b) {
+        uint32_t w = total;
+        if (!ran_out) {
+            w = atomicAdd(&sched[0], 1u);
+            if (w >= total) {
+                ran_out = true;
+                if (atomicAdd(&sched[1], 1u) == gridDim.x - 1) {
+                    sched[0] = 0u;
+                    sched[1] = 0u;
+                }
+            }
         }
         item_s[b] = w;
-        if (w < nact) {  // an active block of this combination: stage its tile
-            const BlockItem it = items[w];
-            const SceneDev& sc = args.scenes[it.scene];
+        if (w >= total) {
+            mbarArrive(&full[b]);
+            return;
+        }
+        const BlockItem it = w < nact ? items[w] : args.outside[w - nact];
+        its[b] = it;
+        const SceneDev* sg = args.scenes + it.scene;
+        const bool tile = w < nact;
+        fenceProxyAsyncShared();  // the slot's earlier generic reads come first
+        mbarExpectTx(&full[b], (unsigned)(sizeof(SceneDev) + sizeof(MaterialDev)) +
+                                   (tile ? (APIC ? kTileBytes : 2u * kTileBytes) : 0u));
+        bulkLoad(&scs[b], sg, (unsigned)sizeof(SceneDev), &full[b]);
+        bulkLoad(&mat0[b], sg->mats, (unsigned)sizeof(MaterialDev), &full[b]);
+        if (tile) {
             int t0[3];
-            tileOrigin(sc, it.block, t0);
+            tileOrigin(*sg, it.block, t0);
             const unsigned char* maps = args.tmaps + (size_t)it.scene * 2 * kTensorMapBytes;
-            fenceProxyAsyncShared();
-            mbarExpectTx(&bar[b], APIC ? kTileBytes : 2u * kTileBytes);
             tensorMapAcquire(maps);
-            tmaLoadTile(&tvs[b][0], maps, t0[0], t0[1], t0[2], &bar[b]);
+            tmaLoadTile(&tvs[b][0], maps, t0[0], t0[1], t0[2], &full[b]);
             if (!APIC) {
                 tensorMapAcquire(maps + kTensorMapBytes);
-                tmaLoadTile(&tvo[b][0], maps + kTensorMapBytes, t0[0], t0[1], t0[2], &bar[b]);
+                tmaLoadTile(&tvo[b][0], maps + kTensorMapBytes, t0[0], t0[1], t0[2], &full[b]);
             }
         }
     };
     spanBegin(args.spans, SPAN_G2P);
     if (threadIdx.x == 0) {
-        mbarInit(&bar[0], 1);
-        mbarInit(&bar[1], 1);
+        mbarInit(&full[0], 1);
+        mbarInit(&full[1], 1);
+        mbarInit(&empty[0], kWarps);
+        mbarInit(&empty[1], kWarps);
         mbarInitFence();
-        fetch(0);
+        produce(0);
     }
     __syncthreads();
-    unsigned phases = 0u;  // bit b: the parity of buffer b's next wait
-    for (int cur = 0;; cur ^= 1) {
-        const uint32_t w = item_s[cur];
-        if (w >= total) break;
-        // the next item's tile goes into the other buffer, which the previous
-        // item finished reading before the barrier at the end of its loop
-        if (threadIdx.x == 0) fetch(cur ^ 1);
-        const bool inside = w < nact;
-        const BlockItem it = inside ? items[w] : args.outside[w - nact];
-        const SceneDev& sc = args.scenes[it.scene];
-        int t0[3] = {0, 0, 0};
-        if (inside) {
-            tileOrigin(sc, it.block, t0);
-            const bool ok = waitTile(&bar[cur], (phases >> cur) & 1u, args.err);
-            phases ^= 1u << cur;
-            if (__syncthreads_or(!ok)) {
-                // A tile never arrived (flagged; never expected): wait, again
-                // bounded, for the copies of the other buffer, then stop this
-                // CTA.  The host reports MPM_ERR_TIMEOUT.
-                if (item_s[cur ^ 1] < nact) waitTile(&bar[cur ^ 1], (phases >> (cur ^ 1)) & 1u, args.err);
-                return;
+    unsigned full_ph = 0u, empty_ph = 0u;  // bit b: parity of slot b's next wait
+    for (int k = 0, b = 0;; ++k, b ^= 1) {
+        if (threadIdx.x == 0) {
+            // slot b ^ 1 gets item k + 1; it held item k - 1
+            if (k >= 1) {
+                if (!waitTile(&empty[b ^ 1], (empty_ph >> (b ^ 1)) & 1u, args.err)) return;
+                empty_ph ^= 1u << (b ^ 1);
             }
+            produce(b ^ 1);
         }
+        if (!waitTile(&full[b], (full_ph >> b) & 1u, args.err)) return;  // flagged; never expected
+        full_ph ^= 1u << b;
+        const uint32_t w = item_s[b];
+        if (w >= total) break;
+        const bool inside = w < nact;
+        const BlockItem it = its[b];
+        const SceneDev& sc = scs[b];
+        int t0[3] = {0, 0, 0};
+        if (inside) tileOrigin(sc, it.block, t0);
         if (inside || (sc.S == S && sc.transfer == want))
             for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
-                particleUpdate<S, APIC>(args, sc, it.start + i, inside ? &tvs[cur][0] : nullptr,
-                                        APIC ? nullptr : &tvo[cur][0], t0, fused != 0,
-                                        pre + threadIdx.x * kPreStride);
-        __syncthreads();  // buffer cur is free again; item_s[cur ^ 1] is visible
+                particleUpdate<S, APIC>(args, sc, it.start + i, inside ? &tvs[b][0] : nullptr,
+                                        APIC ? nullptr : &tvo[b][0], t0, fused != 0,
+                                        pre + threadIdx.x * kPreStride, mat0[b]);
+        __syncwarp();
+        if (lane == 0) mbarArrive(&empty[b]);
     }
     spanEnd(args.spans, SPAN_G2P);
 }

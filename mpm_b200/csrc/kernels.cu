@@ -955,35 +955,64 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
 // (S+3)^3 node tile of v* (and v) is staged in shared memory, then one thread
 // per particle.  Writes the particle to its sorted slot of the other buffer.
 // ---------------------------------------------------------------------------
+// The first loads of a particle's update, issued one particle ahead: the
+// permutation entry, x and v into registers, and Fe, Fp, V0 into the thread's
+// shared-memory row by cp.async (one commit group per particle, possibly
+// empty), so their latency overlaps the previous particle's update.
+struct G2PIn {
+    uint32_t old;
+    bool ok;
+    float x[3], v[3];
+};
+__device__ __forceinline__ G2PIn g2pFetch(const StepArgs& args, const SceneDev& sc, uint32_t gs, float* pre) {
+    G2PIn p;
+    const float* pf = sc.buf[args.parity].f;
+    const size_t cap = sc.cap;
+    const uint32_t old = args.perm[gs] - sc.key_offset;
+    const uint32_t dst = gs - sc.key_offset;
+    p.ok = old < sc.n && dst < sc.n;  // range check: never expected, skip instead of faulting
+    p.old = p.ok ? old : 0u;
+    if (p.ok) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            cpAsync4(pre + k, pf + (F_FE + k) * cap + old);
+            cpAsync4(pre + 9 + k, pf + (F_FP + k) * cap + old);
+        }
+        cpAsync4(pre + 18, pf + F_VOL * cap + old);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            p.x[a] = ldg(pf + (F_X + a) * cap + old);
+            p.v[a] = ldg(pf + (F_V + a) * cap + old);
+        }
+    } else {
+        atomicOr(args.err, ERR_INDEX);
+    }
+    cpAsyncCommit();
+    return p;
+}
+__device__ __forceinline__ void cpAsyncWaitPrevious() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 template <int S, bool APIC>
-__device__ __forceinline__ void particleUpdate(const StepArgs& args, const SceneDev& sc, uint32_t gs,
-                                               const float4* tvs, const float4* tvo, const int* t0, bool fused,
-                                               float* pre, const MaterialDev& mat0) {
+__device__ __forceinline__ void particleUpdate(const StepArgs& args, const SceneDev& sc, uint32_t gs, const G2PIn& in,
+                                               bool next_pending, const float4* tvs, const float4* tvo, const int* t0,
+                                               bool fused, float* pre, const MaterialDev& mat0) {
     constexpr int T = S + 3;
     const float* pf = sc.buf[args.parity].f;
     float* nf = sc.buf[args.parity ^ 1].f;
     const size_t cap = sc.cap;
-    const uint32_t old = args.perm[gs] - sc.key_offset;
-    const uint32_t dst = gs - sc.key_offset;
-    if (old >= sc.n || dst >= sc.n) {  // range check: never expected, skip instead of faulting
-        atomicOr(args.err, ERR_INDEX);
+    if (!in.ok) {
+        if (next_pending) cpAsyncWaitPrevious();
+        else cpAsyncWaitAll();
         return;
     }
-    // Fe, Fp and V0 are needed only after the gather: start their copies into
-    // this thread's shared-memory row now so the loads overlap the gather.
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        cpAsync4(pre + k, pf + (F_FE + k) * cap + old);
-        cpAsync4(pre + 9 + k, pf + (F_FP + k) * cap + old);
-    }
-    cpAsync4(pre + 18, pf + F_VOL * cap + old);
-    cpAsyncCommit();
+    const uint32_t old = in.old;
+    const uint32_t dst = gs - sc.key_offset;
     const float h = sc.h, dt = sc.dt;
     float x[3], v[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        x[a] = ldg(pf + (F_X + a) * cap + old);
-        v[a] = ldg(pf + (F_V + a) * cap + old);
+        x[a] = in.x[a];
+        v[a] = in.v[a];
     }
     float vpic[3] = {0.f, 0.f, 0.f}, dflip[3] = {0.f, 0.f, 0.f};
     float gv[9], K[9];
@@ -1114,7 +1143,8 @@ __device__ __forceinline__ void particleUpdate(const StepArgs& args, const Scene
     }
     // Fe <- (I + dt grad v) Fe ; F = Fe Fp ; SVD clamp (src/material_point3d.cu:53-70).
     float Fe[9], Fp[9], A[9], Fn[9];
-    cpAsyncWaitAll();
+    if (next_pending) cpAsyncWaitPrevious();  // this particle's group; the next one's may still run
+    else cpAsyncWaitAll();
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
         Fe[k] = pre[k];
@@ -1358,7 +1388,10 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
     static_assert(sizeof(SceneDev) % 16 == 0 && sizeof(MaterialDev) % 16 == 0, "bulk copies need 16-byte sizes");
     __shared__ __align__(128) float4 tvs[2][TNP];
     __shared__ __align__(128) float4 tvo[APIC ? 1 : 2][APIC ? 8 : TNP];
-    __shared__ float pre[kThreads * kPreStride];  // per-thread prefetch row: Fe, Fp, V0
+    // two per-thread prefetch rows of Fe, Fp, V0 (dynamic shared memory: with
+    // the tiles they exceed the 48 KB of static shared memory)
+    extern __shared__ float4 g2p_dyn[];
+    float (*pre)[kThreads * kPreStride] = reinterpret_cast<float (*)[kThreads * kPreStride]>(g2p_dyn);
     __shared__ SceneDev scs[2];
     __shared__ MaterialDev mat0[2];
     __shared__ BlockItem its[2];
@@ -1447,11 +1480,22 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
         const SceneDev& sc = scs[b];
         int t0[3] = {0, 0, 0};
         if (inside) tileOrigin(sc, it.block, t0);
-        if (inside || (sc.S == S && sc.transfer == want))
-            for (uint32_t i = threadIdx.x; i < it.count; i += kThreads)
-                particleUpdate<S, APIC>(args, sc, it.start + i, inside ? &tvs[b][0] : nullptr,
+        if ((inside || (sc.S == S && sc.transfer == want)) && threadIdx.x < it.count) {
+            // each thread's particles of the item, the next one's loads in
+            // flight during the current one's update (rows alternate)
+            int row = 0;
+            G2PIn cur = g2pFetch(args, sc, it.start + threadIdx.x, &pre[0][threadIdx.x * kPreStride]);
+            for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
+                const bool more = i + kThreads < it.count;
+                G2PIn nxt;
+                if (more) nxt = g2pFetch(args, sc, it.start + i + kThreads, &pre[row ^ 1][threadIdx.x * kPreStride]);
+                particleUpdate<S, APIC>(args, sc, it.start + i, cur, more, inside ? &tvs[b][0] : nullptr,
                                         APIC ? nullptr : &tvo[b][0], t0, fused != 0,
-                                        pre + threadIdx.x * kPreStride, mat0[b]);
+                                        &pre[row][threadIdx.x * kPreStride], mat0[b]);
+                if (more) cur = nxt;
+                row ^= 1;
+            }
+        }
         __syncwarp();
         if (lane == 0) mbarArrive(&empty[b]);
     }
@@ -1747,14 +1791,25 @@ void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want
 #undef GRID_CASE
 }
 
+constexpr size_t kG2PDynSmem = sizeof(float) * 2 * kThreads * kPreStride;
+template <int S, bool APIC>
+static void g2pLaunch(const LaunchCtx& c, const StepArgs& a, int fused) {
+    static bool attr = [] {
+        cudaFuncSetAttribute(g2pKernel<S, APIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2PDynSmem);
+        return true;
+    }();
+    (void)attr;
+    g2pKernel<S, APIC><<<c.persistent_blocks, kThreads, kG2PDynSmem, c.stream>>>(a, fused);
+}
+
 void launchG2P(const LaunchCtx& c, const StepArgs& args, int S, bool apic, bool fused, int combo) {
     noteLaunches(1);
     StepArgs a = args;
     a.combo = combo;
-#define G2P_CASE(SS)                                                                                   \
-    if (S == SS) {                                                                                     \
-        if (apic) g2pKernel<SS, true><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, fused ? 1 : 0); \
-        else g2pKernel<SS, false><<<c.persistent_blocks, kThreads, 0, c.stream>>>(a, fused ? 1 : 0);     \
+#define G2P_CASE(SS)                                  \
+    if (S == SS) {                                    \
+        if (apic) g2pLaunch<SS, true>(c, a, fused ? 1 : 0); \
+        else g2pLaunch<SS, false>(c, a, fused ? 1 : 0);     \
     }
     G2P_CASE(2) G2P_CASE(3) G2P_CASE(4)
 #undef G2P_CASE

@@ -203,6 +203,39 @@ struct SceneHost {
 };
 
 // ---------------------------------------------------------------------------
+// Page-locked host words for asynchronous read-backs of single device words
+// (the P2G staging decision).  One page-locked block for the process, handed
+// out word by word: cudaHostAlloc per engine costs milliseconds (it pins
+// pages), which a solver's construction and first step would pay.
+// ---------------------------------------------------------------------------
+struct PinnedWords {
+    std::mutex mu;
+    uint32_t* base = nullptr;
+    std::vector<int> free_slots;
+    static constexpr int kSlots = 4096;
+    uint32_t* take() {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!base) {
+            if (cudaHostAlloc((void**)&base, sizeof(uint32_t) * kSlots, cudaHostAllocPortable) != cudaSuccess) {
+                cudaGetLastError();
+                base = nullptr;
+                return nullptr;
+            }
+            for (int i = kSlots - 1; i >= 0; --i) free_slots.push_back(i);
+        }
+        if (free_slots.empty()) return nullptr;
+        const int i = free_slots.back();
+        free_slots.pop_back();
+        return base + i;
+    }
+    void give(uint32_t* p) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (p && base) free_slots.push_back((int)(p - base));
+    }
+};
+static PinnedWords g_pinned_words;
+
+// ---------------------------------------------------------------------------
 // Tuning cache of the autotuner: launch settings per (device, stencil size,
 // transfer, particles-per-cell bucket), kept for the process and in a text
 // file ("<device> <S> <transfer> <bucket> <g2p_chunk> <p2g_stage>" per line;
@@ -300,7 +333,7 @@ public:
         for (auto& e4 : tune_ev_)
             for (auto e : e4)
                 if (e) cudaEventDestroy(e);
-        if (host_word_) cudaFreeHost(host_word_);
+        if (host_word_) g_pinned_words.give(host_word_);
         if (stage_event_) cudaEventDestroy(stage_event_);
         if (stream_) cudaStreamDestroy(stream_);
     }
@@ -1622,7 +1655,8 @@ public:
         if (!stage_check_) return MPM_OK;
         if (!stage_pending_) {
             if (!host_word_) {
-                CUDA_TRY(cudaHostAlloc((void**)&host_word_, sizeof(uint32_t), cudaHostAllocDefault));
+                host_word_ = g_pinned_words.take();
+                if (!host_word_) return fail(MPM_ERR_OOM, "no page-locked host word for the staging read-back");
                 CUDA_TRY(cudaEventCreateWithFlags(&stage_event_, cudaEventDisableTiming));
             }
             CUDA_TRY(cudaMemcpyAsync(host_word_, counters_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));

@@ -434,11 +434,14 @@ struct P2GLayout {
     static constexpr size_t smemFor(int nw) {
         return ((size_t)nw * kStage * P + (size_t)kSlots * F * NS) * 4 + (size_t)kCtlInts * 4;
     }
-    // Threads per CTA: where two CTAs of 12 warps fit an SM's shared memory
-    // (the cubic stencil, at most ~113 KB each), 24 warps per SM -- the
-    // register file's limit at 80 registers -- come from two CTAs of 12 warps;
-    // otherwise CTAs of 8 warps (three per SM where they fit).
-    static constexpr int NT = (S == 4 && smemFor(12) <= 113 * 1024) ? 384 : 256;
+    // Threads per CTA.  Dense cubic scenes (staging 24 or 32 particles per
+    // pass) get two CTAs of 12 warps per SM where they fit its shared memory
+    // (at most ~113 KB each): 24 warps, the register file's limit at 80
+    // registers, working on two blocks.  Otherwise CTAs of 8 warps, three per
+    // SM where they fit: sparse scenes (staging 16, chosen below 8 particles
+    // per cell) have too few staging windows per block to keep 12 warps busy
+    // (8.4M-particle slab P2G 2.8 ms with 8 warps against 3.4 ms with 12).
+    static constexpr int NT = (S == 4 && STAGE >= 24 && smemFor(12) <= 113 * 1024) ? 384 : 256;
     static constexpr int NW = NT / 32;
     static constexpr int MIN_CTAS = NT == 384 ? 2 : (S == 4 ? 2 : 3);
     static constexpr int TJ = (TN + NT - 1) / NT;

@@ -26,6 +26,9 @@ constexpr int kSortTileKeys = kThreads * 8;  // keys per radix-sort tile (8 per 
 // ceil(count / kBlockChunk) P2G items of nearly equal size (each with its own
 // P2G tile, merged in item order), so that one crowded block cannot serialize
 // a step.  The split fixes the order of P2G's sums, so it is a constant.
+// (Splits of 2048 and 1024 particles were no faster on the dense two-ball
+// scene -- P2G 0.150 and 0.144 ms against 0.145 ms -- and slowed the grid
+// pass, which sums more tiles per node.)
 constexpr uint32_t kBlockChunk = 4096;
 // G2P has no sums across particles, so its work items can be smaller without
 // changing any result: a block is split into ceil(count / chunk) G2P items,

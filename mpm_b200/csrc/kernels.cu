@@ -443,7 +443,10 @@ struct P2GLayout {
     // (8.4M-particle slab P2G 2.8 ms with 8 warps against 3.4 ms with 12).
     static constexpr int NT = (S == 4 && STAGE >= 24 && smemFor(12) <= 113 * 1024) ? 384 : 256;
     static constexpr int NW = NT / 32;
-    static constexpr int MIN_CTAS = NT == 384 ? 2 : (S == 4 ? 2 : 3);
+    // CTAs per SM the launch bound asks for: as many as the shared memory
+    // holds (228 KB per SM, 1 KB of it reserved per CTA), at most 3 (80
+    // registers); the register budget follows from it.
+    static constexpr int MIN_CTAS = NT == 384 ? 2 : ((smemFor(8) + 1024) * 3 <= 228 * 1024 ? 3 : 2);
     static constexpr int TJ = (TN + NT - 1) / NT;
     static constexpr size_t kPartialOff = (size_t)NW * kStage * P;
     static constexpr size_t kCtlOff = kPartialOff + (size_t)kSlots * F * NS;

@@ -1680,10 +1680,9 @@ __global__ void gatherFieldKernel(const SceneDev* __restrict__ scenes, int scene
     const size_t cap = sc.cap;
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
         const uint32_t o = pid[i];
-        if (mode == 1) {  // position4
-#pragma unroll
-            for (int a = 0; a < 3; ++a) out[4 * (size_t)o + a] = f[(F_X + a) * cap + i];
-            out[4 * (size_t)o + 3] = 1.0f;
+        if (mode == 1) {  // position4: one 16-byte store per particle
+            reinterpret_cast<float4*>(out)[o] =
+                make_float4(f[F_X * cap + i], f[(F_X + 1) * cap + i], f[(F_X + 2) * cap + i], 1.0f);
         } else if (mode == 2) {  // det of a 3x3 field
             float M[9];
 #pragma unroll

@@ -1,6 +1,6 @@
 // naive_mpm.cu -- reference-naive GPU restatement of the MPM snow step.
 //
-// A BASELINE, not the product: it keeps the reference's execution model so
+// A yardstick, not the product: it keeps the reference's execution model so
 // that the B200 engine can be measured against it on the same GPU.
 //   * AoS particles (128 B PIC-FLIP point, 236 B APIC point:
 //     include/material_point3d.h:14-24, include/apic_material_point3d.h:14-24)

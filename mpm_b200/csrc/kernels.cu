@@ -1336,14 +1336,18 @@ __device__ __forceinline__ void tmaLoadTile(void* dst, const void* map, int x, i
         : "memory");
 }
 
-// Bounded wait for a tile: gives up after ~2^22 polls (seconds), raising
-// ERR_WAIT_TIMEOUT instead of hanging.  Returns false on a timeout.
-__device__ __forceinline__ bool waitTile(uint64_t* bar, unsigned parity, uint32_t* err) {
+// Bounded wait on an mbarrier phase: gives up after ~2^22 polls (seconds),
+// raising ERR_WAIT_TIMEOUT and setting *abort (when given) so that the CTA's
+// other waiters give up too (they look at it every 256 polls).  Returns false
+// when it gave up.
+__device__ __forceinline__ bool waitTile(uint64_t* bar, unsigned parity, uint32_t* err, volatile int* abort) {
     for (uint32_t i = 0; !mbarTryWait(bar, parity); ++i) {
         if (i > (1u << 22)) {
-            if (threadIdx.x == 0) atomicOr(err, ERR_WAIT_TIMEOUT);
+            atomicOr(err, ERR_WAIT_TIMEOUT);
+            if (abort) *abort = 1;
             return false;
         }
+        if (abort && (i & 255u) == 255u && *abort) return false;
         if (i > 64) __nanosleep(64);
     }
     return true;
@@ -1457,8 +1461,14 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
             }
         }
     };
+    // A wait that gives up (never expected) sets abort_s: the producer stops
+    // issuing copies, every warp leaves the loop at its next slot wait (as a
+    // whole warp), and thread 0 waits for the copies still in flight before
+    // the CTA exits, so that none lands in shared memory it no longer owns.
+    __shared__ int abort_s;
     spanBegin(args.spans, SPAN_G2P);
     if (threadIdx.x == 0) {
+        abort_s = 0;
         mbarInit(&full[0], 1);
         mbarInit(&full[1], 1);
         mbarInit(&empty[0], kWarps);
@@ -1468,16 +1478,23 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
     }
     __syncthreads();
     unsigned full_ph = 0u, empty_ph = 0u;  // bit b: parity of slot b's next wait
+    unsigned issued = 1u;                  // thread 0: slots whose copies it has not yet seen land
     for (int k = 0, b = 0;; ++k, b ^= 1) {
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !abort_s) {
             // slot b ^ 1 gets item k + 1; it held item k - 1
+            bool free_slot = true;
             if (k >= 1) {
-                if (!waitTile(&empty[b ^ 1], (empty_ph >> (b ^ 1)) & 1u, args.err)) return;
-                empty_ph ^= 1u << (b ^ 1);
+                free_slot = waitTile(&empty[b ^ 1], (empty_ph >> (b ^ 1)) & 1u, args.err, &abort_s);
+                if (free_slot) empty_ph ^= 1u << (b ^ 1);
             }
-            produce(b ^ 1);
+            if (free_slot) {
+                produce(b ^ 1);
+                issued |= 1u << (b ^ 1);
+            }
         }
-        if (!waitTile(&full[b], (full_ph >> b) & 1u, args.err)) return;  // flagged; never expected
+        const bool landed = waitTile(&full[b], (full_ph >> b) & 1u, args.err, &abort_s);
+        if (__any_sync(0xffffffffu, !landed)) break;  // gave up (never expected): the whole warp leaves
+        if (threadIdx.x == 0) issued &= ~(1u << b);
         full_ph ^= 1u << b;
         const uint32_t w = item_s[b];
         if (w >= total) break;
@@ -1504,6 +1521,11 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
         }
         __syncwarp();
         if (lane == 0) mbarArrive(&empty[b]);
+    }
+    if (threadIdx.x == 0 && abort_s) {
+        // copies issued and not seen landing: wait for them, bounded again
+        for (int s = 0; s < 2; ++s)
+            if ((issued >> s) & 1u) waitTile(&full[s], (full_ph >> s) & 1u, args.err, nullptr);
     }
     spanEnd(args.spans, SPAN_G2P);
 }

@@ -600,10 +600,10 @@ def run_e2e(work, steps, ws, tuning=None):
     t0 = time.perf_counter()
     g = work.engine(scenes=pinned)
     if tuning and not work.batched:  # the settings the autotuner chose for this scene
-        g.set_tuning(tuning["g2p_chunk"], tuning["p2g_stage"])
+        g.set_tuning(tuning["g2p_chunk"], tuning["p2g_stage"], tuning["p2g_warp_max"])
     elif tuning:
         for c in tuning["combinations"]:
-            g.set_tuning(c["g2p_chunk"], c["p2g_stage"], c["interpolation"], c["transfer"])
+            g.set_tuning(c["g2p_chunk"], c["p2g_stage"], c["interpolation"], c["transfer"], c["p2g_warp_max"])
     for k in range(steps):
         g.step(1)
         if work.batched:

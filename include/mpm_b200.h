@@ -358,14 +358,21 @@ MPM_API mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out);
  * thrust launches run one thread per particle or node).  They decide how the
  * work is spread over the GPU and never the order of any sum, so every result
  * is bitwise the same for any setting.
- *   g2p_chunk: particles per G2P work item, MPM_G2P_CHUNK_MIN..MPM_G2P_CHUNK_MAX
- *              (a grid block's particles are split into items of this size);
- *   p2g_stage: particles staged per P2G warp pass, 16, 24 or 32 (0: chosen
- *              from the particle density after the first step). */
+ *   g2p_chunk:    particles per G2P work item, MPM_G2P_CHUNK_MIN..MPM_G2P_CHUNK_MAX
+ *                 (a grid block's particles are split into items of this size);
+ *   p2g_stage:    particles staged per P2G warp pass, 16, 24 or 32 (0: chosen
+ *                 from the particle density after the first step);
+ *   p2g_warp_max: P2G work items of at most this many particles are taken by
+ *                 single warps instead of whole CTAs, 0..MPM_P2G_WARP_MAX_MAX
+ *                 (0: none; -1: chosen after the first step -- 256 where a
+ *                 (stencil, transfer) combination has at least 1024 items of
+ *                 at most 256 particles, else 0). */
 typedef struct mpm_tuning {
     int32_t g2p_chunk;
     int32_t p2g_stage;
+    int32_t p2g_warp_max;
 } mpm_tuning;
+#define MPM_P2G_WARP_MAX_MAX 4096
 #define MPM_G2P_CHUNK_MIN 256
 #define MPM_G2P_CHUNK_MAX 4096
 
@@ -378,8 +385,10 @@ MPM_API mpm_status mpm_solver_set_tuning(mpm_solver* s, const mpm_tuning* t);
  * cache (this process's, then the per-device cache file) takes the cached
  * settings; otherwise every G2P chunk of {256, 512, 1024, 2048, 4096} and
  * every P2G staging size of {16, 24, 32} is timed with CUDA events around the
- * P2G and G2P launches over `steps_per_candidate` steps (after one untimed
- * step each) and the fastest of each is kept and cached.  The tuning steps
+ * P2G and G2P launches of each combination (one combination after another)
+ * over `steps_per_candidate` steps (after one untimed step each) and the fastest
+ * of each is kept and cached; the P2G warp threshold stays the engine's
+ * choice (-1).  The tuning steps
  * are real steps of the simulation (they advance it; their results are those
  * of any other settings); *steps_run (may be NULL) returns how many were
  * taken.  The cache file is $MPM_TUNE_CACHE, else

@@ -39,10 +39,11 @@ KERNEL_FAMILIES = ["keys", "sort", "compact", "stress", "p2g", "grid", "g2p"]
 # autotuner flags (mpm_solver_autotune)
 TUNE_FORCE, TUNE_NO_DISK = 1, 2
 G2P_CHUNK_MIN, G2P_CHUNK_MAX = 256, 4096
+P2G_WARP_MAX_MAX = 4096
 
 
 class Tuning(C.Structure):
-    _fields_ = [("g2p_chunk", C.c_int32), ("p2g_stage", C.c_int32)]
+    _fields_ = [("g2p_chunk", C.c_int32), ("p2g_stage", C.c_int32), ("p2g_warp_max", C.c_int32)]
 
 
 class Material(C.Structure):

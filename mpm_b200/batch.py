@@ -191,10 +191,11 @@ class Batch:
         t = _abi.Tuning()
         check(self._lib.mpm_batch_get_tuning(self._h, int(interpolation), int(transfer), C.byref(t)),
               "mpm_batch_get_tuning")
-        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage)
+        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage, p2g_warp_max=t.p2g_warp_max)
 
-    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0, interpolation: int = -1, transfer: int = -1):
-        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage))
+    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0, interpolation: int = -1, transfer: int = -1,
+                   p2g_warp_max: int = -1):
+        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage), int(p2g_warp_max))
         check(self._lib.mpm_batch_set_tuning(self._h, int(interpolation), int(transfer), C.byref(t)),
               "mpm_batch_set_tuning")
 

@@ -213,10 +213,11 @@ struct PinnedWords {
     uint32_t* base = nullptr;
     std::vector<int> free_slots;
     static constexpr int kSlots = 4096;
-    uint32_t* take() {
+    static constexpr int kLine = 8;  // words per slot
+    uint32_t* take() {  // kLine contiguous words
         std::lock_guard<std::mutex> lock(mu);
         if (!base) {
-            if (cudaHostAlloc((void**)&base, sizeof(uint32_t) * kSlots, cudaHostAllocPortable) != cudaSuccess) {
+            if (cudaHostAlloc((void**)&base, sizeof(uint32_t) * kSlots * kLine, cudaHostAllocPortable) != cudaSuccess) {
                 cudaGetLastError();
                 base = nullptr;
                 return nullptr;
@@ -226,11 +227,11 @@ struct PinnedWords {
         if (free_slots.empty()) return nullptr;
         const int i = free_slots.back();
         free_slots.pop_back();
-        return base + i;
+        return base + (size_t)i * kLine;
     }
     void give(uint32_t* p) {
         std::lock_guard<std::mutex> lock(mu);
-        if (p && base) free_slots.push_back((int)(p - base));
+        if (p && base) free_slots.push_back((int)((p - base) / kLine));
     }
 };
 static PinnedWords g_pinned_words;
@@ -264,11 +265,15 @@ struct TuneCache {
         if (p.empty()) return;
         FILE* f = fopen(p.c_str(), "r");
         if (!f) return;
-        char dev[256];
-        int S, tr, bucket, chunk, stage;
-        while (fscanf(f, "%255s %d %d %d %d %d", dev, &S, &tr, &bucket, &chunk, &stage) == 6)
-            if (chunk >= (int)kMinG2PChunk && chunk <= (int)kMaxG2PChunk && (stage == 16 || stage == 24 || stage == 32))
-                entries[key(dev, S, tr, bucket)] = mpm_tuning{chunk, stage};
+        // one entry per line; lines of an older format (fewer values) are
+        // skipped, so their keys are tuned again
+        char line[512], dev[256];
+        int S, tr, bucket, chunk, stage, warp;
+        while (fgets(line, sizeof(line), f))
+            if (sscanf(line, "%255s %d %d %d %d %d %d", dev, &S, &tr, &bucket, &chunk, &stage, &warp) == 7 &&
+                chunk >= (int)kMinG2PChunk && chunk <= (int)kMaxG2PChunk && (stage == 16 || stage == 24 || stage == 32) &&
+                warp >= -1 && warp <= MPM_P2G_WARP_MAX_MAX)
+                entries[key(dev, S, tr, bucket)] = mpm_tuning{chunk, stage, warp};
         fclose(f);
     }
     void store(const std::string& k, const mpm_tuning& t, bool disk) {
@@ -280,12 +285,21 @@ struct TuneCache {
         for (size_t i = 1; i < p.size(); ++i)
             if (p[i] == '/') mkdir(p.substr(0, i).c_str(), 0755);
         if (FILE* f = fopen(p.c_str(), "a")) {
-            fprintf(f, "%s %d %d\n", k.c_str(), t.g2p_chunk, t.p2g_stage);
+            fprintf(f, "%s %d %d %d\n", k.c_str(), t.g2p_chunk, t.p2g_stage, t.p2g_warp_max);
             fclose(f);
         }
     }
 };
 static TuneCache g_tune_cache;
+
+// An unsigned setting from the environment, or `dflt` when unset or not a number.
+static uint32_t envU32(const char* name, uint32_t dflt) {
+    const char* v = getenv(name);
+    if (!v || !*v) return dflt;
+    char* end = nullptr;
+    const unsigned long x = strtoul(v, &end, 10);
+    return (end && *end == 0) ? (uint32_t)x : dflt;
+}
 
 class Engine {
 public:
@@ -354,7 +368,7 @@ public:
         DevMem* all[] = {&cell_range_, &block_range_, &solve_pofs_, &solve_prep_, &solve_T_, &solve_iter_,
                          &keys_[0], &keys_[1], &vals_[0], &vals_[1], &sort_scratch_, &inc_scratch_,
                          &compact_scratch_, &block_count_, &sbb_, &active_, &outside_, &counters_, &block_slot_,
-                         &tiles_, &scenes_dev_, &err_, &tmp_, &g2p_items_, &tmaps_, &spans_};
+                         &tiles_, &scenes_dev_, &err_, &tmp_, &g2p_items_, &tmaps_, &spans_, &p2g_lists_};
         for (DevMem* m : all) m->release();
     }
 
@@ -858,14 +872,17 @@ public:
         MPM_TRY(grow(outside_, sizeof(BlockItem) * ((size_t)ns + nk / kBlockChunk + 1), "outside blocks"));
         g2p_cap_ = (uint32_t)(std::min<size_t>(tb, nk) + nk / kMinG2PChunk + 1);
         MPM_TRY(grow(g2p_items_, sizeof(BlockItem) * g2p_cap_ * (size_t)combos().size(), "G2P items"));
+        // P2G's two lists of item slots per combination (warp items, CTA items)
+        MPM_TRY(grow(p2g_lists_, sizeof(uint32_t) * max_active_ * 2 * combos().size(), "P2G item lists"));
         // [0] work items, [1] outside items, [2] active nodes, [8 + 8k .. 13 + 8k] item
-        // schedulers of the k-th stencil/transfer combination
-        MPM_TRY(alloc(counters_, sizeof(uint32_t) * 64, "counters"));
+        // schedulers of the k-th stencil/transfer combination, then the G2P
+        // item counts (kG2PCountWord) and the P2G list counts (kP2GListWord)
+        MPM_TRY(alloc(counters_, sizeof(uint32_t) * kCounterWords, "counters"));
         if (!spans_.p) {
             MPM_TRY(alloc(spans_, sizeof(unsigned long long) * kSpanWords * kMaxCombos, "kernel spans"));
             MPM_TRY(resetSpans());
         }
-        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * 64, stream_));
+        CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t) * kCounterWords, stream_));
         MPM_TRY(grow(block_slot_, sizeof(int32_t) * tb, "block slots"));
         int maxS = 2;
         for (auto& s : scenes_) maxS = std::max(maxS, s->S);
@@ -1044,6 +1061,8 @@ public:
         a.sched = counters_.as<uint32_t>() + 8;
         a.tmaps = tmaps_.as<unsigned char>();
         a.spans = nullptr;  // set per combination by the step
+        a.p2g_lists = nullptr;  // the step's P2G launches take their combination's lists
+        a.p2g_list_cap = (uint32_t)max_active_;
         return a;
     }
 
@@ -1057,6 +1076,8 @@ public:
         bb.g2p_cap = g2p_cap_;
         bb.counters = counters_.as<uint32_t>();
         bb.block_slot = block_slot_.as<int32_t>();
+        bb.p2g_lists = p2g_lists_.as<uint32_t>();
+        bb.p2g_list_cap = (uint32_t)max_active_;
         return bb;
     }
 
@@ -1115,7 +1136,7 @@ public:
             CUDA_TRY(cudaStreamWaitEvent(compact_stream_, compact_fork_, 0));
             LaunchCtx cc = ctx();
             cc.stream = compact_stream_;
-            launchCompactOnesweep(cc, blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, g2pChunks(),
+            launchCompactOnesweep(cc, blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, comboSplit(),
                                   err_.as<uint32_t>());
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaEventRecord(compact_join_, compact_stream_));
@@ -1143,7 +1164,7 @@ public:
             CUDA_TRY(cudaStreamWaitEvent(stream_, compact_join_, 0));
         } else {
             mark(KF_COMPACT, 0);
-            launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, g2pChunks(),
+            launchCompactOnesweep(ctx(), blockBuffers(), total_blocks_, compact_scratch_.as<unsigned long long>(), kBlockChunk, comboSplit(),
                                   err_.as<uint32_t>());
             mark(KF_COMPACT, 1);
             collect(KF_COMPACT);
@@ -1368,6 +1389,8 @@ public:
             // items, tiles or nodes: their P2G -> grid -> G2P chains run
             // concurrently, combination k on side stream k - 1, each with its
             // own work-item schedulers; the step joins them on the main stream.
+            // (The autotuner times the combinations one after another: timed
+            // side by side, its G2P choices for the 64-scene batch were worse.)
             MPM_TRY(ensureSideStreams((int)cs.size() - 1));
             CUDA_TRY(cudaEventRecord(fork_, stream_));
             for (size_t k = 0; k < cs.size(); ++k) {
@@ -1381,7 +1404,10 @@ public:
                 }
                 const int mode = cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP;
                 ck.p2g_stage = p2gStageOf(cs[k]);
+                ak.combo = (int)k;
+                ak.p2g_lists = p2g_lists_.as<uint32_t>();
                 launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
+                if (warpMaxOf(cs[k], k)) launchP2GWarp(ck, ak, cs[k].S, mode);
                 launchGrid(ck, ak, cs[k].S, mode, cs[k].transfer);
                 launchG2P(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
                 if (k > 0) {
@@ -1397,8 +1423,11 @@ public:
                 StepArgs ak = a;
                 ak.spans = spans_.as<unsigned long long>() + (size_t)kSpanWords * k;
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][0], stream_));
-                launchP2G(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP,
-                          cs[k].transfer);
+                const int mode = cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP;
+                ak.combo = (int)k;
+                ak.p2g_lists = p2g_lists_.as<uint32_t>();
+                launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
+                if (warpMaxOf(cs[k], k)) launchP2GWarp(ck, ak, cs[k].S, mode);
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][1], stream_));
             }
             mark(KF_P2G, 1);
@@ -1471,18 +1500,29 @@ public:
     // ---- launch settings and the autotuner ---------------------------------
     mpm_tuning tuningOf(int S, int transfer) const {
         auto it = tuning_.find({S, transfer});
-        return it != tuning_.end() ? it->second : mpm_tuning{(int32_t)kDefaultG2PChunk, 0};
+        return it != tuning_.end() ? it->second : mpm_tuning{(int32_t)kDefaultG2PChunk, 0, -1};
+    }
+    // The warp threshold of combination k (index in combos()): its tuned value,
+    // or the engine's own choice.
+    uint32_t warpMaxOf(const Combo& c, size_t k) const {
+        const int w = tuningOf(c.S, c.transfer).p2g_warp_max;
+        return w >= 0 ? (uint32_t)w : (k < (size_t)kMaxCombos ? warp_auto_[k] : 0u);
     }
     int p2gStageOf(const Combo& c) const {
         const int st = tuningOf(c.S, c.transfer).p2g_stage;
         return st ? st : p2g_stage_;
     }
-    G2PChunks g2pChunks() const {
-        G2PChunks g;
-        for (int k = 0; k < kMaxCombos; ++k) g.v[k] = kDefaultG2PChunk;
+    ComboSplit comboSplit() const {
+        ComboSplit g;
+        for (int k = 0; k < kMaxCombos; ++k) {
+            g.g2p_chunk[k] = kDefaultG2PChunk;
+            g.p2g_warp_max[k] = 0;
+        }
         auto cs = combos();
-        for (size_t k = 0; k < cs.size() && k < (size_t)kMaxCombos; ++k)
-            g.v[k] = (uint32_t)tuningOf(cs[k].S, cs[k].transfer).g2p_chunk;
+        for (size_t k = 0; k < cs.size() && k < (size_t)kMaxCombos; ++k) {
+            g.g2p_chunk[k] = (uint32_t)tuningOf(cs[k].S, cs[k].transfer).g2p_chunk;
+            g.p2g_warp_max[k] = warpMaxOf(cs[k], k);
+        }
         return g;
     }
     static mpm_status validTuning(const mpm_tuning& t) {
@@ -1490,6 +1530,8 @@ public:
             return fail(MPM_ERR_INVALID_ARG, "g2p_chunk must be in [MPM_G2P_CHUNK_MIN, MPM_G2P_CHUNK_MAX]");
         if (t.p2g_stage != 0 && t.p2g_stage != 16 && t.p2g_stage != 24 && t.p2g_stage != 32)
             return fail(MPM_ERR_INVALID_ARG, "p2g_stage must be 0, 16, 24 or 32");
+        if (t.p2g_warp_max < -1 || t.p2g_warp_max > MPM_P2G_WARP_MAX_MAX)
+            return fail(MPM_ERR_INVALID_ARG, "p2g_warp_max must be in [-1, MPM_P2G_WARP_MAX_MAX]");
         return MPM_OK;
     }
     // interpolation / transfer of -1 select every value.
@@ -1552,7 +1594,7 @@ public:
         for (auto& ch : dev)
             if (ch == ' ') ch = '_';
         std::map<std::pair<int, int>, mpm_tuning> saved = tuning_;
-        for (size_t k = 0; k < nc; ++k) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)kMaxG2PChunk, 0};
+        for (size_t k = 0; k < nc; ++k) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)kMaxG2PChunk, 0, -1};
         dropGraphs();
         while (tune_ev_.size() < nc) {
             std::array<cudaEvent_t, 4> e4{};
@@ -1598,17 +1640,20 @@ public:
             }
         }
         if (any) {
+            // round r: G2P chunk r, P2G staging size r mod 3 (the two kernels
+            // do not depend on each other's setting).  The P2G warp threshold
+            // stays the engine's choice (-1): searched per combination over a
+            // few steps it chose worse than the item-count rule (64-scene
+            // batch 1.92-1.96 ms against 1.87).
             const uint32_t chunks[] = {256, 512, 1024, 2048, 4096};
             const int stages[] = {16, 24, 32};
             std::vector<double> best_g2p(nc, 1e30), p2g_sum[3], p2g_cnt(3, 0.0);
             std::vector<uint32_t> best_chunk(nc, kDefaultG2PChunk);
             for (auto& v : p2g_sum) v.assign(nc, 0.0);
-            // round r: G2P chunk r, P2G staging size r mod 3 (the two kernels
-            // do not depend on each other's setting)
             for (int r = 0; r < 5; ++r) {
                 const int st = r % 3;
                 for (size_t k = 0; k < nc; ++k)
-                    if (todo[k]) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)chunks[r], stages[st]};
+                    if (todo[k]) tuning_[{cs[k].S, cs[k].transfer}] = mpm_tuning{(int32_t)chunks[r], stages[st], -1};
                 std::vector<double> pm(nc, 0.0), gm(nc, 0.0);
                 MPM_TRY(tuneRound(steps, &pm, &gm, &run));
                 for (size_t k = 0; k < nc; ++k) {
@@ -1632,7 +1677,7 @@ public:
                         bs = stages[st];
                     }
                 }
-                const mpm_tuning t{(int32_t)best_chunk[k], bs};
+                const mpm_tuning t{(int32_t)best_chunk[k], bs, -1};
                 saved[{cs[k].S, cs[k].transfer}] = t;
                 g_tune_cache.store(keys[k], t, !(flags & MPM_TUNE_NO_DISK));
             }
@@ -1660,6 +1705,9 @@ public:
                 CUDA_TRY(cudaEventCreateWithFlags(&stage_event_, cudaEventDisableTiming));
             }
             CUDA_TRY(cudaMemcpyAsync(host_word_, counters_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+            static_assert(1 + kMaxCombos <= PinnedWords::kLine, "read-back line too short");
+            CUDA_TRY(cudaMemcpyAsync(host_word_ + 1, counters_.as<uint32_t>() + kP2GSmallWord,
+                                     sizeof(uint32_t) * kMaxCombos, cudaMemcpyDeviceToHost, stream_));
             CUDA_TRY(cudaEventRecord(stage_event_, stream_));
             stage_pending_ = true;
             return MPM_OK;
@@ -1669,12 +1717,18 @@ public:
         CUDA_TRY(q);
         stage_pending_ = false;
         stage_check_ = false;
-        const uint32_t items = *host_word_;
+        const uint32_t items = host_word_[0];
         const int stage = (items > 0 && ntot_ / items < 512) ? 16 : 32;
-        if (stage != p2g_stage_) {
-            p2g_stage_ = stage;
-            dropGraphs();
+        bool changed = stage != p2g_stage_;
+        p2g_stage_ = stage;
+        // warps take the small P2G items of a combination that has enough of
+        // them to fill the GPU (one warp per item: few items leave it idle)
+        for (int k = 0; k < kMaxCombos; ++k) {
+            const uint32_t w = host_word_[1 + k] >= kWarpAutoMinItems ? kWarpAutoMax : 0u;
+            changed |= w != warp_auto_[k];
+            warp_auto_[k] = w;
         }
+        if (changed) dropGraphs();
         return MPM_OK;
     }
 
@@ -2244,7 +2298,12 @@ private:
     uint32_t total_blocks_ = 0;
     int key_bits_ = 1;
     DevMem keys_[2], vals_[2], sort_scratch_, inc_scratch_, compact_scratch_, block_count_, sbb_, active_,
-        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_, spans_;
+        outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_, spans_, p2g_lists_;
+    // Per combination, the engine's own warp threshold for P2G (used where
+    // the tuning leaves it to the engine): kWarpAutoMax where the first step
+    // after a change of the scene set found at least kWarpAutoMinItems items
+    // of at most kWarpAutoMax particles, else 0 (see checkP2GStage).
+    uint32_t warp_auto_[kMaxCombos] = {};
     bool profiling_ = false;
     bool step_timing_ = false;
     std::deque<std::pair<cudaEvent_t, cudaEvent_t>> step_events_;

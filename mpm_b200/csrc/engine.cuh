@@ -42,6 +42,16 @@ constexpr uint32_t kDefaultG2PChunk = 1024;
 // [kG2PCountWord + k] G2P items of combination k.
 constexpr int kMaxCombos = 6;
 constexpr int kG2PCountWord = 56;
+// [kP2GListWord + 2k + c]: P2G items of combination k in its list c (0: items
+// of at most the warp threshold's particles, taken by whole warps; 1: the
+// others, taken by whole CTAs); counter words in all: kCounterWords.
+constexpr int kP2GListWord = 64;
+// [kP2GSmallWord + k]: P2G items of combination k of at most kWarpAutoMax
+// particles (read back to decide the warp threshold when it is not set).
+constexpr int kP2GSmallWord = kP2GListWord + 2 * kMaxCombos;
+constexpr uint32_t kWarpAutoMax = 256;
+constexpr uint32_t kWarpAutoMinItems = 1024;
+constexpr int kCounterWords = 128;
 
 enum Field : int {
     F_X = 0,
@@ -174,7 +184,12 @@ struct StepArgs {
     uint32_t* block_count;       // dense per block
     uint32_t* err;               // error flags
     uint32_t* stats;             // [2]: nodes with mass written by the grid pass
-    uint32_t* sched;             // work-item schedulers: [0..1] P2G, [4..5] G2P (zero between launches)
+    uint32_t* sched;             // work-item schedulers: [0..1] P2G, [2..3] P2G by warps, [4..5] G2P
+                                 // (zero between launches)
+    const uint32_t* p2g_lists;   // P2G item slots of combination `combo`'s lists (see kP2GListWord):
+                                 // list c at p2g_lists + (2 combo + c) p2g_list_cap; null: P2G
+                                 // takes every item of the active list
+    uint32_t p2g_list_cap;
     const unsigned char* tmaps;  // kTensorMapBytes x 2 per scene (64-byte aligned): TMA maps of v*, v
     unsigned long long* spans;   // this combination's kernel time spans (see KernelSpan), or null
 };
@@ -194,7 +209,9 @@ __device__ __forceinline__ unsigned long long globalTimerNs() {
 __device__ __forceinline__ void spanBegin(unsigned long long* spans, int family) {
     if (spans && threadIdx.x == 0) atomicMin(&spans[4 * family], globalTimerNs());
 }
-__device__ __forceinline__ void spanEnd(unsigned long long* spans, int family) {
+// `counted`: the launch counts as one more of the family's launches (a
+// second launch of a family in the same step adds its time only).
+__device__ __forceinline__ void spanEnd(unsigned long long* spans, int family, bool counted = true) {
     if (spans && threadIdx.x == 0) {
         unsigned long long* sp = spans + 4 * family;
         __threadfence();
@@ -202,7 +219,7 @@ __device__ __forceinline__ void spanEnd(unsigned long long* spans, int family) {
             const unsigned long long t1 = globalTimerNs();
             const unsigned long long t0 = atomicExch(&sp[0], ~0ull);
             sp[1] += t1 - t0;
-            sp[2] += 1;
+            if (counted) sp[2] += 1;
             sp[3] = 0;
         }
     }

@@ -30,8 +30,10 @@ struct BlockBuffers {
     BlockItem* outside;               // nscenes
     BlockItem* g2p_items;             // G2P work items, g2p_cap per combination
     uint32_t g2p_cap;
-    uint32_t* counters;               // see kG2PCountWord
+    uint32_t* counters;               // see kG2PCountWord, kP2GListWord
     int32_t* block_slot;              // total_blocks
+    uint32_t* p2g_lists;              // P2G item slots, 2 lists of p2g_list_cap per combination
+    uint32_t p2g_list_cap;
 };
 
 // Host-side count of kernel launches issued by the library (kernels.cu).
@@ -60,14 +62,20 @@ cudaError_t radixSortPairsInto(const uint32_t* in_keys, uint32_t* out_keys, uint
 // kernels.cu
 void launchKeys(const LaunchCtx& c, int parity, uint32_t* keys, uint32_t* block_count, uint32_t* err);
 size_t compactScratchWords64(uint32_t total_blocks);
-// Particles per G2P work item of each (stencil, transfer) combination.
-struct G2PChunks {
-    uint32_t v[kMaxCombos];
+// How the compaction splits each (stencil, transfer) combination's work:
+// particles per G2P work item, and the largest P2G item taken by a single
+// warp (0: none).
+struct ComboSplit {
+    uint32_t g2p_chunk[kMaxCombos];
+    uint32_t p2g_warp_max[kMaxCombos];
 };
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
-                           unsigned long long* scratch, uint32_t chunk, const G2PChunks& g2p_chunks, uint32_t* err);
+                           unsigned long long* scratch, uint32_t chunk, const ComboSplit& split, uint32_t* err);
 void launchStress(const LaunchCtx& c, int parity);
 void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
+// P2G of the combination a.combo's warp list (a.p2g_lists set): one warp per
+// item, tiles bitwise those of launchP2G.
+void launchP2GWarp(const LaunchCtx& c, const StepArgs& a, int S, int mode);
 void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer);
 void launchG2P(const LaunchCtx& c, const StepArgs& a, int S, bool apic, bool fused, int combo);
 void launchDenseGravity(const LaunchCtx& c);

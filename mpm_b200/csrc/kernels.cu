@@ -192,8 +192,9 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
     uint32_t* __restrict__ block_count, uint32_t total_blocks, const uint32_t* __restrict__ scene_block_base,
     int nscenes, BlockItem* __restrict__ active, BlockItem* __restrict__ outside, uint32_t* __restrict__ counters,
     int32_t* __restrict__ block_slot, unsigned long long* __restrict__ status, uint32_t* __restrict__ tile_counter,
-    uint32_t ntiles, uint32_t chunk, BlockItem* __restrict__ g2p_items, uint32_t g2p_cap, G2PChunks g2p_chunk,
-    const SceneDev* __restrict__ scenes, uint32_t* __restrict__ err) {
+    uint32_t ntiles, uint32_t chunk, BlockItem* __restrict__ g2p_items, uint32_t g2p_cap, ComboSplit split,
+    uint32_t* __restrict__ p2g_lists, uint32_t p2g_list_cap, const SceneDev* __restrict__ scenes,
+    uint32_t* __restrict__ err) {
     __shared__ uint32_t tile_s;
     __shared__ unsigned long long tot, excl_s;
     if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
         if ((packed[j] >> 32) == 0) continue;
         const uint32_t count = (uint32_t)(packed[j] & 0xffffffffull);
         const int k = scenes[scn[j]].combo;
-        gtot += (count + g2p_chunk.v[k] - 1) / g2p_chunk.v[k];
+        gtot += (count + split.g2p_chunk[k] - 1) / split.g2p_chunk[k];
         if (gcombo < 0) gcombo = k;
         else mixed |= k != gcombo;
     }
@@ -296,6 +297,35 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
         if (lane == 31) base = atomicAdd(&counters[kG2PCountWord + lead], inc);
         gnext = __shfl_sync(0xffffffffu, base, 31) + inc - gtot;
     }
+    // Slots of this thread's P2G items in their combination's lists: list 0
+    // for items of at most the combination's warp threshold (P2G by warps),
+    // list 1 for the others; aggregated per warp like the G2P items.  The
+    // items of at most kWarpAutoMax particles are counted as well.
+    uint32_t pnext[2] = {0u, 0u};
+    if (p2g_lists && warp_fast && has) {
+        uint32_t ptot[3] = {0u, 0u, 0u};
+#pragma unroll
+        for (int j = 0; j < kCompactPer; ++j) {
+            const uint32_t items = (uint32_t)(packed[j] >> 32);
+            if (b0 + j >= total_blocks || !items) continue;
+            const uint32_t size = ((uint32_t)(packed[j] & 0xffffffffull) + items - 1) / items;
+            ptot[size <= split.p2g_warp_max[lead] ? 0 : 1] += items;
+            if (size <= kWarpAutoMax) ptot[2] += items;
+        }
+#pragma unroll
+        for (int cls = 0; cls < 3; ++cls) {
+            uint32_t inc = ptot[cls];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            uint32_t base = 0;
+            if (lane == 31 && inc)
+                base = atomicAdd(&counters[cls < 2 ? kP2GListWord + 2 * lead + cls : kP2GSmallWord + lead], inc);
+            if (cls < 2) pnext[cls] = __shfl_sync(0xffffffffu, base, 31) + inc - ptot[cls];
+        }
+    }
 #pragma unroll
     for (int j = 0; j < kCompactPer; ++j) {
         const uint32_t b = b0 + j;
@@ -314,7 +344,7 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
             // G2P's items of the block, in its combination's list at slots
             // taken from a counter (their order does not matter)
             const int k = scenes[scene].combo;
-            const uint32_t parts = (count + g2p_chunk.v[k] - 1) / g2p_chunk.v[k];
+            const uint32_t parts = (count + split.g2p_chunk[k] - 1) / split.g2p_chunk[k];
             uint32_t g0;
             if (warp_fast) {
                 g0 = gnext;
@@ -323,6 +353,20 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
                 g0 = atomicAdd(&counters[kG2PCountWord + k], parts);
             }
             splitItems(g2p_items + (size_t)k * g2p_cap + g0, b, start, count, parts, (uint32_t)scene);
+            if (p2g_lists) {
+                const uint32_t size = (count + items - 1) / items;
+                const int cls = size <= split.p2g_warp_max[k] ? 0 : 1;
+                uint32_t p0;
+                if (warp_fast) {
+                    p0 = pnext[cls];
+                    pnext[cls] += items;
+                } else {
+                    p0 = atomicAdd(&counters[kP2GListWord + 2 * k + cls], items);
+                    if (size <= kWarpAutoMax) atomicAdd(&counters[kP2GSmallWord + k], items);
+                }
+                uint32_t* lst = p2g_lists + (size_t)(2 * k + cls) * p2g_list_cap + p0;
+                for (uint32_t q = 0; q < items; ++q) lst[q] = slot + q;
+            }
         } else {
             block_slot[b] = -1;
             if (count > 0) {
@@ -455,6 +499,167 @@ struct P2GLayout {
     static_assert(kMaxSeg >= 64 + (int)(kBlockChunk / kSeg) + 1, "segment list too small");
 };
 
+// P2G staging of one particle (sorted position gs) at `my`: mass, momentum
+// terms, stress factors and stencil weights in the layout of P2GStage.  The
+// CTA and warp P2G kernels share it (and p2gAccumulate), so their sums are
+// bitwise the same.
+template <int S, int MODE, int P, int WB>
+__device__ __forceinline__ void p2gStageParticle(const StepArgs& args, const SceneDev& sc, const float* pf, size_t cap,
+                                                 float dt, float h, float inv_h, uint32_t gs, float* my) {
+    uint32_t old = args.perm[gs] - sc.key_offset;
+    const bool bad = old >= sc.n;  // range check: flag and contribute nothing
+    if (bad) {
+        atomicOr(args.err, ERR_INDEX);
+        old = 0;
+    }
+    float x[3] = {ldg(pf + (F_X + 0) * cap + old), ldg(pf + (F_X + 1) * cap + old),
+                  ldg(pf + (F_X + 2) * cap + old)};
+    int base[3];
+    stencilBase(sc, x, base);
+    float delta[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
+        delta[a] = x[a] - gp0;
+        // Node distances.  The linear kernel's weights
+        // have relative error ~ulp(d)/w near |d| = 1, so it
+        // forms each one as the reference does,
+        // (x_p - (o + h i)) / h; the B-splines are smooth
+        // there and use d0 - k (exact subtraction).
+        float dk[S], wk[S], dwk[S];
+        if (S == 2) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
+                dk[k] = __fdiv_rn(__fsub_rn(x[a], gp), h);
+            }
+        } else {
+            dk[0] = __fdiv_rn(delta[a], h);
+#pragma unroll
+            for (int k = 1; k < S; ++k) dk[k] = dk[0] - (float)k;
+        }
+        splineWeights<S>(dk, wk, dwk);
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            if (MODE == MODE_MASS) {
+                my[WB + a * S + k] = wk[k];
+            } else {
+                my[WB + 2 * (a * S + k)] = wk[k];
+                my[WB + 2 * (a * S + k) + 1] = dwk[k] * inv_h;
+            }
+        }
+    }
+    const float m = bad ? 0.f : ldg(pf + F_MASS * cap + old);
+    my[0] = m;
+    if (MODE != MODE_MASS) {
+        float v[3] = {ldg(pf + (F_V + 0) * cap + old), ldg(pf + (F_V + 1) * cap + old),
+                      ldg(pf + (F_V + 2) * cap + old)};
+        const float ts = bad ? 0.f : ((MODE == MODE_APIC_FUSED) ? -dt : -1.0f);
+        float T[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) T[k] = ts * ldg(pf + (F_TAU + k) * cap + old);
+        if (MODE == MODE_FLIP) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) my[1 + a] = m * v[a];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) my[4 + k] = T[k];
+        } else {
+            float mC[9];
+            if (sc.transfer == MPM_TRANSFER_APIC) {
+                const float md = m * sc.dinv;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) mC[k] = md * ldg(pf + (F_B + k) * cap + old);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) mC[k] = 0.f;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                my[1 + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
+                                        mC[3 * a + 2] * delta[2]);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) my[4 + k] = h * mC[k];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) my[13 + k] = T[k];
+        }
+    }
+}
+
+// One lane's sums over the staged particles q0, q0 + G, ... below qhi (its
+// group's share of a segment, in order) for the stencil column (na, nb).
+template <int S, int MODE, int P, int WB, int G>
+__device__ __forceinline__ void p2gAccumulate(const float* st, int q0, int qhi, int na, int nb, NodeAcc* acc) {
+    const float fa = (float)na, fb = (float)nb;
+    for (int q = q0; q < qhi; q += G) {
+        const float* pq = st + q * P;
+        const float4 s0 = *reinterpret_cast<const float4*>(pq);
+        const float m = s0.x;
+        if (MODE == MODE_MASS) {
+            const float mw = m * (pq[WB + na] * pq[WB + S + nb]);
+#pragma unroll
+            for (int c = 0; c < S; ++c) acc[c].mz.x = fmaf(mw, pq[WB + 2 * S + c], acc[c].mz.x);
+            continue;
+        }
+        // column factors: w = wab Z_c and
+        // T grad w = Z_c A + Z'_c Bz with A = T (X'Y, XY', 0), Bz = T (0, 0, XY)
+        const float2 xa = *reinterpret_cast<const float2*>(pq + WB + 2 * na);
+        const float2 yb = *reinterpret_cast<const float2*>(pq + WB + 2 * (S + nb));
+        const float wab = xa.x * yb.x, dab = xa.y * yb.x, adb = xa.x * yb.y;
+        float T[6];
+        float2 uxy, mu;  // (u_x, u_y) and (m, u_z)
+        float2 hxy = make_float2(0.f, 0.f);
+        float hz = 0.f;
+        if (MODE == MODE_FLIP) {
+            const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
+            const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
+            T[0] = s1.x; T[1] = s1.y; T[2] = s1.z; T[3] = s1.w; T[4] = s2.x; T[5] = s2.y;
+            uxy = make_float2(s0.y, s0.z);
+            mu = make_float2(m, s0.w);
+        } else {
+            const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
+            const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
+            const float4 s3 = *reinterpret_cast<const float4*>(pq + 12);
+            const float4 s4 = *reinterpret_cast<const float4*>(pq + 16);
+            const float hC[9] = {s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, s2.w, s3.x};
+            T[0] = s3.y; T[1] = s3.z; T[2] = s3.w; T[3] = s4.x; T[4] = s4.y; T[5] = s4.z;
+            const float qv[3] = {s0.y, s0.z, s0.w};
+            float u[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, qv[i]));
+            uxy = make_float2(u[0], u[1]);
+            mu = make_float2(m, u[2]);
+            hxy = make_float2(hC[2], hC[5]);
+            hz = hC[8];
+        }
+        const float2 Axy = make_float2(fmaf(T[0], dab, T[3] * adb), fmaf(T[3], dab, T[1] * adb));
+        const float Az = fmaf(T[4], dab, T[5] * adb);
+        const float2 Bxy = make_float2(T[4] * wab, T[5] * wab);
+        const float Bz = T[2] * wab;
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+            const float2 zc = *reinterpret_cast<const float2*>(pq + WB + 2 * (2 * S + c));
+            const float wgt = wab * zc.x;
+            const float2 w2 = make_float2(wgt, wgt), zx2 = make_float2(zc.x, zc.x),
+                         zy2 = make_float2(zc.y, zc.y);
+            if (c > 0 && MODE != MODE_FLIP) {  // u at node c: u += h C e_z, component-wise
+                uxy = __fadd2_rn(uxy, hxy);
+                mu.y += hz;
+            }
+            // m += m w and p_z += w u_z in one pair
+            acc[c].mz = __ffma2_rn(mu, w2, acc[c].mz);
+            if (MODE == MODE_APIC_FUSED) {
+                // p += w u + Z_c A + Z'_c Bz (the order of the nested fmaf)
+                acc[c].pxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, __ffma2_rn(w2, uxy, acc[c].pxy)));
+                acc[c].mz.y = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].mz.y));
+            } else {  // PIC-FLIP and SPLIT keep p and f apart
+                acc[c].pxy = __ffma2_rn(w2, uxy, acc[c].pxy);
+                acc[c].fxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, acc[c].fxy));
+                acc[c].fz = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].fz));
+            }
+        }
+    }
+}
+
 template <int S, int MODE, int STAGE>
 __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MODE, STAGE>::MIN_CTAS)
     p2gKernel(StepArgs args, int want_transfer) {
@@ -477,13 +682,16 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
     // grp, grp + G, grp + 2G, ... of each staged batch.
     const int grp = lane / L::PAIRS, na = (lane % L::PAIRS) % S, nb = (lane % L::PAIRS) / S;
     const bool lane_on = grp < L::G;
-    const uint32_t nact = args.counters[0];
+    // the combination's list of items for whole CTAs, or every active item
+    const uint32_t* list = args.p2g_lists ? args.p2g_lists + (size_t)(2 * args.combo + 1) * args.p2g_list_cap : nullptr;
+    const uint32_t nwork = list ? args.counters[kP2GListWord + 2 * args.combo + 1] : args.counters[0];
     spanBegin(args.spans, SPAN_P2G);
     __shared__ uint32_t item_s;
     __shared__ SceneDev sc_s;
     for (;;) {
-        const uint32_t w = nextWorkItem(args.sched, nact, &item_s);
-        if (w >= nact) break;
+        const uint32_t wi = nextWorkItem(args.sched, nwork, &item_s);
+        if (wi >= nwork) break;
+        const uint32_t w = list ? list[wi] : wi;  // the item's slot: its tile
         const BlockItem it = args.active[w];
         {
             const SceneDev& scg = args.scenes[it.scene];
@@ -579,85 +787,8 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
                 for (int g0 = cb; g0 < ce; g0 += L::kStage) {
                     const int np = min(L::kStage, ce - g0);
                     if (lane < np) {
-                        float* my = st + lane * L::P;
-                        const uint32_t gs = i0 + (uint32_t)(g0 + lane);
-                        uint32_t old = args.perm[gs] - sc.key_offset;
-                        const bool bad = old >= sc.n;  // range check: flag and contribute nothing
-                        if (bad) {
-                            atomicOr(args.err, ERR_INDEX);
-                            old = 0;
-                        }
-                        float x[3] = {ldg(pf + (F_X + 0) * cap + old), ldg(pf + (F_X + 1) * cap + old),
-                                      ldg(pf + (F_X + 2) * cap + old)};
-                        int base[3];
-                        stencilBase(sc, x, base);
-                        float delta[3];
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            const float gp0 = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)base[a]));
-                            delta[a] = x[a] - gp0;
-                            // Node distances.  The linear kernel's weights
-                            // have relative error ~ulp(d)/w near |d| = 1, so it
-                            // forms each one as the reference does,
-                            // (x_p - (o + h i)) / h; the B-splines are smooth
-                            // there and use d0 - k (exact subtraction).
-                            float dk[S], wk[S], dwk[S];
-                            if (S == 2) {
-#pragma unroll
-                                for (int k = 0; k < S; ++k) {
-                                    const float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
-                                    dk[k] = __fdiv_rn(__fsub_rn(x[a], gp), h);
-                                }
-                            } else {
-                                dk[0] = __fdiv_rn(delta[a], h);
-#pragma unroll
-                                for (int k = 1; k < S; ++k) dk[k] = dk[0] - (float)k;
-                            }
-                            splineWeights<S>(dk, wk, dwk);
-#pragma unroll
-                            for (int k = 0; k < S; ++k) {
-                                if (MODE == MODE_MASS) {
-                                    my[L::WB + a * S + k] = wk[k];
-                                } else {
-                                    my[L::WB + 2 * (a * S + k)] = wk[k];
-                                    my[L::WB + 2 * (a * S + k) + 1] = dwk[k] * inv_h;
-                                }
-                            }
-                        }
-                        const float m = bad ? 0.f : ldg(pf + F_MASS * cap + old);
-                        my[0] = m;
-                        if (MODE != MODE_MASS) {
-                            float v[3] = {ldg(pf + (F_V + 0) * cap + old), ldg(pf + (F_V + 1) * cap + old),
-                                          ldg(pf + (F_V + 2) * cap + old)};
-                            const float ts = bad ? 0.f : ((MODE == MODE_APIC_FUSED) ? -dt : -1.0f);
-                            float T[6];
-#pragma unroll
-                            for (int k = 0; k < 6; ++k) T[k] = ts * ldg(pf + (F_TAU + k) * cap + old);
-                            if (MODE == MODE_FLIP) {
-#pragma unroll
-                                for (int a = 0; a < 3; ++a) my[1 + a] = m * v[a];
-#pragma unroll
-                                for (int k = 0; k < 6; ++k) my[4 + k] = T[k];
-                            } else {
-                                float mC[9];
-                                if (sc.transfer == MPM_TRANSFER_APIC) {
-                                    const float md = m * sc.dinv;
-#pragma unroll
-                                    for (int k = 0; k < 9; ++k) mC[k] = md * ldg(pf + (F_B + k) * cap + old);
-                                } else {
-#pragma unroll
-                                    for (int k = 0; k < 9; ++k) mC[k] = 0.f;
-                                }
-#pragma unroll
-                                for (int a = 0; a < 3; ++a)
-                                    my[1 + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
-                                                            mC[3 * a + 2] * delta[2]);
-#pragma unroll
-                                for (int k = 0; k < 9; ++k) my[4 + k] = h * mC[k];
-#pragma unroll
-                                for (int k = 0; k < 6; ++k) my[13 + k] = T[k];
-                            }
-                        }
+                        p2gStageParticle<S, MODE, L::P, L::WB>(args, sc, pf, cap, dt, h, inv_h,
+                                                               i0 + (uint32_t)(g0 + lane), st + lane * L::P);
                     }
                     __syncwarp();
                     // the segments overlapping this pass, in order
@@ -667,77 +798,9 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
                     // group grp sums the segment's particles j = grp (mod G), in
                     // order, however the segment is cut into staging passes
                     const int jlo = g0 + qlo - segBeg[cur];
-                    if (lane_on) {
-                        const float fa = (float)na, fb = (float)nb;
-                        for (int q = qlo + (grp - jlo % L::G + L::G) % L::G; q < qhi; q += L::G) {
-                            const float* pq = st + q * L::P;
-                            const float4 s0 = *reinterpret_cast<const float4*>(pq);
-                            const float m = s0.x;
-                            if (MODE == MODE_MASS) {
-                                const float mw = m * (pq[L::WB + na] * pq[L::WB + S + nb]);
-#pragma unroll
-                                for (int c = 0; c < S; ++c) acc[c].mz.x = fmaf(mw, pq[L::WB + 2 * S + c], acc[c].mz.x);
-                                continue;
-                            }
-                            // column factors: w = wab Z_c and
-                            // T grad w = Z_c A + Z'_c Bz with A = T (X'Y, XY', 0), Bz = T (0, 0, XY)
-                            const float2 xa = *reinterpret_cast<const float2*>(pq + L::WB + 2 * na);
-                            const float2 yb = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (S + nb));
-                            const float wab = xa.x * yb.x, dab = xa.y * yb.x, adb = xa.x * yb.y;
-                            float T[6];
-                            float2 uxy, mu;  // (u_x, u_y) and (m, u_z)
-                            float2 hxy = make_float2(0.f, 0.f);
-                            float hz = 0.f;
-                            if (MODE == MODE_FLIP) {
-                                const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
-                                const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
-                                T[0] = s1.x; T[1] = s1.y; T[2] = s1.z; T[3] = s1.w; T[4] = s2.x; T[5] = s2.y;
-                                uxy = make_float2(s0.y, s0.z);
-                                mu = make_float2(m, s0.w);
-                            } else {
-                                const float4 s1 = *reinterpret_cast<const float4*>(pq + 4);
-                                const float4 s2 = *reinterpret_cast<const float4*>(pq + 8);
-                                const float4 s3 = *reinterpret_cast<const float4*>(pq + 12);
-                                const float4 s4 = *reinterpret_cast<const float4*>(pq + 16);
-                                const float hC[9] = {s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, s2.w, s3.x};
-                                T[0] = s3.y; T[1] = s3.z; T[2] = s3.w; T[3] = s4.x; T[4] = s4.y; T[5] = s4.z;
-                                const float qv[3] = {s0.y, s0.z, s0.w};
-                                float u[3];
-#pragma unroll
-                                for (int i = 0; i < 3; ++i) u[i] = fmaf(hC[3 * i], fa, fmaf(hC[3 * i + 1], fb, qv[i]));
-                                uxy = make_float2(u[0], u[1]);
-                                mu = make_float2(m, u[2]);
-                                hxy = make_float2(hC[2], hC[5]);
-                                hz = hC[8];
-                            }
-                            const float2 Axy = make_float2(fmaf(T[0], dab, T[3] * adb), fmaf(T[3], dab, T[1] * adb));
-                            const float Az = fmaf(T[4], dab, T[5] * adb);
-                            const float2 Bxy = make_float2(T[4] * wab, T[5] * wab);
-                            const float Bz = T[2] * wab;
-#pragma unroll
-                            for (int c = 0; c < S; ++c) {
-                                const float2 zc = *reinterpret_cast<const float2*>(pq + L::WB + 2 * (2 * S + c));
-                                const float wgt = wab * zc.x;
-                                const float2 w2 = make_float2(wgt, wgt), zx2 = make_float2(zc.x, zc.x),
-                                             zy2 = make_float2(zc.y, zc.y);
-                                if (c > 0 && MODE != MODE_FLIP) {  // u at node c: u += h C e_z, component-wise
-                                    uxy = __fadd2_rn(uxy, hxy);
-                                    mu.y += hz;
-                                }
-                                // m += m w and p_z += w u_z in one pair
-                                acc[c].mz = __ffma2_rn(mu, w2, acc[c].mz);
-                                if (MODE == MODE_APIC_FUSED) {
-                                    // p += w u + Z_c A + Z'_c Bz (the order of the nested fmaf)
-                                    acc[c].pxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, __ffma2_rn(w2, uxy, acc[c].pxy)));
-                                    acc[c].mz.y = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].mz.y));
-                                } else {  // PIC-FLIP and SPLIT keep p and f apart
-                                    acc[c].pxy = __ffma2_rn(w2, uxy, acc[c].pxy);
-                                    acc[c].fxy = __ffma2_rn(zy2, Bxy, __ffma2_rn(zx2, Axy, acc[c].fxy));
-                                    acc[c].fz = fmaf(zc.y, Bz, fmaf(zc.x, Az, acc[c].fz));
-                                }
-                            }
-                        }
-                    }
+                    if (lane_on)
+                        p2gAccumulate<S, MODE, L::P, L::WB, L::G>(st, qlo + (grp - jlo % L::G + L::G) % L::G, qhi, na,
+                                                                  nb, acc);
                     if (se > g0 + np) break;  // the segment continues in the next pass
                     // Segment done: sum the groups' columns in group order into
                     // group 0 (fixed order, so the partial does not depend on
@@ -795,6 +858,160 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
     spanEnd(args.spans, SPAN_P2G);
 }
 
+
+// ---------------------------------------------------------------------------
+// P2G by whole warps for the small items (the combination's warp list).  Each
+// warp takes an item and sums its particles segment by segment as p2gKernel
+// does -- cells in order, each cut into segments of at most kSeg particles; a
+// segment's particles summed per group in order, the groups then in lane
+// order (p2gStageParticle, p2gAccumulate) -- and adds each segment's sums
+// into its own shared-memory tile in segment order, the order of p2gKernel's
+// merge: the tile is bitwise p2gKernel's, so which kernel takes an item
+// changes no result.  No CTA barrier: an item of a few particles per cell
+// spends most of p2gKernel's time in its per-item set-up, barriers and merge
+// rounds.
+// ---------------------------------------------------------------------------
+template <int S, int MODE>
+struct P2GWarpLayout {
+    using D = P2GLayout<S, MODE, 16>;  // staging layout, column map and segment length
+    static constexpr int F = D::F, TN = D::TN, P = D::P, WB = D::WB, G = D::G, PAIRS = D::PAIRS;
+    static constexpr int kSeg = D::kSeg;
+    static constexpr int kStage = 16;  // particles staged per pass
+    static constexpr int NT = 256, NW = NT / 32;
+    // per warp: its item's scene entry, its tile [F][TN], its staging rows
+    static constexpr int kSceneFloats = (int)((sizeof(SceneDev) + 15) / 16 * 4);
+    static constexpr int kTileFloats = (F * TN + 3) / 4 * 4;
+    static constexpr int kWarpFloats = kSceneFloats + kTileFloats + kStage * P;
+    static constexpr size_t smemBytes = (size_t)NW * kWarpFloats * 4;
+    static constexpr int MIN_CTAS = (smemBytes + 1024) * 3 <= 228 * 1024 ? 3 : 2;
+};
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(P2GWarpLayout<S, MODE>::NT, P2GWarpLayout<S, MODE>::MIN_CTAS)
+    p2gWarpKernel(StepArgs args) {
+    using W = P2GWarpLayout<S, MODE>;
+    constexpr int F = W::F, T = S + 3, TN = W::TN, G = W::G, PAIRS = W::PAIRS;
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* wbase = reinterpret_cast<float*>(smem4) + (size_t)warp * W::kWarpFloats;
+    SceneDev& sc = *reinterpret_cast<SceneDev*>(wbase);
+    float* tile = wbase + W::kSceneFloats;
+    float* st = tile + W::kTileFloats;
+    const int grp = lane / PAIRS, na = (lane % PAIRS) % S, nb = (lane % PAIRS) / S;
+    const bool lane_on = grp < G;
+    const uint32_t* list = args.p2g_lists + (size_t)(2 * args.combo) * args.p2g_list_cap;
+    const uint32_t nwork = args.counters[kP2GListWord + 2 * args.combo];
+    // the warps' item scheduler: [0] hands out list indices, [1] counts the
+    // warps that have run out; the last of them clears both
+    uint32_t* sched = args.sched + 2;
+    const uint32_t warps = gridDim.x * (uint32_t)W::NW;
+    if (nwork == 0) return;  // nothing for warps (the scheduler is untouched)
+    NodeAcc acc[S];
+    // a segment done: the groups' columns summed in group order (as
+    // p2gKernel), added by group 0 into the tile nodes of the segment's cell
+    auto finish = [&](int cell) {
+        const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+#pragma unroll
+            for (int f = 0; f < F; ++f) {
+                const float mine = acc[c].get(f);
+                float sum = mine;
+#pragma unroll
+                for (int g = 1; g < G; ++g) sum += __shfl_sync(0xffffffffu, mine, min(lane + g * PAIRS, 31));
+                if (grp == 0) tile[f * TN + (na + cx) + T * ((nb + cy) + T * (c + cz))] += sum;
+            }
+            acc[c].zero();
+        }
+        __syncwarp();  // the next segment's sums may land on the same nodes from other lanes
+    };
+    spanBegin(args.spans, SPAN_P2G);
+    for (;;) {
+        uint32_t wi = 0;
+        if (lane == 0) {
+            wi = atomicAdd(&sched[0], 1u);
+            if (wi >= nwork && atomicAdd(&sched[1], 1u) == warps - 1) {
+                sched[0] = 0u;
+                sched[1] = 0u;
+            }
+        }
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        if (wi >= nwork) break;
+        const uint32_t w = list[wi];  // the item's slot: its tile
+        const BlockItem it = args.active[w];
+        if (args.scenes[it.scene].S != S) {  // never expected: lists are per combination
+            if (lane == 0) atomicOr(args.err, ERR_INDEX);
+            continue;
+        }
+        {
+            const int4* src = reinterpret_cast<const int4*>(args.scenes + it.scene);
+            int4* dst = reinterpret_cast<int4*>(&sc);
+            for (int q = lane; q < (int)(sizeof(SceneDev) / 16); q += 32) dst[q] = src[q];
+            for (int q = lane; q < F * TN; q += 32) tile[q] = 0.f;
+        }
+        __syncwarp();
+        const float* pf = sc.buf[args.parity].f;
+        const size_t cap = sc.cap;
+        const float dt = sc.dt, h = sc.h, inv_h = sc.inv_h;
+        const uint32_t i0 = it.start;
+        const int count = (int)it.count;
+#pragma unroll
+        for (int c = 0; c < S; ++c) acc[c].zero();
+        int seg_start = 0;     // item index of the open segment's first particle
+        int seg_cell = 0;      // its cell
+        int cell_start = 0;    // item index of the current cell's first particle
+        uint32_t last_cell = 0;  // cell of the previous pass's last particle
+        for (int g0 = 0; g0 < count; g0 += W::kStage) {
+            const int np = min(W::kStage, count - g0);
+            uint32_t cl = 0;
+            if (lane < np) {
+                p2gStageParticle<S, MODE, W::P, W::WB>(args, sc, pf, cap, dt, h, inv_h, i0 + (uint32_t)(g0 + lane),
+                                                       st + lane * W::P);
+                cl = args.sorted_keys[i0 + (uint32_t)(g0 + lane)] & 63u;
+            }
+            // segment starts of this pass: a particle that opens a cell, or
+            // one kSeg particles after its cell's first
+            uint32_t up = __shfl_up_sync(0xffffffffu, cl, 1);
+            if (lane == 0) up = last_cell;
+            const unsigned cells = __ballot_sync(0xffffffffu, lane < np && (g0 + lane == 0 || cl != up));
+            const unsigned upto = cells & (0xffffffffu >> (31 - lane));  // this lane's and the earlier lanes'
+            const int my_cell_start = upto ? g0 + 31 - __clz(upto) : cell_start;
+            const unsigned segs = __ballot_sync(0xffffffffu, lane < np && (g0 + lane - my_cell_start) % W::kSeg == 0);
+            if (cells) cell_start = g0 + 31 - __clz(cells);
+            last_cell = __shfl_sync(0xffffffffu, cl, np - 1);
+            const uint32_t cl0 = __shfl_sync(0xffffffffu, cl, 0);
+            __syncwarp();  // the staged rows are visible to the warp
+            if (g0 == 0) {
+                seg_cell = (int)cl0;
+            } else if (segs & 1u) {  // the open segment ended with the previous pass
+                finish(seg_cell);
+                seg_start = g0;
+                seg_cell = (int)cl0;
+            }
+            int qa = 0;
+            for (;;) {
+                const unsigned rest = segs & ~((2u << qa) - 1u);  // starts after qa
+                const int qb = rest ? __ffs(rest) - 1 : np;
+                // group grp sums the segment's particles j = grp (mod G), in
+                // order, however the segment is cut into passes
+                const int jlo = g0 + qa - seg_start;
+                if (lane_on) p2gAccumulate<S, MODE, W::P, W::WB, G>(st, qa + (grp - jlo % G + G) % G, qb, na, nb, acc);
+                if (qb >= np) break;  // the open segment continues past this pass
+                const uint32_t cq = __shfl_sync(0xffffffffu, cl, qb);
+                finish(seg_cell);
+                seg_start = g0 + qb;
+                seg_cell = (int)cq;
+                qa = qb;
+            }
+            __syncwarp();  // the staged rows are read before the next pass overwrites them
+        }
+        finish(seg_cell);
+        float* out = args.tiles + (size_t)w * args.tile_stride;
+        for (int q = lane; q < F * TN; q += 32) out[q] = tile[q];
+        __syncwarp();  // the tile is read before the next item clears it
+    }
+    spanEnd(args.spans, SPAN_P2G, false);
+}
 
 // ---------------------------------------------------------------------------
 // Grid pass: merge the <= 8 overlapping tiles of every node in fixed order,
@@ -1742,16 +1959,17 @@ size_t compactScratchWords64(uint32_t total_blocks) {
 }
 
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
-                           unsigned long long* scratch, uint32_t chunk, const G2PChunks& g2p_chunk, uint32_t* err) {
+                           unsigned long long* scratch, uint32_t chunk, const ComboSplit& split, uint32_t* err) {
     const uint32_t ntiles = (uint32_t)((total_blocks + kCompactTile - 1) / kCompactTile);
     cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * compactScratchWords64(total_blocks), c.stream);
     cudaMemsetAsync(bb.counters, 0, sizeof(uint32_t) * 4, c.stream);
     cudaMemsetAsync(bb.counters + kG2PCountWord, 0, sizeof(uint32_t) * kMaxCombos, c.stream);
+    cudaMemsetAsync(bb.counters + kP2GListWord, 0, sizeof(uint32_t) * 3 * kMaxCombos, c.stream);  // lists, small
     noteLaunches(1);
     compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
         bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,
         bb.block_slot, scratch + 1, reinterpret_cast<uint32_t*>(scratch), ntiles, chunk, bb.g2p_items, bb.g2p_cap,
-        g2p_chunk, c.scenes, err);
+        split, bb.p2g_lists, bb.p2g_list_cap, c.scenes, err);
 }
 
 void launchStress(const LaunchCtx& c, int parity) {
@@ -1786,6 +2004,26 @@ static void p2gOne(const LaunchCtx& c, const StepArgs& a, int want) {
         case 24: p2gLaunch<S, MODE, 24>(c, a, want); break;
         default: p2gLaunch<S, MODE, 32>(c, a, want); break;
     }
+}
+
+template <int S, int MODE>
+static void p2gWarpLaunch(const LaunchCtx& c, const StepArgs& a) {
+    using W = P2GWarpLayout<S, MODE>;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(p2gWarpKernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W::smemBytes);
+        attr = true;
+    }
+    const unsigned grid = std::min<unsigned>(c.persistent_blocks, (unsigned)std::max(1, c.num_sms) * W::MIN_CTAS);
+    p2gWarpKernel<S, MODE><<<grid, W::NT, W::smemBytes, c.stream>>>(a);
+}
+
+void launchP2GWarp(const LaunchCtx& c, const StepArgs& a, int S, int mode) {
+    noteLaunches(1);
+    const bool apic = mode == MODE_APIC_FUSED;
+    if (S == 4) apic ? p2gWarpLaunch<4, MODE_APIC_FUSED>(c, a) : p2gWarpLaunch<4, MODE_FLIP>(c, a);
+    else if (S == 3) apic ? p2gWarpLaunch<3, MODE_APIC_FUSED>(c, a) : p2gWarpLaunch<3, MODE_FLIP>(c, a);
+    else apic ? p2gWarpLaunch<2, MODE_APIC_FUSED>(c, a) : p2gWarpLaunch<2, MODE_FLIP>(c, a);
 }
 
 void launchP2G(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want_transfer) {

@@ -297,15 +297,17 @@ class _SolverBase:
 
     # ---- launch settings (no counterpart in the reference) -----------------
     def tuning(self) -> dict:
-        """Launch settings of the step kernels: particles per G2P work item and
-        particles staged per P2G pass (0 = chosen from density)."""
+        """Launch settings of the step kernels: particles per G2P work item,
+        particles staged per P2G pass (0 = chosen from density) and the
+        largest P2G work item taken by a single warp (0 = none, -1 = chosen
+        from the item counts)."""
         t = _abi.Tuning()
         check(self._lib.mpm_solver_get_tuning(self._h, C.byref(t)), "get_tuning")
-        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage)
+        return dict(g2p_chunk=t.g2p_chunk, p2g_stage=t.p2g_stage, p2g_warp_max=t.p2g_warp_max)
 
-    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0):
+    def set_tuning(self, g2p_chunk: int = 1024, p2g_stage: int = 0, p2g_warp_max: int = -1):
         """Set the launch settings; results are bitwise the same for any."""
-        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage))
+        t = _abi.Tuning(int(g2p_chunk), int(p2g_stage), int(p2g_warp_max))
         check(self._lib.mpm_solver_set_tuning(self._h, C.byref(t)), "set_tuning")
 
     def autotune(self, steps_per_candidate: int = 3, force: bool = False, use_disk: bool = True) -> dict:

@@ -428,23 +428,65 @@ def test_download_async_matches_sync(gpu):
 
 @pytest.mark.parametrize("transfer,interp", [(1, 2), (0, 1)])
 def test_results_do_not_depend_on_the_tuned_settings(gpu, transfer, interp):
-    """The settings the autotuner chooses -- particles per G2P work item and
-    particles staged per P2G pass -- change only how work is spread over the
-    CTAs, never the order of a sum, so every result is bitwise the same."""
+    """The settings the autotuner chooses -- particles per G2P work item,
+    particles staged per P2G pass, the largest P2G item taken by one warp --
+    change only how work is spread over the CTAs, never the order of a sum, so
+    every result is bitwise the same."""
     sc = scenes.tiny_scene(n=60000, res=24, transfer=transfer, interpolation=interp)  # ~160 per cell
     runs = []
-    for chunk, stage in ((1024, 0), (256, 16), (4096, 24), (512, 32)):
+    for chunk, stage, wmax in ((1024, 0, -1), (256, 16, 0), (4096, 24, 4096), (512, 32, 256)):
         g = sc.solver()
-        g.set_tuning(g2p_chunk=chunk, p2g_stage=stage)
-        assert g.tuning() == dict(g2p_chunk=chunk, p2g_stage=stage)
+        g.set_tuning(g2p_chunk=chunk, p2g_stage=stage, p2g_warp_max=wmax)
+        assert g.tuning() == dict(g2p_chunk=chunk, p2g_stage=stage, p2g_warp_max=wmax)
         g.step(3)
-        g.set_tuning(g2p_chunk=4096 if chunk != 4096 else 256, p2g_stage=32)  # changed mid-run
+        g.set_tuning(g2p_chunk=4096 if chunk != 4096 else 256, p2g_stage=32, p2g_warp_max=0)  # changed mid-run
         g.step(2)
         runs.append({f: g.download(f) for f in _particle_fields(transfer)})
         g.close()
     for r in runs[1:]:
         for f in _particle_fields(transfer):
             assert np.array_equal(runs[0][f], r[f]), f
+
+
+@pytest.mark.parametrize("transfer,interp", [(1, 2), (0, 1), (1, 1), (0, 0)])
+def test_p2g_by_warps_is_bitwise_p2g_by_ctas(gpu, transfer, interp):
+    """P2G items taken by whole warps sum their particles in p2gKernel's
+    order, so which kernel takes an item changes no bit: every item by CTAs
+    (threshold 0), every item by warps (4096: dense items whose cells hold
+    more than one 96-particle segment, segments across staging passes) and
+    the engine's own choice agree bitwise, on a dense and on a sparse scene."""
+    dense = scenes.tiny_scene(seed=41, n=60000, res=24, transfer=transfer, interpolation=interp)  # ~160 per cell
+    sparse = scenes.tiny_scene(seed=42, n=6000, res=32, transfer=transfer, interpolation=interp)  # < 1 per cell
+    for sc in (dense, sparse):
+        runs = []
+        for wmax in (0, 4096, -1):
+            g = sc.solver()
+            g.set_tuning(p2g_warp_max=wmax)
+            g.step(4)
+            runs.append({f: g.download(f) for f in _particle_fields(transfer)})
+            g.close()
+        for r in runs[1:]:
+            for f in _particle_fields(transfer):
+                assert np.array_equal(runs[0][f], r[f]), (sc.name, f)
+
+
+def test_p2g_by_warps_in_a_batch(gpu):
+    """The same in a batch of two (stencil, transfer) combinations, whose
+    P2G lists are kept per combination."""
+    from mpm_b200.batch import Batch
+    scs = [scenes.tiny_scene(seed=43, n=20000, res=24, transfer=1, interpolation=2),
+           scenes.tiny_scene(seed=44, n=3000, res=20, transfer=0, interpolation=1),
+           scenes.tiny_scene(seed=45, n=8000, res=28, transfer=1, interpolation=2)]
+    runs = []
+    for wmax in (0, 4096):
+        with Batch() as b:
+            ids = [b.add(sc) for sc in scs]
+            b.set_tuning(p2g_warp_max=wmax)
+            b.step(4)
+            runs.append([{f: b.download(sid, f) for f in _particle_fields(sc.transfer)} for sc, sid in zip(scs, ids)])
+    for sc, a, c in zip(scs, runs[0], runs[1]):
+        for f in a:
+            assert np.array_equal(a[f], c[f]), (sc.name, f)
 
 
 def test_autotune_keeps_results_and_caches(gpu, tmp_path, monkeypatch):
@@ -456,16 +498,18 @@ def test_autotune_keeps_results_and_caches(gpu, tmp_path, monkeypatch):
     a = sc.solver()
     got = a.autotune(steps_per_candidate=1)
     assert got["g2p_chunk"] in (256, 512, 1024, 2048, 4096) and got["p2g_stage"] in (16, 24, 32)
+    assert got["p2g_warp_max"] == -1
     assert got["steps"] == 1 + 5 * 2
     a.step(2)
     b = sc.solver()
     b.step(got["steps"] + 2)
     for f in _particle_fields(1):
         assert np.array_equal(a.download(f), b.download(f)), f
-    assert (tmp_path / "tuning.txt").read_text().split()[-2:] == [str(got["g2p_chunk"]), str(got["p2g_stage"])]
+    assert (tmp_path / "tuning.txt").read_text().split()[-3:] == [str(got["g2p_chunk"]), str(got["p2g_stage"]),
+                                                                  str(got["p2g_warp_max"])]
     c = sc.solver()
     again = c.autotune(steps_per_candidate=1)
-    assert again["steps"] == 1 and again["g2p_chunk"] == got["g2p_chunk"] and again["p2g_stage"] == got["p2g_stage"]
+    assert again["steps"] == 1 and all(again[k] == got[k] for k in ("g2p_chunk", "p2g_stage", "p2g_warp_max"))
 
 
 def test_batch_autotune_per_combination(gpu, tmp_path, monkeypatch):
@@ -479,7 +523,7 @@ def test_batch_autotune_per_combination(gpu, tmp_path, monkeypatch):
     with Batch() as b:
         ids = [b.add(sc) for sc in scs]
         rep = b.autotune(steps_per_candidate=1)
-        assert len(rep["combinations"]) == 2 and rep["steps"] == 11
+        assert len(rep["combinations"]) == 2 and rep["steps"] == 1 + 5 * 2
         b.step(3)
         for sc, sid in zip(scs, ids):
             g = sc.solver()

@@ -1019,22 +1019,55 @@ __global__ void __launch_bounds__(P2GWarpLayout<S, MODE>::NT, P2GWarpLayout<S, M
 // Node-block N (4^3 nodes starting at 4N-4) is processed by the active block
 // B = N - d with the smallest d in {0,1}^3 (x + 2y + 4z order).
 // ---------------------------------------------------------------------------
+// Barrier of the 64 threads (two warps) of group g of a 256-thread CTA:
+// named barrier 1 + g (immediate ids, so the kernel reserves only those).
+__device__ __forceinline__ void groupBarrier(int g) {
+    switch (g) {
+        case 0: asm volatile("bar.sync 1, 64;\n" ::: "memory"); break;
+        case 1: asm volatile("bar.sync 2, 64;\n" ::: "memory"); break;
+        case 2: asm volatile("bar.sync 3, 64;\n" ::: "memory"); break;
+        default: asm volatile("bar.sync 4, 64;\n" ::: "memory"); break;
+    }
+}
+
 __device__ __forceinline__ int blockSlotAt(const StepArgs& args, const SceneDev& sc, int x, int y, int z) {
     if (x < 0 || y < 0 || z < 0 || x >= sc.nb[0] || y >= sc.nb[1] || z >= sc.nb[2]) return -1;
     return args.block_slot[sc.block_base + (uint32_t)((z * sc.nb[1] + y) * sc.nb[0] + x)];
 }
 
+// CTAs per SM: 4 (64 registers) where that costs at most a few bytes of
+// spills, else 3 (80 registers): the 8.4M-particle slab's grid pass took
+// 0.15 ms at 4 against 0.26 at 3; quadratic APIC and PIC-FLIP spill 36-44
+// bytes at 64 registers.
 template <int S, int MODE>
-__global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int want_transfer) {
+struct GridBounds {
+    static constexpr int MIN_CTAS = (MODE == MODE_FLIP || (MODE == MODE_APIC_FUSED && S != 4)) ? 3 : 4;
+};
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(kThreads, GridBounds<S, MODE>::MIN_CTAS) gridKernel(StepArgs args, int want_transfer) {
     constexpr int F = modeFields(MODE);
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
-    // first work item and number of work items of the 3^3 blocks around the
-    // current one, index (ox + 1) + 3 (oy + 1) + 9 (oz + 1)
-    __shared__ int nbSlot[27], nbItems[27];
+    // A block's merge is a chain of dependent loads.  With at least two work
+    // items per CTA, each group of 64 threads merges its own blocks (four in
+    // flight per CTA), group g taking items g, g + 4, ... of the CTA's share
+    // and synchronising on its own named barrier; with fewer, the whole CTA
+    // merges one block, four node blocks at a time.  Per group, the first
+    // work item and number of work items of the 3^3 blocks around the
+    // current one, index (ox + 1) + 3 (oy + 1) + 9 (oz + 1).
+    constexpr int kGroups = kThreads / 64;
+    __shared__ int nbSlotAll[kGroups][27], nbItemsAll[kGroups][27];
     const uint32_t nact = args.counters[0];
+    const bool grouped = nact >= 2u * gridDim.x;  // uniform over the CTA
+    const int ngroups = grouped ? kGroups : 1;
+    const int grp = grouped ? (int)(threadIdx.x >> 6) : 0;
+    const int gt = grouped ? (int)(threadIdx.x & 63) : (int)threadIdx.x;  // thread within the group
+    const int dstep = grouped ? 1 : kGroups;  // node blocks per round
+    int* nbSlot = nbSlotAll[grp];
+    int* nbItems = nbItemsAll[grp];
     spanBegin(args.spans, SPAN_GRID);
-    for (uint32_t w = blockIdx.x; w < nact; w += gridDim.x) {
+    for (uint32_t w = blockIdx.x * ngroups + grp; w < nact; w += gridDim.x * ngroups) {
         const BlockItem it = args.active[w];
         const SceneDev& sc = args.scenes[it.scene];
         if (sc.S != S || (want_transfer >= 0 && sc.transfer != want_transfer)) continue;
@@ -1043,20 +1076,22 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
         const uint32_t lb = it.block - sc.block_base;
         const int B[3] = {(int)(lb % (uint32_t)sc.nb[0]), (int)((lb / (uint32_t)sc.nb[0]) % (uint32_t)sc.nb[1]),
                           (int)(lb / ((uint32_t)sc.nb[0] * (uint32_t)sc.nb[1]))};
-        if (threadIdx.x < 27) {
-            const int o[3] = {(int)threadIdx.x % 3 - 1, ((int)threadIdx.x / 3) % 3 - 1, (int)threadIdx.x / 9 - 1};
+        if (gt < 27) {
+            const int o[3] = {gt % 3 - 1, (gt / 3) % 3 - 1, gt / 9 - 1};
             const int slot = blockSlotAt(args, sc, B[0] + o[0], B[1] + o[1], B[2] + o[2]);
             int cnt = 0;
             if (slot >= 0) {
                 const uint32_t blk = args.active[slot].block;
                 for (uint32_t s2 = (uint32_t)slot; s2 < nact && args.active[s2].block == blk; ++s2) ++cnt;
             }
-            nbSlot[threadIdx.x] = slot;
-            nbItems[threadIdx.x] = cnt;
+            nbSlot[gt] = slot;
+            nbItems[gt] = cnt;
         }
-        __syncthreads();
-        for (int round = 0; round < 2; ++round) {
-            const int d = round * 4 + (threadIdx.x >> 6);
+        if (grouped) groupBarrier(grp);
+        else __syncthreads();
+#pragma unroll 1
+        for (int d0 = 0; d0 < 8; d0 += dstep) {  // the 8 node blocks this block may own
+            const int d = d0 + (gt >> 6);
             const int dd[3] = {d & 1, (d >> 1) & 1, (d >> 2) & 1};
             const int N[3] = {B[0] + dd[0], B[1] + dd[1], B[2] + dd[2]};
             if (N[0] >= sc.nb[0] || N[1] >= sc.nb[1] || N[2] >= sc.nb[2]) continue;
@@ -1065,7 +1100,7 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
                 if (nbSlot[(dd[0] - (e & 1) + 1) + 3 * (dd[1] - ((e >> 1) & 1) + 1) + 9 * (dd[2] - ((e >> 2) & 1) + 1)] >= 0)
                     owner = false;
             if (!owner) continue;
-            const int l = threadIdx.x & 63;
+            const int l = gt & 63;
             const int L[3] = {l & 3, (l >> 2) & 3, l >> 4};
             const int n[3] = {4 * N[0] - 4 + L[0], 4 * N[1] - 4 + L[1], 4 * N[2] - 4 + L[2]};
             if (n[0] < 0 || n[1] < 0 || n[2] < 0 || n[0] >= sc.res[0] || n[1] >= sc.res[1] || n[2] >= sc.res[2])
@@ -1168,8 +1203,10 @@ __global__ void __launch_bounds__(kThreads, 4) gridKernel(StepArgs args, int wan
             sc.vstar[node] = make_float4(vs[0], vs[1], vs[2], m);
             if (MODE == MODE_FLIP) sc.vold[node] = make_float4(vo[0], vo[1], vo[2], 0.f);
         }
-        __syncthreads();  // the neighbour table is rewritten for the next item
+        if (grouped) groupBarrier(grp);  // the neighbour table is rewritten for the next item
+        else __syncthreads();
     }
+    __syncthreads();  // every group done: the CTA's span ends here
     spanEnd(args.spans, SPAN_GRID);
 }
 

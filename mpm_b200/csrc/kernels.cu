@@ -1640,11 +1640,16 @@ __device__ __forceinline__ void mbarArrive(uint64_t* bar) {
 // Resident G2P CTAs per SM the register budget is fitted to: 2 gives 128
 // registers a thread and no spills (two-ball G2P 0.132 -> 0.117 ms against 3
 // CTAs at 80 registers, which spill ~150 bytes a thread).
+#ifndef MPM_G2P_THREADS
+#define MPM_G2P_THREADS 256
+#endif
+constexpr int kG2PThreads = MPM_G2P_THREADS;
+constexpr int kG2PWarps = kG2PThreads / 32;
 #ifndef MPM_G2P_MIN_CTAS
-#define MPM_G2P_MIN_CTAS 2
+#define MPM_G2P_MIN_CTAS (2 * 256 / MPM_G2P_THREADS)
 #endif
 template <int S, bool APIC>
-__global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs args, int fused) {
+__global__ void __launch_bounds__(kG2PThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs args, int fused) {
     constexpr int T = S + 3;
     constexpr int TN = tileNodes(S);
     constexpr int TNP = (TN + 7) & ~7;  // buffers 128-byte aligned
@@ -1655,7 +1660,7 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
     // two per-thread prefetch rows of Fe, Fp, V0 (dynamic shared memory: with
     // the tiles they exceed the 48 KB of static shared memory)
     extern __shared__ float4 g2p_dyn[];
-    float (*pre)[kThreads * kPreStride] = reinterpret_cast<float (*)[kThreads * kPreStride]>(g2p_dyn);
+    float (*pre)[kG2PThreads * kPreStride] = reinterpret_cast<float (*)[kG2PThreads * kPreStride]>(g2p_dyn);
     __shared__ SceneDev scs[2];
     __shared__ MaterialDev mat0[2];
     __shared__ BlockItem its[2];
@@ -1725,8 +1730,8 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
         abort_s = 0;
         mbarInit(&full[0], 1);
         mbarInit(&full[1], 1);
-        mbarInit(&empty[0], kWarps);
-        mbarInit(&empty[1], kWarps);
+        mbarInit(&empty[0], kG2PWarps);
+        mbarInit(&empty[1], kG2PWarps);
         mbarInitFence();
         produce(0);
     }
@@ -1762,10 +1767,10 @@ __global__ void __launch_bounds__(kThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepArgs
             // flight during the current one's update (rows alternate)
             int row = 0;
             G2PIn cur = g2pFetch(args, sc, it.start + threadIdx.x, &pre[0][threadIdx.x * kPreStride]);
-            for (uint32_t i = threadIdx.x; i < it.count; i += kThreads) {
-                const bool more = i + kThreads < it.count;
+            for (uint32_t i = threadIdx.x; i < it.count; i += kG2PThreads) {
+                const bool more = i + kG2PThreads < it.count;
                 G2PIn nxt;
-                if (more) nxt = g2pFetch(args, sc, it.start + i + kThreads, &pre[row ^ 1][threadIdx.x * kPreStride]);
+                if (more) nxt = g2pFetch(args, sc, it.start + i + kG2PThreads, &pre[row ^ 1][threadIdx.x * kPreStride]);
                 particleUpdate<S, APIC>(args, sc, it.start + i, cur, more, inside ? &tvs[b][0] : nullptr,
                                         APIC ? nullptr : &tvo[b][0], t0, fused != 0,
                                         &pre[row][threadIdx.x * kPreStride], mat0[b]);
@@ -2093,7 +2098,7 @@ void launchGrid(const LaunchCtx& c, const StepArgs& a, int S, int mode, int want
 #undef GRID_CASE
 }
 
-constexpr size_t kG2PDynSmem = sizeof(float) * 2 * kThreads * kPreStride;
+constexpr size_t kG2PDynSmem = sizeof(float) * 2 * kG2PThreads * kPreStride;
 template <int S, bool APIC>
 static void g2pLaunch(const LaunchCtx& c, const StepArgs& a, int fused) {
     static bool attr = [] {
@@ -2101,7 +2106,7 @@ static void g2pLaunch(const LaunchCtx& c, const StepArgs& a, int fused) {
         return true;
     }();
     (void)attr;
-    g2pKernel<S, APIC><<<c.persistent_blocks, kThreads, kG2PDynSmem, c.stream>>>(a, fused);
+    g2pKernel<S, APIC><<<c.persistent_blocks * (256 / kG2PThreads), kG2PThreads, kG2PDynSmem, c.stream>>>(a, fused);
 }
 
 void launchG2P(const LaunchCtx& c, const StepArgs& args, int S, bool apic, bool fused, int combo) {

@@ -49,9 +49,16 @@ constexpr int kP2GListWord = 64;
 // [kP2GSmallWord + k]: P2G items of combination k of at most kWarpAutoMax
 // particles (read back to decide the warp threshold when it is not set).
 constexpr int kP2GSmallWord = kP2GListWord + 2 * kMaxCombos;
+// The CTA list (c = 1) of combination k holds its items of at least
+// kBigItem particles from the front (counters[kP2GListWord + 2k + 1] of
+// them) and the others from the back (counters[kP2GBackWord + k]), so that
+// the CTAs take the long items first and the short ones fill the tail.
+constexpr int kP2GBackWord = kP2GSmallWord + kMaxCombos;
+constexpr uint32_t kBigItem = 1024;
 constexpr uint32_t kWarpAutoMax = 256;
 constexpr uint32_t kWarpAutoMinItems = 1024;
 constexpr int kCounterWords = 128;
+static_assert(kP2GBackWord + kMaxCombos <= kCounterWords, "counter words");
 
 enum Field : int {
     F_X = 0,

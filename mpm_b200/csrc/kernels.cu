@@ -299,21 +299,25 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
     }
     // Slots of this thread's P2G items in their combination's lists: list 0
     // for items of at most the combination's warp threshold (P2G by warps),
-    // list 1 for the others; aggregated per warp like the G2P items.  The
-    // items of at most kWarpAutoMax particles are counted as well.
-    uint32_t pnext[2] = {0u, 0u};
+    // list 1 for the others -- those of at least kBigItem particles from its
+    // front, the rest from its back (class 2); aggregated per warp like the
+    // G2P items.  The items of at most kWarpAutoMax particles are counted
+    // as well (class 3).
+    uint32_t pnext[3] = {0u, 0u, 0u};
     if (p2g_lists && warp_fast && has) {
-        uint32_t ptot[3] = {0u, 0u, 0u};
+        uint32_t ptot[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int j = 0; j < kCompactPer; ++j) {
             const uint32_t items = (uint32_t)(packed[j] >> 32);
             if (b0 + j >= total_blocks || !items) continue;
             const uint32_t size = ((uint32_t)(packed[j] & 0xffffffffull) + items - 1) / items;
-            ptot[size <= split.p2g_warp_max[lead] ? 0 : 1] += items;
-            if (size <= kWarpAutoMax) ptot[2] += items;
+            ptot[size <= split.p2g_warp_max[lead] ? 0 : (size >= kBigItem ? 1 : 2)] += items;
+            if (size <= kWarpAutoMax) ptot[3] += items;
         }
+        const int words[4] = {kP2GListWord + 2 * lead, kP2GListWord + 2 * lead + 1, kP2GBackWord + lead,
+                              kP2GSmallWord + lead};
 #pragma unroll
-        for (int cls = 0; cls < 3; ++cls) {
+        for (int cls = 0; cls < 4; ++cls) {
             uint32_t inc = ptot[cls];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -321,9 +325,8 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
                 if (lane >= o) inc += y;
             }
             uint32_t base = 0;
-            if (lane == 31 && inc)
-                base = atomicAdd(&counters[cls < 2 ? kP2GListWord + 2 * lead + cls : kP2GSmallWord + lead], inc);
-            if (cls < 2) pnext[cls] = __shfl_sync(0xffffffffu, base, 31) + inc - ptot[cls];
+            if (lane == 31 && inc) base = atomicAdd(&counters[words[cls]], inc);
+            if (cls < 3) pnext[cls] = __shfl_sync(0xffffffffu, base, 31) + inc - ptot[cls];
         }
     }
 #pragma unroll
@@ -355,17 +358,21 @@ __global__ void __launch_bounds__(kThreads) compactOnesweepKernel(
             splitItems(g2p_items + (size_t)k * g2p_cap + g0, b, start, count, parts, (uint32_t)scene);
             if (p2g_lists) {
                 const uint32_t size = (count + items - 1) / items;
-                const int cls = size <= split.p2g_warp_max[k] ? 0 : 1;
+                const int cls = size <= split.p2g_warp_max[k] ? 0 : (size >= kBigItem ? 1 : 2);
+                const int words[3] = {kP2GListWord + 2 * k, kP2GListWord + 2 * k + 1, kP2GBackWord + k};
                 uint32_t p0;
                 if (warp_fast) {
                     p0 = pnext[cls];
                     pnext[cls] += items;
                 } else {
-                    p0 = atomicAdd(&counters[kP2GListWord + 2 * k + cls], items);
+                    p0 = atomicAdd(&counters[words[cls]], items);
                     if (size <= kWarpAutoMax) atomicAdd(&counters[kP2GSmallWord + k], items);
                 }
-                uint32_t* lst = p2g_lists + (size_t)(2 * k + cls) * p2g_list_cap + p0;
-                for (uint32_t q = 0; q < items; ++q) lst[q] = slot + q;
+                uint32_t* lst = p2g_lists + (size_t)(2 * k + (cls == 0 ? 0 : 1)) * p2g_list_cap;
+                for (uint32_t q = 0; q < items; ++q) {
+                    if (cls == 2) lst[p2g_list_cap - 1 - (p0 + q)] = slot + q;  // from the back
+                    else lst[p0 + q] = slot + q;
+                }
             }
         } else {
             block_slot[b] = -1;
@@ -684,14 +691,16 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
     const bool lane_on = grp < L::G;
     // the combination's list of items for whole CTAs, or every active item
     const uint32_t* list = args.p2g_lists ? args.p2g_lists + (size_t)(2 * args.combo + 1) * args.p2g_list_cap : nullptr;
-    const uint32_t nwork = list ? args.counters[kP2GListWord + 2 * args.combo + 1] : args.counters[0];
+    // the long items from the list's front first, then the others from its back
+    const uint32_t nfront = list ? args.counters[kP2GListWord + 2 * args.combo + 1] : 0u;
+    const uint32_t nwork = list ? nfront + args.counters[kP2GBackWord + args.combo] : args.counters[0];
     spanBegin(args.spans, SPAN_P2G);
     __shared__ uint32_t item_s;
     __shared__ SceneDev sc_s;
     for (;;) {
         const uint32_t wi = nextWorkItem(args.sched, nwork, &item_s);
         if (wi >= nwork) break;
-        const uint32_t w = list ? list[wi] : wi;  // the item's slot: its tile
+        const uint32_t w = !list ? wi : (wi < nfront ? list[wi] : list[args.p2g_list_cap - 1 - (wi - nfront)]);
         const BlockItem it = args.active[w];
         {
             const SceneDev& scg = args.scenes[it.scene];
@@ -2006,7 +2015,7 @@ void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t 
     cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * compactScratchWords64(total_blocks), c.stream);
     cudaMemsetAsync(bb.counters, 0, sizeof(uint32_t) * 4, c.stream);
     cudaMemsetAsync(bb.counters + kG2PCountWord, 0, sizeof(uint32_t) * kMaxCombos, c.stream);
-    cudaMemsetAsync(bb.counters + kP2GListWord, 0, sizeof(uint32_t) * 3 * kMaxCombos, c.stream);  // lists, small
+    cudaMemsetAsync(bb.counters + kP2GListWord, 0, sizeof(uint32_t) * 4 * kMaxCombos, c.stream);  // lists, small, back
     noteLaunches(1);
     compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
         bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <deque>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -380,6 +381,12 @@ public:
             if (!pool_) return pst;
         }
         CUDA_TRY(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_));
+        {   // the host-transfer kernels, once per device (see preloadTransferKernels)
+            static std::mutex mu;
+            static std::set<int> done;
+            std::lock_guard<std::mutex> lock(mu);
+            if (done.insert(device_).second) preloadTransferKernels();
+        }
         CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CUDA_TRY(cudaStreamCreateWithFlags(&compact_stream_, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&compact_fork_, cudaEventDisableTiming));
@@ -889,6 +896,20 @@ public:
         tile_stride_ = (size_t)7 * tileNodes(maxS);
         MPM_TRY(grow(tiles_, sizeof(float) * tile_stride_ * max_active_, "P2G tiles"));
         MPM_TRY(grow(scenes_dev_, sizeof(SceneDev) * std::max(ns, 1), "scene table"));
+        // Room in the pool for the download staging buffers (two float4 per
+        // particle, taken at a scene's first download): taken and given back
+        // here, so that the first download -- or a later engine's -- finds the
+        // memory in the pool instead of growing it in the middle of a run
+        // (about 1 ms for a 1M-particle scene).  Best effort.
+        if (ntot > staging_reserved_) {
+            void* p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, (size_t)32 * ntot, pool_, stream_) == cudaSuccess) {
+                CUDA_TRY(cudaFreeAsync(p, stream_));
+                staging_reserved_ = ntot;
+            } else {
+                cudaGetLastError();
+            }
+        }
         // TMA maps of each scene's v* and v grids (G2P stages its tiles with them)
         {
             std::vector<unsigned char> maps((size_t)2 * kTensorMapBytes * std::max(ns, 1), 0);
@@ -2262,6 +2283,7 @@ public:
 private:
     int device_ = 0, num_sms_ = 148;
     cudaMemPool_t pool_ = nullptr;         // the device's scene pool (init)
+    size_t staging_reserved_ = 0;          // particles whose download staging the pool was grown for
     uint32_t* host_word_ = nullptr;        // pinned: work-item count read back by checkP2GStage
     cudaEvent_t stage_event_ = nullptr;    // completion of that read-back
     bool stage_pending_ = false;

@@ -119,6 +119,7 @@ cudaError_t launchSolve(const LaunchCtx& c, const SolveBuffers& b, int parity, c
 // A non-finite particle speed sets ERR_NONFINITE in err.
 void launchCfl(const LaunchCtx& c, int parity, size_t max_n, uint32_t* err);
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out);
+void preloadTransferKernels();
 void launchScatterField(const LaunchCtx& c, int scene, int parity, int field, int comps, const float* in);
 size_t p2gSmemBytes(int S, int mode);
 // Writes the kTensorMapBytes TMA tensor map of a dense float4 grid (res[3]

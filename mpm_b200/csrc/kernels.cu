@@ -2235,6 +2235,17 @@ void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float 
                                                                           (size_t)c.num_sms * 16));
     densityKernel<<<blocks, kThreads, 0, c.stream>>>(vstar, nodes, inv_cell_vol, out);
 }
+// Loads the kernels of the host transfers (gather for downloads, scatter
+// for uploads) on the current device: with CUDA's lazy loading a kernel is
+// loaded at its first launch, which would otherwise stall a user's first
+// download after the steps (about 2 ms).  Called once per device.
+void preloadTransferKernels() {
+    cudaFuncAttributes attr;
+    cudaFuncGetAttributes(&attr, gatherFieldKernel);
+    cudaFuncGetAttributes(&attr, scatterFieldKernel);
+    cudaGetLastError();
+}
+
 void launchGatherField(const LaunchCtx& c, int scene, int parity, int field, int comps, int mode, float* out) {
     noteLaunches(1);
     gatherFieldKernel<<<c.particle_blocks, kThreads, 0, c.stream>>>(c.scenes, scene, parity, field, comps, mode, out);

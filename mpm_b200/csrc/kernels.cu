@@ -550,14 +550,13 @@ __device__ __forceinline__ void p2gStageParticle(const StepArgs& args, const Sce
         for (int k = 0; k < S; ++k) {
             if (MODE == MODE_MASS) {
                 my[WB + a * S + k] = wk[k];
-            } else {
-                my[WB + 2 * (a * S + k)] = wk[k];
-                my[WB + 2 * (a * S + k) + 1] = dwk[k] * inv_h;
+            } else {  // (w, w'/h) pairs: 8-byte stores (WB is even, rows 16-byte aligned)
+                *reinterpret_cast<float2*>(my + WB + 2 * (a * S + k)) = make_float2(wk[k], dwk[k] * inv_h);
             }
         }
     }
     const float m = bad ? 0.f : ldg(pf + F_MASS * cap + old);
-    my[0] = m;
+    if (MODE == MODE_MASS) my[0] = m;
     if (MODE != MODE_MASS) {
         float v[3] = {ldg(pf + (F_V + 0) * cap + old), ldg(pf + (F_V + 1) * cap + old),
                       ldg(pf + (F_V + 2) * cap + old)};
@@ -565,11 +564,13 @@ __device__ __forceinline__ void p2gStageParticle(const StepArgs& args, const Sce
         float T[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) T[k] = ts * ldg(pf + (F_TAU + k) * cap + old);
+        // the row's header in 16-byte stores: (m, p), then the stress
+        // factors (and APIC's h m C): the layout the accumulation reads
+        float4* my4 = reinterpret_cast<float4*>(my);
         if (MODE == MODE_FLIP) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) my[1 + a] = m * v[a];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) my[4 + k] = T[k];
+            my4[0] = make_float4(m, m * v[0], m * v[1], m * v[2]);
+            my4[1] = make_float4(T[0], T[1], T[2], T[3]);
+            *reinterpret_cast<float2*>(my + 8) = make_float2(T[4], T[5]);
         } else {
             float mC[9];
             if (sc.transfer == MPM_TRANSFER_APIC) {
@@ -580,14 +581,17 @@ __device__ __forceinline__ void p2gStageParticle(const StepArgs& args, const Sce
 #pragma unroll
                 for (int k = 0; k < 9; ++k) mC[k] = 0.f;
             }
+            float q[3], hC[9];
 #pragma unroll
             for (int a = 0; a < 3; ++a)
-                my[1 + a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] +
-                                        mC[3 * a + 2] * delta[2]);
+                q[a] = m * v[a] - (mC[3 * a] * delta[0] + mC[3 * a + 1] * delta[1] + mC[3 * a + 2] * delta[2]);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) my[4 + k] = h * mC[k];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) my[13 + k] = T[k];
+            for (int k = 0; k < 9; ++k) hC[k] = h * mC[k];
+            my4[0] = make_float4(m, q[0], q[1], q[2]);
+            my4[1] = make_float4(hC[0], hC[1], hC[2], hC[3]);
+            my4[2] = make_float4(hC[4], hC[5], hC[6], hC[7]);
+            my4[3] = make_float4(hC[8], T[0], T[1], T[2]);
+            my4[4] = make_float4(T[3], T[4], T[5], 0.f);  // [19] is padding of the header
         }
     }
 }
@@ -888,6 +892,8 @@ struct P2GWarpLayout {
     static constexpr int kStage = 16;  // particles staged per pass
     static constexpr int NT = 256, NW = NT / 32;
     // per warp: its item's scene entry, its tile [F][TN], its staging rows
+    // (field-major: a column's 16 lanes add to 16 different banks; a
+    // node-major tile of 16-byte words had bank conflicts and was slower)
     static constexpr int kSceneFloats = (int)((sizeof(SceneDev) + 15) / 16 * 4);
     static constexpr int kTileFloats = (F * TN + 3) / 4 * 4;
     static constexpr int kWarpFloats = kSceneFloats + kTileFloats + kStage * P;
@@ -956,7 +962,7 @@ __global__ void __launch_bounds__(P2GWarpLayout<S, MODE>::NT, P2GWarpLayout<S, M
             const int4* src = reinterpret_cast<const int4*>(args.scenes + it.scene);
             int4* dst = reinterpret_cast<int4*>(&sc);
             for (int q = lane; q < (int)(sizeof(SceneDev) / 16); q += 32) dst[q] = src[q];
-            for (int q = lane; q < F * TN; q += 32) tile[q] = 0.f;
+            for (int q = lane; q < W::kTileFloats; q += 32) tile[q] = 0.f;
         }
         __syncwarp();
         const float* pf = sc.buf[args.parity].f;

@@ -364,9 +364,10 @@ MPM_API mpm_status mpm_solver_stats(mpm_solver* s, mpm_step_stats* out);
  *                 from the particle density after the first step);
  *   p2g_warp_max: P2G work items of at most this many particles are taken by
  *                 single warps instead of whole CTAs, 0..MPM_P2G_WARP_MAX_MAX
- *                 (0: none; -1: chosen after the first step -- 256 where a
- *                 (stencil, transfer) combination has at least 1024 items of
- *                 at most 256 particles, else 0). */
+ *                 (0: none; -1: the engine's choice -- items of at most 256
+ *                 particles, taken by warps in a step where their
+ *                 (stencil, transfer) combination has at least 1024 of them,
+ *                 decided on the device each step). */
 typedef struct mpm_tuning {
     int32_t g2p_chunk;
     int32_t p2g_stage;

@@ -936,6 +936,7 @@ public:
         incremental_ok_ = false;
         stage_check_ = true;
         stage_pending_ = false;  // a read-back issued before the sync above is stale
+        for (bool& f : warp_few_) f = false;  // the new set's small items: decided on the device until read back
         any_implicit_ = false;
         for (auto& s : scenes_) any_implicit_ |= s->beta > 0.f;
         MPM_TRY(ensureSolveBuffers());
@@ -1084,6 +1085,7 @@ public:
         a.spans = nullptr;  // set per combination by the step
         a.p2g_lists = nullptr;  // the step's P2G launches take their combination's lists
         a.p2g_list_cap = (uint32_t)max_active_;
+        a.p2g_warp = P2G_WARP_NONE;
         return a;
     }
 
@@ -1427,8 +1429,9 @@ public:
                 ck.p2g_stage = p2gStageOf(cs[k]);
                 ak.combo = (int)k;
                 ak.p2g_lists = p2g_lists_.as<uint32_t>();
+                ak.p2g_warp = warpModeOf(cs[k], k);
                 launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
-                if (warpMaxOf(cs[k], k)) launchP2GWarp(ck, ak, cs[k].S, mode);
+                if (ak.p2g_warp != P2G_WARP_NONE) launchP2GWarp(ck, ak, cs[k].S, mode);
                 launchGrid(ck, ak, cs[k].S, mode, cs[k].transfer);
                 launchG2P(ck, ak, cs[k].S, cs[k].transfer == MPM_TRANSFER_APIC, true, (int)k);
                 if (k > 0) {
@@ -1447,8 +1450,9 @@ public:
                 const int mode = cs[k].transfer == MPM_TRANSFER_APIC ? MODE_APIC_FUSED : MODE_FLIP;
                 ak.combo = (int)k;
                 ak.p2g_lists = p2g_lists_.as<uint32_t>();
+                ak.p2g_warp = warpModeOf(cs[k], k);
                 launchP2G(ck, ak, cs[k].S, mode, cs[k].transfer);
-                if (warpMaxOf(cs[k], k)) launchP2GWarp(ck, ak, cs[k].S, mode);
+                if (ak.p2g_warp != P2G_WARP_NONE) launchP2GWarp(ck, ak, cs[k].S, mode);
                 if (tune_run_) CUDA_TRY(cudaEventRecord(tune_ev_[k][1], stream_));
             }
             mark(KF_P2G, 1);
@@ -1523,11 +1527,21 @@ public:
         auto it = tuning_.find({S, transfer});
         return it != tuning_.end() ? it->second : mpm_tuning{(int32_t)kDefaultG2PChunk, 0, -1};
     }
-    // The warp threshold of combination k (index in combos()): its tuned value,
-    // or the engine's own choice.
-    uint32_t warpMaxOf(const Combo& c, size_t k) const {
+    // The P2G items of at most this many particles make combination c's
+    // small list (list 0): its tuned warp threshold, or kWarpAutoMax.
+    uint32_t warpMaxOf(const Combo& c) const {
         const int w = tuningOf(c.S, c.transfer).p2g_warp_max;
-        return w >= 0 ? (uint32_t)w : (k < (size_t)kMaxCombos ? warp_auto_[k] : 0u);
+        return w >= 0 ? (uint32_t)w : kWarpAutoMax;
+    }
+    // Who takes the small list of combination k (index in combos()) this
+    // step: with the engine's own choice (-1) the device decides from the
+    // list's length (P2G_WARP_AUTO), unless the last read-back found too few
+    // small items to launch the warp kernel at all.
+    int warpModeOf(const Combo& c, size_t k) const {
+        const int w = tuningOf(c.S, c.transfer).p2g_warp_max;
+        if (w > 0) return P2G_WARP_ALWAYS;
+        if (w == 0) return P2G_WARP_NONE;
+        return (k < (size_t)kMaxCombos && !warp_few_[k]) ? P2G_WARP_AUTO : P2G_WARP_NONE;
     }
     int p2gStageOf(const Combo& c) const {
         const int st = tuningOf(c.S, c.transfer).p2g_stage;
@@ -1542,7 +1556,7 @@ public:
         auto cs = combos();
         for (size_t k = 0; k < cs.size() && k < (size_t)kMaxCombos; ++k) {
             g.g2p_chunk[k] = (uint32_t)tuningOf(cs[k].S, cs[k].transfer).g2p_chunk;
-            g.p2g_warp_max[k] = warpMaxOf(cs[k], k);
+            g.p2g_warp_max[k] = warpMaxOf(cs[k]);
         }
         return g;
     }
@@ -1742,12 +1756,12 @@ public:
         const int stage = (items > 0 && ntot_ / items < 512) ? 16 : 32;
         bool changed = stage != p2g_stage_;
         p2g_stage_ = stage;
-        // warps take the small P2G items of a combination that has enough of
-        // them to fill the GPU (one warp per item: few items leave it idle)
+        // a combination with too few small P2G items for warps skips the
+        // warp kernel's launch (the device would leave them to p2gKernel)
         for (int k = 0; k < kMaxCombos; ++k) {
-            const uint32_t w = host_word_[1 + k] >= kWarpAutoMinItems ? kWarpAutoMax : 0u;
-            changed |= w != warp_auto_[k];
-            warp_auto_[k] = w;
+            const bool few = host_word_[1 + k] < kWarpAutoMinItems;
+            changed |= few != warp_few_[k];
+            warp_few_[k] = few;
         }
         if (changed) dropGraphs();
         return MPM_OK;
@@ -2321,11 +2335,10 @@ private:
     int key_bits_ = 1;
     DevMem keys_[2], vals_[2], sort_scratch_, inc_scratch_, compact_scratch_, block_count_, sbb_, active_,
         outside_, counters_, block_slot_, tiles_, scenes_dev_, err_, tmp_, g2p_items_, tmaps_, spans_, p2g_lists_;
-    // Per combination, the engine's own warp threshold for P2G (used where
-    // the tuning leaves it to the engine): kWarpAutoMax where the first step
-    // after a change of the scene set found at least kWarpAutoMinItems items
-    // of at most kWarpAutoMax particles, else 0 (see checkP2GStage).
-    uint32_t warp_auto_[kMaxCombos] = {};
+    // Per combination: the first step after a change of the scene set found
+    // fewer than kWarpAutoMinItems small P2G items, so the step does not
+    // launch the warp kernel (see checkP2GStage, warpModeOf).
+    bool warp_few_[kMaxCombos] = {};
     bool profiling_ = false;
     bool step_timing_ = false;
     std::deque<std::pair<cudaEvent_t, cudaEvent_t>> step_events_;

@@ -57,6 +57,14 @@ constexpr int kP2GBackWord = kP2GSmallWord + kMaxCombos;
 constexpr uint32_t kBigItem = 1024;
 constexpr uint32_t kWarpAutoMax = 256;
 constexpr uint32_t kWarpAutoMinItems = 1024;
+// Who takes the small P2G items (list 0) in a step: p2gKernel after its own
+// list (no warp kernel launched), p2gWarpKernel, or -- decided on the device
+// from the list's length, the same way by both kernels -- p2gWarpKernel when
+// the list holds at least kWarpAutoMinItems items, else p2gKernel.
+enum P2GWarp : int { P2G_WARP_NONE = 0, P2G_WARP_ALWAYS = 1, P2G_WARP_AUTO = 2 };
+__host__ __device__ inline bool p2gWarpTakesSmall(int mode, uint32_t n_small) {
+    return mode == P2G_WARP_ALWAYS || (mode == P2G_WARP_AUTO && n_small >= kWarpAutoMinItems);
+}
 constexpr int kCounterWords = 128;
 static_assert(kP2GBackWord + kMaxCombos <= kCounterWords, "counter words");
 
@@ -197,6 +205,7 @@ struct StepArgs {
                                  // list c at p2g_lists + (2 combo + c) p2g_list_cap; null: P2G
                                  // takes every item of the active list
     uint32_t p2g_list_cap;
+    int p2g_warp;                // who takes list 0 (the small items): P2G_WARP_NONE, _ALWAYS or _AUTO
     const unsigned char* tmaps;  // kTensorMapBytes x 2 per scene (64-byte aligned): TMA maps of v*, v
     unsigned long long* spans;   // this combination's kernel time spans (see KernelSpan), or null
 };

@@ -695,16 +695,24 @@ __global__ void __launch_bounds__(P2GLayout<S, MODE, STAGE>::NT, P2GLayout<S, MO
     const bool lane_on = grp < L::G;
     // the combination's list of items for whole CTAs, or every active item
     const uint32_t* list = args.p2g_lists ? args.p2g_lists + (size_t)(2 * args.combo + 1) * args.p2g_list_cap : nullptr;
-    // the long items from the list's front first, then the others from its back
+    // the long items from the list's front first, then the others from its
+    // back, then -- unless the warp kernel takes them -- the small items
     const uint32_t nfront = list ? args.counters[kP2GListWord + 2 * args.combo + 1] : 0u;
-    const uint32_t nwork = list ? nfront + args.counters[kP2GBackWord + args.combo] : args.counters[0];
+    const uint32_t nlist1 = list ? nfront + args.counters[kP2GBackWord + args.combo] : 0u;
+    const uint32_t nsmall = list ? args.counters[kP2GListWord + 2 * args.combo] : 0u;
+    const uint32_t nwork = !list ? args.counters[0]
+                                 : nlist1 + (p2gWarpTakesSmall(args.p2g_warp, nsmall) ? 0u : nsmall);
+    const uint32_t* small = list ? args.p2g_lists + (size_t)(2 * args.combo) * args.p2g_list_cap : nullptr;
     spanBegin(args.spans, SPAN_P2G);
     __shared__ uint32_t item_s;
     __shared__ SceneDev sc_s;
     for (;;) {
         const uint32_t wi = nextWorkItem(args.sched, nwork, &item_s);
         if (wi >= nwork) break;
-        const uint32_t w = !list ? wi : (wi < nfront ? list[wi] : list[args.p2g_list_cap - 1 - (wi - nfront)]);
+        const uint32_t w = !list ? wi
+                           : wi < nfront ? list[wi]
+                           : wi < nlist1 ? list[args.p2g_list_cap - 1 - (wi - nfront)]
+                                         : small[wi - nlist1];
         const BlockItem it = args.active[w];
         {
             const SceneDev& scg = args.scenes[it.scene];
@@ -920,7 +928,9 @@ __global__ void __launch_bounds__(P2GWarpLayout<S, MODE>::NT, P2GWarpLayout<S, M
     // warps that have run out; the last of them clears both
     uint32_t* sched = args.sched + 2;
     const uint32_t warps = gridDim.x * (uint32_t)W::NW;
-    if (nwork == 0) return;  // nothing for warps (the scheduler is untouched)
+    // nothing for warps (the scheduler is untouched): p2gKernel takes the
+    // small items when the list is too short to fill the GPU with warps
+    if (nwork == 0 || !p2gWarpTakesSmall(args.p2g_warp, nwork)) return;
     NodeAcc acc[S];
     // a segment done: the groups' columns summed in group order (as
     // p2gKernel), added by group 0 into the tile nodes of the segment's cell

@@ -1,10 +1,13 @@
 // kernels.cu -- the MPM step kernels for sm_100a.
 //
 //   keyKernel       cell keys of the live particle order (first step / after uploads)
-//   packBlocks / compactBlocks   active-block list from per-block particle counts
+//   compactOnesweepKernel   work items from per-block particle counts (P2G's,
+//                   with their per-combination lists, and G2P's)
 //   stressKernel    V0 * stress (tau) from Fe, Fp (first step / after uploads)
-//   p2gKernel       deterministic block scatter (src/mpm_solver3d.cu:237-294,
-//                   src/apic_mpm_solver3d.cu:245-304)
+//   p2gKernel       deterministic block scatter by whole CTAs
+//                   (src/mpm_solver3d.cu:237-294, src/apic_mpm_solver3d.cu:245-304)
+//   p2gWarpKernel   the same scatter by single warps for small work items
+//                   (bitwise p2gKernel's tiles)
 //   gridKernel      tile merge + gravity + velocity update + collision in one
 //                   pass (src/mpm_solver3d.cu:394-426, src/grid3d.cu:36-41)
 //   g2pKernel       gather + transfer blend + Fe/Fp plasticity + SVD + next

@@ -308,7 +308,7 @@ def peaks():
 TRAFFIC_SOURCE = ("ncu capture of one launch of the kernel in a separate run of this bench on the same workload "
                   "(dram__bytes_read.sum + dram__bytes_write.sum)")
 NCU_TRAFFIC = {
-    "two_balls": {"p2g": 104.7e6, "g2p": 240.4e6, "grid": 4.45e6},
+    "two_balls": {"p2g": 104.8e6, "g2p": 240.4e6, "grid": 4.45e6},
 }
 
 

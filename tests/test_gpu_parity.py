@@ -470,6 +470,23 @@ def test_p2g_by_warps_is_bitwise_p2g_by_ctas(gpu, transfer, interp):
                 assert np.array_equal(runs[0][f], r[f]), (sc.name, f)
 
 
+def test_p2g_warp_rule_decided_on_the_device(gpu):
+    """A sparse scene with thousands of small work items (the engine's rule
+    gives them to warps from the first step, decided on the device) against
+    every item by CTAs and every item by warps: bitwise the same."""
+    sc = scenes.tiny_scene(seed=46, n=20000, res=192, transfer=1, interpolation=2)  # ~3k blocks of ~6
+    runs = []
+    for wmax in (-1, 0, 4096):
+        g = sc.solver()
+        g.set_tuning(p2g_warp_max=wmax)
+        g.step(3)
+        runs.append({f: g.download(f) for f in _particle_fields(1)})
+        g.close()
+    for r in runs[1:]:
+        for f in _particle_fields(1):
+            assert np.array_equal(runs[0][f], r[f]), f
+
+
 def test_p2g_by_warps_in_a_batch(gpu):
     """The same in a batch of two (stencil, transfer) combinations, whose
     P2G lists are kept per combination."""

@@ -293,15 +293,6 @@ struct TuneCache {
 };
 static TuneCache g_tune_cache;
 
-// An unsigned setting from the environment, or `dflt` when unset or not a number.
-static uint32_t envU32(const char* name, uint32_t dflt) {
-    const char* v = getenv(name);
-    if (!v || !*v) return dflt;
-    char* end = nullptr;
-    const unsigned long x = strtoul(v, &end, 10);
-    return (end && *end == 0) ? (uint32_t)x : dflt;
-}
-
 class Engine {
 public:
     struct GraphSlot {

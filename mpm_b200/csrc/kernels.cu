@@ -1038,6 +1038,7 @@ __global__ void __launch_bounds__(P2GWarpLayout<S, MODE>::NT, P2GWarpLayout<S, M
         for (int q = lane; q < F * TN; q += 32) out[q] = tile[q];
         __syncwarp();  // the tile is read before the next item clears it
     }
+    __syncthreads();  // every warp done: the CTA's span ends here
     spanEnd(args.spans, SPAN_P2G, false);
 }
 
@@ -1814,6 +1815,7 @@ __global__ void __launch_bounds__(kG2PThreads, MPM_G2P_MIN_CTAS) g2pKernel(StepA
         for (int s = 0; s < 2; ++s)
             if ((issued >> s) & 1u) waitTile(&full[s], (full_ph >> s) & 1u, args.err, nullptr);
     }
+    __syncthreads();  // every warp done: the CTA's span ends here
     spanEnd(args.spans, SPAN_G2P);
 }
 

@@ -316,6 +316,21 @@ def traffic_of(family, workload):
     return NCU_TRAFFIC.get(workload, {}).get(family)
 
 
+# FP32 pipe use of one launch of each kernel family (sm__pipe_fma_cycles_active,
+# fraction of the peak sustained while active) from the same ncu captures: the
+# cubic configurations are FP32-issue bound rather than HBM bound, so this
+# fraction is reported beside the HBM one.
+FP32_SOURCE = ("ncu capture of one launch of the kernel in a separate run of this bench on the same workload "
+               "(sm__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active / 100)")
+NCU_FP32 = {
+    "two_balls": {"p2g": 0.401, "g2p": 0.447, "grid": 0.048},
+}
+
+
+def fp32_of(family, workload):
+    return NCU_FP32.get(workload, {}).get(family)
+
+
 # --- CPU and naive-GPU baselines --------------------------------------------------
 def cpu_model():
     try:
@@ -467,6 +482,7 @@ def run_ours(args, ws, rank, local):
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
             "traffic": traffic_of(dom, work.name), "traffic_source": TRAFFIC_SOURCE,
+            "fp32_pipe_frac": fp32_of(dom, work.name), "fp32_source": FP32_SOURCE,
             "algorithmic_bytes": byt, "avg_launch_ms": spans[dom][0],
             "kernel_ms_in_step": {k: v[0] for k, v in spans.items()}, "span_steps": spans[dom][1],
             "kernel_timing": "device-measured span of every launch (first CTA start to last CTA end, %globaltimer) "

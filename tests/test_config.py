@@ -148,6 +148,22 @@ def test_read_reference_point_cloud():
     assert np.allclose(g.min(0), [89, 19, 89], atol=1e-3) and np.allclose(g.max(0), [111, 41, 111], atol=1e-3)
 
 
+def test_reference_two_ball_scene(tmp_path):
+    """config/snow_two_balls_sparse.yaml with its two point clouds: two groups
+    of different plasticity limits, 6,101 + 56,907 particles on the 200^3
+    grid, scaled by the stride."""
+    from mpm_b200.config import build_particles
+    from ref_scenes import unpack_two_balls
+    cfg = parseYAML(unpack_two_balls(str(tmp_path)))
+    p = build_particles(cfg)
+    assert p.n == 6101 + 56907
+    assert cfg.compressions == pytest.approx([5.0e-2, 0.1e-2]) and cfg.stretches == pytest.approx([9.0e-3, 1.0e-3])
+    x = np.asarray(p.positions)
+    assert x.min() > 0.0 and x.max() < 200 * 5e-3
+    v = np.asarray(p.velocities)
+    assert np.allclose(v[:6101, 0], 2.5) and np.allclose(v[6101:, 0], -2.5)
+
+
 def test_cpp_facade_compiles_and_links(tmp_path):
     src = tmp_path / "facade.cpp"
     src.write_text("""

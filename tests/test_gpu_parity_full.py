@@ -197,25 +197,28 @@ def test_reference_snow_cube_yaml_five_steps(gpu):
     assert abs(float(np.median(v[:, 1])) + 9.80665 * 5e-3) < 1e-3
 
 
-def test_reference_two_balls_yaml_five_steps(gpu, tmp_path):
+@pytest.mark.parametrize("transfer", [_abi.TRANSFER_PIC_FLIP, _abi.TRANSFER_APIC])
+def test_reference_two_balls_yaml_five_steps(gpu, tmp_path, transfer):
     """config/snow_two_balls_sparse.yaml of the reference with its two point
     clouds (6,101 + 56,907 particles, two materials of different plasticity
     limits, cubic B-splines, dt 1e-3 on the 200^3 grid), built by the YAML
-    builder (PIC-FLIP solver, as the reference's PIC-FLIP demo), five steps
-    against the oracle built from the same configuration."""
-    from mpm_b200.config import build_particles, buildMPMSolver3DFromYAML, parseYAML
+    builders (the PIC-FLIP and the APIC solver, as the reference's two
+    demos), five steps against the oracle built from the same configuration."""
+    from mpm_b200.config import (build_particles, buildAPICMPMSolver3DFromYAML, buildMPMSolver3DFromYAML,
+                                 parseYAML)
     from mpm_b200.solver import scene_desc
     from ref_scenes import unpack_two_balls
     cfg = parseYAML(unpack_two_balls(str(tmp_path)))
-    g, n = buildMPMSolver3DFromYAML(cfg)
+    build = buildAPICMPMSolver3DFromYAML if transfer == _abi.TRANSFER_APIC else buildMPMSolver3DFromYAML
+    g, n = build(cfg)
     assert n == 6101 + 56907
     p = build_particles(cfg)
     desc = scene_desc(cfg.origin, cfg.resolution, cfg.stride, cfg.friction_coeff, cfg.blend_coeff, cfg.interp_type,
-                      cfg.delta_time, transfer=_abi.TRANSFER_PIC_FLIP, gravity=cfg.gravity, boundary=cfg.boundary,
+                      cfg.delta_time, transfer=transfer, gravity=cfg.gravity, boundary=cfg.boundary,
                       sticky_cells=cfg.sticky_cells)
     g.step(5)
     o64, o32 = _oracles(desc, p, 5)
-    _compare(g.download, o64, o32, _abi.TRANSFER_PIC_FLIP, tag="snow_two_balls_sparse.yaml")
+    _compare(g.download, o64, o32, transfer, tag="snow_two_balls_sparse.yaml transfer %d" % transfer)
     # the balls approach each other at 2.5 m/s
     v = g.download(_abi.FIELD_VELOCITY)
     assert float(np.median(v[:6101, 0])) > 2.0 and float(np.median(v[6101:, 0])) < -2.0

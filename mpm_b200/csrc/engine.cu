@@ -60,6 +60,9 @@ mpm_status writeDensityVdb(const float* density, const int32_t* res, const char*
 
 enum KernelFamily { KF_KEYS = 0, KF_SORT, KF_COMPACT, KF_STRESS, KF_P2G, KF_GRID, KF_G2P, KF_COUNT };
 
+// Scenes of at least this many particles are uploaded in cell-sorted order.
+constexpr size_t kSortedUploadMin = (size_t)1 << 16;
+
 static int stencilSize(int interp) {
     return interp == MPM_INTERP_LINEAR ? 2 : (interp == MPM_INTERP_QUADRATIC_BSPLINE ? 3 : 4);
 }
@@ -100,6 +103,40 @@ static cudaMemPool_t scenePool(int device, mpm_status* st) {
     }
     *st = MPM_OK;
     return pools[device];
+}
+
+// Streams of destroyed engines, kept per device for the next engines (a
+// solver that is created per request, a benchmark's repeated constructions):
+// creating a stream costs about 0.1 ms, taking an idle one nothing.  A
+// stream is given back after its engine's last synchronize; what it still
+// holds (stream-ordered frees to the pool) runs before the next owner's work.
+static std::mutex g_stream_mu;
+static std::vector<std::pair<int, cudaStream_t>> g_idle_streams;
+constexpr size_t kMaxIdleStreams = 64;
+
+static cudaError_t takeStream(int device, cudaStream_t* s) {
+    {
+        std::lock_guard<std::mutex> lock(g_stream_mu);
+        for (size_t i = g_idle_streams.size(); i-- > 0;)
+            if (g_idle_streams[i].first == device) {
+                *s = g_idle_streams[i].second;
+                g_idle_streams.erase(g_idle_streams.begin() + (long)i);
+                return cudaSuccess;
+            }
+    }
+    return cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+}
+
+static void giveStream(int device, cudaStream_t s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(g_stream_mu);
+        if (g_idle_streams.size() < kMaxIdleStreams) {
+            g_idle_streams.push_back({device, s});
+            return;
+        }
+    }
+    cudaStreamDestroy(s);
 }
 
 struct DevMem {
@@ -304,7 +341,7 @@ public:
         if (stream_) cudaStreamSynchronize(stream_);
         if (copy_stream_) cudaStreamSynchronize(copy_stream_);
         scenes_.clear();  // their staging events before the copy stream
-        if (copy_stream_) cudaStreamDestroy(copy_stream_);
+        giveStream(device_, copy_stream_);
         dropGraphs();
         for (int k = 0; k < KF_COUNT; ++k) {
             if (ev_[k][0]) cudaEventDestroy(ev_[k][0]);
@@ -319,14 +356,14 @@ public:
         for (int k = 0; k < kMaxSide; ++k) {
             if (side_[k]) {
                 cudaStreamSynchronize(side_[k]);
-                cudaStreamDestroy(side_[k]);
+                giveStream(device_, side_[k]);
             }
             if (join_[k]) cudaEventDestroy(join_[k]);
         }
         if (fork_) cudaEventDestroy(fork_);
         if (compact_stream_) {
             cudaStreamSynchronize(compact_stream_);
-            cudaStreamDestroy(compact_stream_);
+            giveStream(device_, compact_stream_);
         }
         if (compact_fork_) cudaEventDestroy(compact_fork_);
         if (compact_join_) cudaEventDestroy(compact_join_);
@@ -341,7 +378,7 @@ public:
                 if (e) cudaEventDestroy(e);
         if (host_word_) g_pinned_words.give(host_word_);
         if (stage_event_) cudaEventDestroy(stage_event_);
-        if (stream_) cudaStreamDestroy(stream_);
+        giveStream(device_, stream_);
     }
 
     // Device memory of the engine (batch scratch, scene buffers) comes from
@@ -378,8 +415,8 @@ public:
             std::lock_guard<std::mutex> lock(mu);
             if (done.insert(device_).second) preloadTransferKernels();
         }
-        CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        CUDA_TRY(cudaStreamCreateWithFlags(&compact_stream_, cudaStreamNonBlocking));
+        CUDA_TRY(takeStream(device_, &stream_));
+        CUDA_TRY(takeStream(device_, &compact_stream_));
         CUDA_TRY(cudaEventCreateWithFlags(&compact_fork_, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&compact_join_, cudaEventDisableTiming));
         MPM_TRY(alloc(err_, sizeof(uint32_t), "error flags"));
@@ -514,29 +551,55 @@ public:
         std::unique_ptr<SceneHost> sc;
         MPM_TRY(newScene(d, p.materials, p.nmaterials, p.n, &sc));
         const size_t cap = std::max<size_t>(p.n, 1);
-        // Particle state in the caller's order: the caller's arrays are copied
-        // as they are (x, v interleaved; m; V0 if prescribed) into a staging
-        // buffer and a kernel writes the SoA planes (Fe = Fp = I, B = 0).
+        // The caller's arrays are copied as they are (x, v interleaved; m; V0
+        // if prescribed; material ids) into a staging buffer and a kernel
+        // writes the SoA planes (Fe = Fp = I, B = 0).  A large scene is
+        // written in cell-sorted order (pid keeps the caller's indices), the
+        // order its first step's P2G, grid and G2P read it in: in the
+        // caller's order (a random order, say) those gathers touch a new
+        // sector per particle and the first step costs three steady ones.
+        // The order of equal keys is the caller's, as in the step's stable
+        // sort, so the scene's steps are the same to the bit.
         if (p.n > 0) {
             const bool has_vol = d.volume_mode == MPM_VOLUME_PRESCRIBED;
             const size_t n = p.n;
-            MPM_TRY(grow(tmp_, sizeof(float) * (has_vol ? 8 : 7) * n, "particle upload buffer"));
+            const size_t mat_off = (sizeof(float) * (has_vol ? 8 : 7) * n + 15) / 16 * 16;
+            MPM_TRY(grow(tmp_, mat_off + (p.material ? sizeof(uint16_t) * n : 0), "particle upload buffer"));
             float* staged = tmp_.as<float>();
+            uint16_t* staged_mat = p.material ? (uint16_t*)((char*)tmp_.p + mat_off) : nullptr;
             CUDA_TRY(cudaMemcpyAsync(staged, p.position, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
             CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
                                      stream_));
             CUDA_TRY(cudaMemcpyAsync(staged + 6 * n, p.mass, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
             if (has_vol)
                 CUDA_TRY(cudaMemcpyAsync(staged + 7 * n, p.volume, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
-            const int b = parity_;
-            launchInitState(stream_, num_sms_, sc->buf_f[b].as<float>(), sc->buf_pid[b].as<uint32_t>(), cap, staged, n,
-                            has_vol);
-            CUDA_TRY(cudaGetLastError());
             if (p.material)
-                CUDA_TRY(cudaMemcpyAsync(sc->buf_mat[b].p, p.material, sizeof(uint16_t) * n, cudaMemcpyHostToDevice,
+                CUDA_TRY(cudaMemcpyAsync(staged_mat, p.material, sizeof(uint16_t) * n, cudaMemcpyHostToDevice,
                                          stream_));
-            else
-                CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * n, stream_));
+            const uint32_t* perm = nullptr;
+            DevMem sk[2], sv[2], sscr;  // back to the pool in the stream's order on return
+            if (n >= kSortedUploadMin && n < ((size_t)1 << 30)) {
+                SceneDev g{};
+                sceneGeometry(*sc, 0, g);
+                int bits = 1;
+                while (((uint64_t)1 << bits) < ((uint64_t)sc->nblocks + 1) * 64) ++bits;
+                for (int k = 0; k < 2; ++k) {
+                    MPM_TRY(alloc(sk[k], sizeof(uint32_t) * n, "upload sort keys"));
+                    MPM_TRY(alloc(sv[k], sizeof(uint32_t) * n, "upload sort values"));
+                }
+                MPM_TRY(alloc(sscr, sizeof(uint32_t) * onesweepScratchWords(n, bits), "upload sort scratch"));
+                launchStagedKeys(stream_, num_sms_, g, staged, (uint32_t)n, sk[0].as<uint32_t>(), err_.as<uint32_t>());
+                bool in_b = false;
+                CUDA_TRY(radixSortOnesweep(sk[0].as<uint32_t>(), sv[0].as<uint32_t>(), sk[1].as<uint32_t>(),
+                                           sv[1].as<uint32_t>(), n, bits, sscr.as<uint32_t>(), err_.as<uint32_t>(),
+                                           &in_b, stream_));
+                perm = sv[in_b ? 1 : 0].as<uint32_t>();
+            }
+            const int b = parity_;
+            launchInitState(stream_, num_sms_, sc->buf_f[b].as<float>(), sc->buf_pid[b].as<uint32_t>(),
+                            sc->buf_mat[b].as<uint16_t>(), cap, staged, n, has_vol, perm, staged_mat);
+            CUDA_TRY(cudaGetLastError());
+            if (!p.material) CUDA_TRY(cudaMemsetAsync(sc->buf_mat[b].p, 0, sizeof(uint16_t) * n, stream_));
             // The caller's arrays may be freed once this returns.  Copies from
             // pageable memory have taken the data by then; copies from
             // page-locked memory are asynchronous, so wait for those only.
@@ -772,6 +835,23 @@ public:
 
     // Rebuild the device scene table and the batch-wide scratch after the
     // set of scenes changed.
+    // The grid geometry of a scene's table entry (what its cell keys need),
+    // with its blocks numbered from block_base.
+    static void sceneGeometry(const SceneHost& s, uint32_t block_base, SceneDev& d) {
+        for (int a = 0; a < 3; ++a) {
+            d.origin[a] = s.desc.origin[a];
+            d.res[a] = s.desc.resolution[a];
+            d.nb[a] = s.nb[a];
+            d.target[a] = s.desc.origin[a] + s.desc.stride * (float)s.desc.resolution[a];
+        }
+        d.h = s.desc.stride;
+        d.inv_h = 1.0f / s.desc.stride;
+        d.range = stencilRange(s.desc.interpolation);
+        d.block_base = block_base;
+        d.nblocks = s.nblocks;
+        d.S = s.S;
+    }
+
     mpm_status rebuild() {
         if (!dirty_) return MPM_OK;
         CUDA_TRY(cudaStreamSynchronize(stream_));
@@ -786,17 +866,7 @@ public:
         for (int i = 0; i < ns; ++i) {
             SceneHost& s = *scenes_[i];
             SceneDev& d = host_scenes_[i];
-            for (int a = 0; a < 3; ++a) {
-                d.origin[a] = s.desc.origin[a];
-                d.res[a] = s.desc.resolution[a];
-                d.nb[a] = s.nb[a];
-                d.target[a] = s.desc.origin[a] + s.desc.stride * (float)s.desc.resolution[a];
-            }
-            d.h = s.desc.stride;
-            d.inv_h = 1.0f / s.desc.stride;
-            d.range = stencilRange(s.desc.interpolation);
-            d.block_base = (uint32_t)tb;
-            d.nblocks = s.nblocks;
+            sceneGeometry(s, (uint32_t)tb, d);
             sbb[i] = (uint32_t)tb;
             tb += (uint64_t)s.nblocks + 1;  // + the scene's outside block
             d.key_offset = (uint32_t)ntot;
@@ -815,7 +885,6 @@ public:
             }
             d.transfer = s.desc.transfer;
             d.interp = s.desc.interpolation;
-            d.S = s.S;
             d.combo = comboIndex(s.S, s.desc.transfer);
             d.boundary = s.desc.boundary;
             d.sticky = s.desc.sticky_cells;
@@ -2092,7 +2161,7 @@ public:
         if (field == MPM_FIELD_B && s.desc.transfer != MPM_TRANSFER_APIC)
             return fail(MPM_ERR_INVALID_ARG, "B is only defined for APIC scenes");
         if (s.n == 0) return MPM_OK;
-        if (!copy_stream_) CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+        if (!copy_stream_) CUDA_TRY(takeStream(device_, &copy_stream_));
         if (!s.stage_ready[0])
             for (int k = 0; k < 2; ++k) {
                 CUDA_TRY(cudaEventCreateWithFlags(&s.stage_ready[k], cudaEventDisableTiming));
@@ -2344,7 +2413,7 @@ private:
         if (!fork_) CUDA_TRY(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
         for (int k = 0; k < n; ++k)
             if (!side_[k]) {
-                CUDA_TRY(cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking));
+                CUDA_TRY(takeStream(device_, &side_[k]));
                 CUDA_TRY(cudaEventCreateWithFlags(&join_[k], cudaEventDisableTiming));
             }
         return MPM_OK;

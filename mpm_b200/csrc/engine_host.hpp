@@ -85,8 +85,13 @@ void launchDensePack(const LaunchCtx& c);
 void launchParticlesCollision(const LaunchCtx& c, int parity, float dt);
 void launchAdvect(const LaunchCtx& c, int parity, float dt);
 void launchVolume(const LaunchCtx& c, int parity, int S);
-void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, size_t cap, const float* staged, size_t n,
-                     bool has_volume);
+// A new scene's particle planes from its staged arrays, slot i from the
+// caller's particle perm[i] (perm null: i); mat_in null: no material ids.
+void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, uint16_t* mat, size_t cap,
+                     const float* staged, size_t n, bool has_volume, const uint32_t* perm, const uint16_t* mat_in);
+// Cell keys (sc's block numbering) of n staged interleaved positions.
+void launchStagedKeys(cudaStream_t st, int num_sms, const SceneDev& sc, const float* xyz, uint32_t n, uint32_t* keys,
+                      uint32_t* err);
 void launchDensity(const LaunchCtx& c, const float4* vstar, size_t nodes, float inv_cell_vol, float* out);
 // Semi-implicit solve (implicit.cu) of the scenes with beta > 0.  Global
 // buffers over the sorted particles of the batch and its cell keys.

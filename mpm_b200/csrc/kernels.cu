@@ -132,11 +132,20 @@ __global__ void __launch_bounds__(kThreads) keyKernel(const SceneDev* __restrict
     const SceneDev& sc = scenes[blockIdx.y];
     const float* f = sc.buf[parity].f;
     const size_t cap = sc.cap;
-    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < sc.n; i += gridDim.x * kThreads) {
-        float x[3] = {f[(F_X + 0) * cap + i], f[(F_X + 1) * cap + i], f[(F_X + 2) * cap + i]};
-        uint32_t key = particleKey(sc, x, err);
-        keys[sc.key_offset + i] = key;
-        atomicAdd(&block_count[key >> 6], 1u);
+    // whole warps iterate together, so that a warp's particles of one block
+    // add to its count with one atomic (cell-sorted particles share blocks)
+    const uint32_t n_round = (sc.n + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n_round; i += gridDim.x * kThreads) {
+        const bool valid = i < sc.n;
+        uint32_t blk = 0xffffffffu;
+        if (valid) {
+            float x[3] = {f[(F_X + 0) * cap + i], f[(F_X + 1) * cap + i], f[(F_X + 2) * cap + i]};
+            const uint32_t key = particleKey(sc, x, err);
+            keys[sc.key_offset + i] = key;
+            blk = key >> 6;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, blk);
+        if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&block_count[blk], (uint32_t)__popc(peers));
     }
 }
 
@@ -404,6 +413,17 @@ __global__ void __launch_bounds__(kThreads) stressKernel(const SceneDev* __restr
         for (int k = 0; k < 9; ++k) {
             Fe[k] = f[(F_FE + k) * cap + i];
             Fp[k] = f[(F_FP + k) * cap + i];
+        }
+        // Fe = I (a new scene): tau = 0 exactly for both models (R = I,
+        // J = 1), without the FP32 SVD's round-off in s (~1e-7), which a
+        // stiff material turns into a spurious force at light surface nodes.
+        bool identity = true;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) identity = identity && Fe[k] == ((k % 4 == 0) ? 1.f : 0.f);
+        if (identity) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) f[(F_TAU + k) * cap + i] = 0.f;
+            continue;
         }
         MaterialDev m = sc.mats[sc.nmat > 1 ? mat[i] : 0];
         stressFromFe(m, Fe, Fp, f[F_VOL * cap + i], tau);
@@ -1922,13 +1942,18 @@ __global__ void advectKernel(const SceneDev* __restrict__ scenes, int parity, fl
 // as [x: 3n interleaved][v: 3n interleaved][m: n][V0: n, prescribed only]:
 // SoA planes with Fe = Fp = I, B = tau = 0 and V0 = 0 unless prescribed
 // (the reference's MaterialPoint3D constructor, src/material_point3d.cu:10-30).
-__global__ void initStateKernel(float* __restrict__ f, uint32_t* __restrict__ pid, size_t cap,
-                                const float* __restrict__ staged, size_t n, int has_volume) {
+// With `perm` slot i takes the caller's particle perm[i] (the cell-sorted
+// order), else particle i; pid records it.  mat_in: the caller's material ids
+// (staged), else none.
+__global__ void initStateKernel(float* __restrict__ f, uint32_t* __restrict__ pid, uint16_t* __restrict__ mat,
+                                size_t cap, const float* __restrict__ staged, size_t n, int has_volume,
+                                const uint32_t* __restrict__ perm, const uint16_t* __restrict__ mat_in) {
     for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
+        const size_t o = perm ? (size_t)perm[i] : i;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            f[(F_X + a) * cap + i] = staged[3 * i + a];
-            f[(F_V + a) * cap + i] = staged[3 * n + 3 * i + a];
+            f[(F_X + a) * cap + i] = staged[3 * o + a];
+            f[(F_V + a) * cap + i] = staged[3 * n + 3 * o + a];
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
@@ -1938,9 +1963,21 @@ __global__ void initStateKernel(float* __restrict__ f, uint32_t* __restrict__ pi
         }
 #pragma unroll
         for (int k = 0; k < 6; ++k) f[(F_TAU + k) * cap + i] = 0.f;
-        f[F_MASS * cap + i] = staged[6 * n + i];
-        f[F_VOL * cap + i] = has_volume ? staged[7 * n + i] : 0.f;
-        pid[i] = (uint32_t)i;
+        f[F_MASS * cap + i] = staged[6 * n + o];
+        f[F_VOL * cap + i] = has_volume ? staged[7 * n + o] : 0.f;
+        pid[i] = (uint32_t)o;
+        if (mat_in) mat[i] = mat_in[o];
+    }
+}
+
+// Cell keys of a new scene's staged positions (caller order, x y z
+// interleaved), for the cell-sorted initial order.
+__global__ void __launch_bounds__(kThreads) stagedKeyKernel(const SceneDev sc, const float* __restrict__ xyz,
+                                                             uint32_t n, uint32_t* __restrict__ keys,
+                                                             uint32_t* __restrict__ err) {
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        const float x[3] = {xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2]};
+        keys[i] = particleKey(sc, x, err);
     }
 }
 
@@ -2176,12 +2213,19 @@ void launchAdvect(const LaunchCtx& c, int parity, float dt) {
     noteLaunches(1);
     advectKernel<<<dim3(c.particle_blocks, c.nscenes), kThreads, 0, c.stream>>>(c.scenes, parity, dt);
 }
-void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, size_t cap, const float* staged, size_t n,
-                     bool has_volume) {
+void launchInitState(cudaStream_t st, int num_sms, float* f, uint32_t* pid, uint16_t* mat, size_t cap,
+                     const float* staged, size_t n, bool has_volume, const uint32_t* perm, const uint16_t* mat_in) {
     if (n == 0) return;
     noteLaunches(1);
     const unsigned blocks = (unsigned)std::min<size_t>((n + kThreads - 1) / kThreads, (size_t)num_sms * 8);
-    initStateKernel<<<blocks, kThreads, 0, st>>>(f, pid, cap, staged, n, has_volume ? 1 : 0);
+    initStateKernel<<<blocks, kThreads, 0, st>>>(f, pid, mat, cap, staged, n, has_volume ? 1 : 0, perm, mat_in);
+}
+void launchStagedKeys(cudaStream_t st, int num_sms, const SceneDev& sc, const float* xyz, uint32_t n, uint32_t* keys,
+                      uint32_t* err) {
+    if (n == 0) return;
+    noteLaunches(1);
+    const unsigned blocks = (unsigned)std::min<size_t>((n + kThreads - 1) / kThreads, (size_t)num_sms * 8);
+    stagedKeyKernel<<<blocks, kThreads, 0, st>>>(sc, xyz, n, keys, err);
 }
 void launchVolume(const LaunchCtx& c, int parity, int S) {
     noteLaunches(1);

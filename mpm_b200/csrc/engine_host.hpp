@@ -41,6 +41,15 @@ void noteLaunches(uint64_t n);
 uint64_t kernelLaunches();
 
 // sort.cu
+// Up to four word ranges zeroed by one kernel launch (launchClear): the
+// step's scratch clears are kernels rather than memset nodes, which a
+// device-to-host copy running beside the step (an asynchronous download on
+// another stream) held back by 8-20 us each.
+struct ClearRanges {
+    uint32_t* p[4] = {};
+    size_t n[4] = {};
+};
+void launchClear(const ClearRanges& r, cudaStream_t st);
 size_t scanScratchElems(size_t n);
 template <class T>
 cudaError_t exclusiveScan(const T* in, T* out, size_t n, T* partials, T* total, cudaStream_t st);

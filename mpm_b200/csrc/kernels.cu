@@ -2070,10 +2070,16 @@ size_t compactScratchWords64(uint32_t total_blocks) {
 void launchCompactOnesweep(const LaunchCtx& c, const BlockBuffers& bb, uint32_t total_blocks,
                            unsigned long long* scratch, uint32_t chunk, const ComboSplit& split, uint32_t* err) {
     const uint32_t ntiles = (uint32_t)((total_blocks + kCompactTile - 1) / kCompactTile);
-    cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * compactScratchWords64(total_blocks), c.stream);
-    cudaMemsetAsync(bb.counters, 0, sizeof(uint32_t) * 4, c.stream);
-    cudaMemsetAsync(bb.counters + kG2PCountWord, 0, sizeof(uint32_t) * kMaxCombos, c.stream);
-    cudaMemsetAsync(bb.counters + kP2GListWord, 0, sizeof(uint32_t) * 4 * kMaxCombos, c.stream);  // lists, small, back
+    ClearRanges cr;
+    cr.p[0] = reinterpret_cast<uint32_t*>(scratch);
+    cr.n[0] = 2 * compactScratchWords64(total_blocks);
+    cr.p[1] = bb.counters;
+    cr.n[1] = 4;
+    cr.p[2] = bb.counters + kG2PCountWord;
+    cr.n[2] = kMaxCombos;
+    cr.p[3] = bb.counters + kP2GListWord;  // lists, small, back
+    cr.n[3] = 4 * kMaxCombos;
+    launchClear(cr, c.stream);
     noteLaunches(1);
     compactOnesweepKernel<<<ntiles, kThreads, 0, c.stream>>>(
         bb.block_count, total_blocks, bb.scene_block_base, c.nscenes, bb.active, bb.outside, bb.counters,

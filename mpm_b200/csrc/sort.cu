@@ -346,7 +346,27 @@ __global__ void __launch_bounds__(kThreads, 4) onesweepPassKernel(const uint32_t
     }
 }
 
+__global__ void __launch_bounds__(kThreads) clearRangesKernel(ClearRanges r) {
+    const size_t stride = (size_t)gridDim.x * kThreads;
+    const size_t t = (size_t)blockIdx.x * kThreads + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        for (size_t i = t; i < r.n[k]; i += stride) r.p[k][i] = 0u;
+}
+
 }  // namespace
+
+void launchClear(const ClearRanges& r, cudaStream_t st) {
+    size_t most = 0;
+    for (int k = 0; k < 4; ++k) most = std::max(most, r.p[k] ? r.n[k] : 0);
+    if (most == 0) return;
+    ClearRanges q = r;
+    for (int k = 0; k < 4; ++k)
+        if (!q.p[k]) q.n[k] = 0;
+    noteLaunches(1);
+    const unsigned blocks = (unsigned)std::min<size_t>((most + kThreads - 1) / kThreads, 148 * 4);
+    clearRangesKernel<<<blocks, kThreads, 0, st>>>(q);
+}
 
 // ---------------------------------------------------------------------------
 // Host wrappers.
@@ -372,8 +392,12 @@ cudaError_t radixSortOnesweep(uint32_t* keys_a, uint32_t* vals_a, uint32_t* keys
     uint32_t* ghist = scratch;
     uint32_t* counters = scratch + (size_t)passes * 256;
     uint32_t* status = counters + 32;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * onesweepScratchWords(n, bits), st);
-    if (e != cudaSuccess) return e;
+    {
+        ClearRanges cr;
+        cr.p[0] = scratch;
+        cr.n[0] = onesweepScratchWords(n, bits);
+        launchClear(cr, st);
+    }
     // ~4 keys per thread: the histogram is bound by each thread's serial
     // chain of match/atomic rounds, not by the per-block flush (1M keys:
     // 16 keys per thread 0.072 ms for the whole sort, 4 keys 0.065 ms)
@@ -686,8 +710,13 @@ cudaError_t incrementalSort(const uint32_t* keys, const uint32_t* prev, size_t n
     uint32_t* split = status + ptiles;
     const size_t nsplit = mergeSplits(n);
     uint32_t* sort_scratch = split + nsplit;
-    cudaError_t e = cudaMemsetAsync(m_dev, 0, sizeof(uint32_t) * (2 + ptiles), st);
-    if (e != cudaSuccess) return e;
+    {
+        ClearRanges cr;
+        cr.p[0] = m_dev;
+        cr.n[0] = 2 + ptiles;
+        launchClear(cr, st);
+    }
+    cudaError_t e = cudaSuccess;
     noteLaunches(3);
     moverPartitionKernel<<<(unsigned)ptiles, kThreads, 0, st>>>(keys, prev, (uint32_t)n, a_keys, a_idx, b_keys, b_idx,
                                                                 m_dev, tile_counter, status, (uint32_t)ptiles, err);

@@ -567,18 +567,39 @@ public:
             MPM_TRY(grow(tmp_, mat_off + (p.material ? sizeof(uint16_t) * n : 0), "particle upload buffer"));
             float* staged = tmp_.as<float>();
             uint16_t* staged_mat = p.material ? (uint16_t*)((char*)tmp_.p + mat_off) : nullptr;
+            const bool sorted = n >= kSortedUploadMin && n < ((size_t)1 << 30);
+            // On an error return below, copies already queued still read the
+            // caller's arrays: wait for them first.
+            struct Drain {
+                cudaStream_t a, b;
+                bool on;
+                ~Drain() {
+                    if (on) {
+                        cudaStreamSynchronize(a);
+                        cudaStreamSynchronize(b);
+                    }
+                }
+            } drain{stream_, compact_stream_, true};
             CUDA_TRY(cudaMemcpyAsync(staged, p.position, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
-            CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
-                                     stream_));
-            CUDA_TRY(cudaMemcpyAsync(staged + 6 * n, p.mass, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+            // With the sort, the other arrays follow the positions on the
+            // compaction stream (idle here), so that the positions' keys and
+            // sort run while they cross the bus.
+            cudaStream_t rest = stream_;
+            if (sorted) {
+                CUDA_TRY(cudaEventRecord(compact_fork_, stream_));
+                CUDA_TRY(cudaStreamWaitEvent(compact_stream_, compact_fork_, 0));
+                rest = compact_stream_;
+            }
+            CUDA_TRY(cudaMemcpyAsync(staged + 3 * n, p.velocity, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, rest));
+            CUDA_TRY(cudaMemcpyAsync(staged + 6 * n, p.mass, sizeof(float) * n, cudaMemcpyHostToDevice, rest));
             if (has_vol)
-                CUDA_TRY(cudaMemcpyAsync(staged + 7 * n, p.volume, sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+                CUDA_TRY(cudaMemcpyAsync(staged + 7 * n, p.volume, sizeof(float) * n, cudaMemcpyHostToDevice, rest));
             if (p.material)
-                CUDA_TRY(cudaMemcpyAsync(staged_mat, p.material, sizeof(uint16_t) * n, cudaMemcpyHostToDevice,
-                                         stream_));
+                CUDA_TRY(cudaMemcpyAsync(staged_mat, p.material, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, rest));
+            if (sorted) CUDA_TRY(cudaEventRecord(compact_join_, compact_stream_));
             const uint32_t* perm = nullptr;
             DevMem sk[2], sv[2], sscr;  // back to the pool in the stream's order on return
-            if (n >= kSortedUploadMin && n < ((size_t)1 << 30)) {
+            if (sorted) {
                 SceneDev g{};
                 sceneGeometry(*sc, 0, g);
                 int bits = 1;
@@ -594,6 +615,7 @@ public:
                                            sv[1].as<uint32_t>(), n, bits, sscr.as<uint32_t>(), err_.as<uint32_t>(),
                                            &in_b, stream_));
                 perm = sv[in_b ? 1 : 0].as<uint32_t>();
+                CUDA_TRY(cudaStreamWaitEvent(stream_, compact_join_, 0));
             }
             const int b = parity_;
             launchInitState(stream_, num_sms_, sc->buf_f[b].as<float>(), sc->buf_pid[b].as<uint32_t>(),
@@ -604,6 +626,7 @@ public:
             // pageable memory have taken the data by then; copies from
             // page-locked memory are asynchronous, so wait for those only.
             if (anyPinned({p.position, p.velocity, p.mass, p.volume, p.material})) CUDA_TRY(cudaStreamSynchronize(stream_));
+            drain.on = false;
         }
         sc->need_init = true;
         sc->stress_stale = true;

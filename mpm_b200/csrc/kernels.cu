@@ -2003,16 +2003,26 @@ __global__ void volumeKernel(const SceneDev* __restrict__ scenes, int parity) {
                     float gp = __fadd_rn(sc.origin[a], __fmul_rn(h, (float)(base[a] + k)));
                     w[a][k] = splineN<S>(__fdiv_rn(__fsub_rn(x[a], gp), h));
                 }
+            // nodes in the grid per axis (all of them but at the edges); the
+            // sum runs over the stencil in the same order either way
+            bool in[3][S];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int k = 0; k < S; ++k) in[a][k] = base[a] + k >= 0 && base[a] + k < sc.res[a];
+            const size_t X = (size_t)sc.res[0], XY = X * (size_t)sc.res[1];
+            const float* mass = reinterpret_cast<const float*>(sc.vstar) + 3;  // vstar[node].w
+            const long long n0 = (long long)base[0] + (long long)X * base[1] + (long long)XY * base[2];
+#pragma unroll
             for (int c = 0; c < S; ++c)
+#pragma unroll
                 for (int b = 0; b < S; ++b)
+#pragma unroll
                     for (int a = 0; a < S; ++a) {
-                        int n[3] = {base[0] + a, base[1] + b, base[2] + c};
-                        if (n[0] < 0 || n[1] < 0 || n[2] < 0 || n[0] >= sc.res[0] || n[1] >= sc.res[1] ||
-                            n[2] >= sc.res[2])
-                            continue;
-                        size_t node = (size_t)n[0] + (size_t)sc.res[0] * ((size_t)n[1] + (size_t)sc.res[1] * n[2]);
-                        float wgt = w[0][a] * w[1][b] * w[2][c];
-                        dens += (sc.vstar[node].w * wgt) * inv_cell_vol;
+                        if (!(in[0][a] && in[1][b] && in[2][c])) continue;
+                        const size_t node = (size_t)(n0 + a + (long long)X * b + (long long)XY * c);
+                        const float wgt = w[0][a] * w[1][b] * w[2][c];
+                        dens += (__ldg(mass + 4 * node) * wgt) * inv_cell_vol;
                     }
         }
         f[F_VOL * cap + i] = f[F_MASS * cap + i] / dens;

@@ -356,6 +356,10 @@ __global__ void __launch_bounds__(kThreads) clearRangesKernel(ClearRanges r) {
 
 }  // namespace
 
+// A grid-stride clear: four CTAs of 256 threads per SM of a B200 cover the
+// largest range (a few MB) in one or two passes.
+constexpr size_t kClearMaxBlocks = 148 * 4;
+
 void launchClear(const ClearRanges& r, cudaStream_t st) {
     size_t most = 0;
     for (int k = 0; k < 4; ++k) most = std::max(most, r.p[k] ? r.n[k] : 0);
@@ -364,7 +368,7 @@ void launchClear(const ClearRanges& r, cudaStream_t st) {
     for (int k = 0; k < 4; ++k)
         if (!q.p[k]) q.n[k] = 0;
     noteLaunches(1);
-    const unsigned blocks = (unsigned)std::min<size_t>((most + kThreads - 1) / kThreads, 148 * 4);
+    const unsigned blocks = (unsigned)std::min<size_t>((most + kThreads - 1) / kThreads, kClearMaxBlocks);
     clearRangesKernel<<<blocks, kThreads, 0, st>>>(q);
 }
 
